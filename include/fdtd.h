@@ -1,0 +1,149 @@
+/*
+ * C ABI of the B200 FDTD engine (librfn_fdtd.so).
+ *
+ * Replaces the reference's engine entry points for the 3D FDTD time loop:
+ *   cuda_func.solver_run_cu  rfnetwork/core/src/cuda_binding.cpp:20-68
+ *   core_func.solver_run     rfnetwork/core/src/core_binding.cpp:350-394
+ * both called from FDTD_Solver.solve() at rfnetwork/solver.py:1636-1641, and the
+ * engine behind them, SolverFDTD (rfnetwork/core/inc/solver.h:116-176).
+ *
+ * The reference takes one Python call with a dict of 30 coefficient arrays, a
+ * probe list and a monitor list. Here the same data goes through plain
+ * pointers and sizes on a handle; rfnetwork_b200/cuda_func.py rebuilds the
+ * reference call (same signature, in-place results) on top of these.
+ *
+ * Conventions
+ *  - Every function returns 0 on success and a nonzero FDTD_ERR_* code on
+ *    failure; the message is in fdtd_last_error(). Nothing throws across the ABI.
+ *  - Coefficient arrays are float32, C order [x][y][z] (z fastest), shape
+ *    (nx, ny, nz): the "GPU shapes" the reference packs with gpu=True
+ *    (rfnetwork/solver.py:1460-1518).
+ *  - Field codes: 0 ex, 1 ey, 2 ez, 3 hx, 4 hy, 5 hz (rfnetwork/solver.py:1560).
+ *  - Probe indices are full-grid component indices (the "idx" entry of a
+ *    probe dict, rfnetwork/solver.py:1557-1575); the engine applies the Yee
+ *    shift of solver_init_probes (rfnetwork/core/src/solver.cpp:503-525).
+ *  - A handle is not thread-safe; distinct handles may be used concurrently.
+ */
+#ifndef RFN_FDTD_H
+#define RFN_FDTD_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FDTD_OK 0
+#define FDTD_ERR_ARG 1        /* invalid argument, shape or index */
+#define FDTD_ERR_CUDA 2       /* CUDA runtime error */
+#define FDTD_ERR_STATE 3      /* call out of order (e.g. run before coefficients) */
+#define FDTD_ERR_LIMIT 4      /* a size limit was exceeded */
+#define FDTD_ERR_DEVICE 5     /* the kernel reported an error status */
+
+typedef struct fdtd_sim fdtd_sim;
+typedef struct fdtd_batch fdtd_batch;
+
+/* Statistics of the last prepared / run simulation. */
+typedef struct fdtd_stats {
+  int nx, ny, nz, nt;
+  int n_rows;            /* distinct coefficient rows in the material table */
+  int id_bytes;          /* bytes per cell of the material index (1 or 2) */
+  int64_t e_split_cells; /* cells whose E components are stored as split fields */
+  int64_t h_split_cells; /* cells whose H components are stored as split fields */
+  int n_tiles;           /* thread blocks per time step */
+  int64_t step_launches; /* time-step kernel launches issued by the last run */
+  int64_t dft_launches;  /* DFT kernel launches issued by the last run */
+  double last_run_ms;    /* device time of the last run (CUDA events) */
+  double compile_ms;     /* host time spent building the material table */
+} fdtd_stats;
+
+/* --------------------------------------------------------------- one grid */
+
+/* New simulation of nx x ny x nz cells (SolverFDTD::solver_init_fields,
+ * rfnetwork/core/src/solver.cpp:239-349). Device memory is taken on first run. */
+int fdtd_create(int nx, int ny, int nz, fdtd_sim** out);
+
+/* Set one of the 30 coefficient arrays by its reference name ("Ca_ex_y",
+ * "Db_hz_y2", ...; rfnetwork/solver.py:1473-1518). The data is copied. The
+ * last x plane of the Cy, Cz and Dx groups is treated as zero, as
+ * solver_init_fields does (rfnetwork/core/src/solver.cpp:294-328). */
+int fdtd_set_coefficient(fdtd_sim* s, const char* name, const float* data, int nx, int ny, int nz);
+
+/* Add a probe (solver_init_probes, rfnetwork/core/src/solver.cpp:465-532).
+ * values: n_values >= nt floats, the soft-source amplitude per time step when
+ * is_source is nonzero (copied). The recorded field series is read back with
+ * fdtd_get_probe_values. Returns the probe's index through *index (may be NULL). */
+int fdtd_add_probe(fdtd_sim* s, int field, int i, int j, int k, int is_source, const float* values,
+                   int n_values, int* index);
+
+/* Plane field monitor (solver_init_monitors, rfnetwork/core/src/solver.cpp:351-463,
+ * GPU layout): axis 0/1/2, position = plane index as in the monitor dict,
+ * samples every n_step steps. n_freq == 0: time samples, output float32
+ * [nt/n_step+1][N1][N2]. n_freq > 0: phasors, output complex64 [n_freq][N1][N2]
+ * accumulated with phase[m][f] (complex64 [nt/n_step+1][n_freq], interleaved re/im). */
+int fdtd_add_monitor(fdtd_sim* s, int field, int axis, int position, int n_step, int n_freq,
+                     const float* phase, int n_phase_rows, int* index);
+
+/* Running DFT in FP64 of n_series probe combinations at n_freq angular
+ * frequencies (radians per time step): X[s][f] = sum_n (sum_t w_t probe_t[n]) e^{-j omega_f n}.
+ * Terms t = 0..n_terms-1 give (series, probe, weight). This is the DTFT of
+ * rfnetwork/utils.py:14-71 applied to the port voltage / current series of
+ * rfnetwork/solver.py:2482-2504, accumulated on the device during the run. */
+int fdtd_set_dft(fdtd_sim* s, int n_series, int n_terms, const int* term_series, const int* term_probe,
+                 const double* term_weight, int n_freq, const double* omega);
+
+/* Build the material table on the host now (the first run does it otherwise).
+ * Needs no GPU. Any output pointer may be NULL. */
+int fdtd_compile(fdtd_sim* s, int* n_rows, int64_t* e_split_cells, int64_t* h_split_cells);
+
+/* Copy the compiled material table: ids in the reference order [x][y][z]
+ * (nx*ny*nz uint16 row indices) and rows (n_rows x 32 uint32 words: 30
+ * coefficients as float bits in the kernel's slot order, flags, probe-list
+ * offset). Either output may be NULL. */
+int fdtd_get_material_table(fdtd_sim* s, uint16_t* ids, int64_t n_ids, uint32_t* rows, int n_rows);
+
+/* Run nt time steps from zero fields (SolverFDTD::solver_run_cu,
+ * rfnetwork/core/src/solver.cu:546-1143). Synchronous. */
+int fdtd_run(fdtd_sim* s, int nt);
+
+/* Asynchronous run on the handle's stream; fdtd_synchronize waits for it. */
+int fdtd_run_async(fdtd_sim* s, int nt);
+int fdtd_synchronize(fdtd_sim* s);
+
+/* Launch on a caller stream (cudaStream_t passed as void*); NULL = own stream. */
+int fdtd_set_stream(fdtd_sim* s, void* stream);
+
+/* Results of the last run. out: n_probes x nt floats, probe-major. */
+int fdtd_get_probe_values(fdtd_sim* s, float* out, int n_probes, int nt);
+/* out: n_series x n_freq x 2 doubles (re, im). */
+int fdtd_get_dft(fdtd_sim* s, double* out, int n_series, int n_freq);
+/* Monitor m's output buffer (see fdtd_add_monitor for the layout); n_bytes checked. */
+int fdtd_get_monitor(fdtd_sim* s, int m, void* out, int64_t n_bytes);
+
+int fdtd_get_stats(const fdtd_sim* s, fdtd_stats* out);
+const char* fdtd_last_error(const fdtd_sim* s);
+void fdtd_destroy(fdtd_sim* s);
+
+/* ---------------------------------------------------------------- batches */
+
+/* Many independent simulations of uneven sizes stepped together: one kernel
+ * launch per time step covers the tile work lists of all members, and the time
+ * loop is captured as a CUDA graph. The reference has no batched engine; its
+ * counterpart is one solver_run_cu call per simulation
+ * (rfnetwork/core/src/cuda_binding.cpp:20-68). Members keep their own
+ * coefficients, probes and DFT; results are read per member after the run. */
+int fdtd_batch_create(fdtd_sim* const* sims, int n_sims, fdtd_batch** out);
+int fdtd_batch_run(fdtd_batch* b, int nt);
+int fdtd_batch_set_stream(fdtd_batch* b, void* stream);
+int fdtd_batch_get_stats(const fdtd_batch* b, fdtd_stats* out);
+const char* fdtd_batch_last_error(const fdtd_batch* b);
+void fdtd_batch_destroy(fdtd_batch* b);
+
+/* Last error of calls that have no handle (fdtd_create, fdtd_batch_create). */
+const char* fdtd_global_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* RFN_FDTD_H */

@@ -1,0 +1,280 @@
+"""ctypes binding of librfn_fdtd.so (declarations: include/fdtd.h).
+
+The library is the only compute path: if it is missing or cannot be loaded,
+every entry point raises -- there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes
+from pathlib import Path
+
+import numpy as np
+
+LIB_PATH = Path(__file__).resolve().parent / "librfn_fdtd.so"
+
+FDTD_ERRORS = {1: "invalid argument", 2: "CUDA error", 3: "call out of order", 4: "size limit", 5: "device error"}
+
+EXPORTED = (
+    "fdtd_create", "fdtd_set_coefficient", "fdtd_add_probe", "fdtd_add_monitor", "fdtd_set_dft",
+    "fdtd_compile", "fdtd_get_material_table",
+    "fdtd_run", "fdtd_run_async", "fdtd_synchronize", "fdtd_set_stream", "fdtd_get_probe_values",
+    "fdtd_get_dft", "fdtd_get_monitor", "fdtd_get_stats", "fdtd_last_error", "fdtd_destroy",
+    "fdtd_batch_create", "fdtd_batch_run", "fdtd_batch_set_stream", "fdtd_batch_get_stats",
+    "fdtd_batch_last_error", "fdtd_batch_destroy", "fdtd_global_error",
+)
+
+
+class FdtdStats(ctypes.Structure):
+    _fields_ = [
+        ("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int), ("nt", ctypes.c_int),
+        ("n_rows", ctypes.c_int), ("id_bytes", ctypes.c_int),
+        ("e_split_cells", ctypes.c_int64), ("h_split_cells", ctypes.c_int64),
+        ("n_tiles", ctypes.c_int), ("step_launches", ctypes.c_int64), ("dft_launches", ctypes.c_int64),
+        ("last_run_ms", ctypes.c_double), ("compile_ms", ctypes.c_double),
+    ]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+_lib = None
+
+
+def load():
+    """Load the engine library (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not LIB_PATH.exists():
+        raise RuntimeError(f"{LIB_PATH.name} is not built; run `python -m rfnetwork_b200.build` "
+                           "(the FDTD engine has no CPU fallback).")
+    lib = ctypes.CDLL(str(LIB_PATH))
+    vp, ip, i64 = ctypes.c_void_p, ctypes.c_int, ctypes.c_int64
+    pp = ctypes.POINTER(ctypes.c_void_p)
+    sig = {
+        "fdtd_create": ([ip, ip, ip, pp], ip),
+        "fdtd_set_coefficient": ([vp, ctypes.c_char_p, vp, ip, ip, ip], ip),
+        "fdtd_add_probe": ([vp, ip, ip, ip, ip, ip, vp, ip, ctypes.POINTER(ip)], ip),
+        "fdtd_add_monitor": ([vp, ip, ip, ip, ip, ip, vp, ip, ctypes.POINTER(ip)], ip),
+        "fdtd_set_dft": ([vp, ip, ip, vp, vp, vp, ip, vp], ip),
+        "fdtd_compile": ([vp, ctypes.POINTER(ip), ctypes.POINTER(i64), ctypes.POINTER(i64)], ip),
+        "fdtd_get_material_table": ([vp, vp, i64, vp, ip], ip),
+        "fdtd_run": ([vp, ip], ip),
+        "fdtd_run_async": ([vp, ip], ip),
+        "fdtd_synchronize": ([vp], ip),
+        "fdtd_set_stream": ([vp, vp], ip),
+        "fdtd_get_probe_values": ([vp, vp, ip, ip], ip),
+        "fdtd_get_dft": ([vp, vp, ip, ip], ip),
+        "fdtd_get_monitor": ([vp, ip, vp, i64], ip),
+        "fdtd_get_stats": ([vp, ctypes.POINTER(FdtdStats)], ip),
+        "fdtd_last_error": ([vp], ctypes.c_char_p),
+        "fdtd_destroy": ([vp], None),
+        "fdtd_batch_create": ([pp, ip, pp], ip),
+        "fdtd_batch_run": ([vp, ip], ip),
+        "fdtd_batch_set_stream": ([vp, vp], ip),
+        "fdtd_batch_get_stats": ([vp, ctypes.POINTER(FdtdStats)], ip),
+        "fdtd_batch_last_error": ([vp], ctypes.c_char_p),
+        "fdtd_batch_destroy": ([vp], None),
+        "fdtd_global_error": ([], ctypes.c_char_p),
+    }
+    for name, (args, res) in sig.items():
+        fn = getattr(lib, name)
+        fn.argtypes = args
+        fn.restype = res
+    _lib = lib
+    return lib
+
+
+def _ptr(a: np.ndarray):
+    return ctypes.c_void_p(a.ctypes.data)
+
+
+class FdtdError(RuntimeError):
+    pass
+
+
+class Simulation:
+    """One FDTD grid on the GPU (an ``fdtd_sim`` handle).
+
+    Coefficients are the reference's GPU-shaped (nx, ny, nz) float32 arrays.
+    """
+
+    def __init__(self, nx: int, ny: int, nz: int):
+        self.lib = load()
+        h = ctypes.c_void_p()
+        rc = self.lib.fdtd_create(int(nx), int(ny), int(nz), ctypes.byref(h))
+        if rc:
+            raise ValueError(self.lib.fdtd_global_error().decode())
+        self.h = h
+        self.shape = (int(nx), int(ny), int(nz))
+        self.n_probes = 0
+        self.n_series = 0
+        self.n_freq = 0
+        self.monitors = []
+        self.nt = None
+
+    def _check(self, rc):
+        if rc:
+            msg = self.lib.fdtd_last_error(self.h).decode()
+            if rc == 1:
+                raise ValueError(msg)
+            raise FdtdError(f"{FDTD_ERRORS.get(rc, rc)}: {msg}")
+
+    def set_coefficient(self, name: str, arr: np.ndarray):
+        a = np.ascontiguousarray(arr, dtype=np.float32)
+        if a.ndim != 3:
+            raise ValueError("Invalid data array. Wrong number of dimensions.")
+        self._check(self.lib.fdtd_set_coefficient(self.h, name.encode(), _ptr(a), *a.shape))
+
+    def set_coefficients(self, coefficients: dict):
+        for k, v in coefficients.items():
+            self.set_coefficient(k, v)
+
+    def add_probe(self, field: int, idx, is_source: bool = False, values=None) -> int:
+        out = ctypes.c_int()
+        if values is not None:
+            v = np.ascontiguousarray(values, dtype=np.float32)
+            rc = self.lib.fdtd_add_probe(self.h, int(field), int(idx[0]), int(idx[1]), int(idx[2]),
+                                         int(bool(is_source)), _ptr(v), int(v.size), ctypes.byref(out))
+        else:
+            rc = self.lib.fdtd_add_probe(self.h, int(field), int(idx[0]), int(idx[1]), int(idx[2]),
+                                         int(bool(is_source)), None, 0, ctypes.byref(out))
+        self._check(rc)
+        self.n_probes = out.value + 1
+        return out.value
+
+    def add_monitor(self, field: int, axis: int, position: int, n_step: int = 1, phase=None) -> int:
+        out = ctypes.c_int()
+        if phase is not None:
+            ph = np.ascontiguousarray(phase, dtype=np.complex64)
+            rc = self.lib.fdtd_add_monitor(self.h, int(field), int(axis), int(position), int(n_step),
+                                           int(ph.shape[1]), _ptr(ph), int(ph.shape[0]), ctypes.byref(out))
+            nf = int(ph.shape[1])
+        else:
+            rc = self.lib.fdtd_add_monitor(self.h, int(field), int(axis), int(position), int(n_step), 0, None, 0,
+                                           ctypes.byref(out))
+            nf = 0
+        self._check(rc)
+        nx, ny, nz = self.shape
+        n1 = ny if axis == 0 else nx
+        n2 = ny if axis == 2 else nz
+        self.monitors.append(dict(n_freq=nf, n_step=int(n_step), n1=n1, n2=n2))
+        return out.value
+
+    def set_dft(self, terms, omega):
+        """terms: iterable of (series, probe, weight); omega: radians per time step."""
+        terms = list(terms)
+        ts = np.array([t[0] for t in terms], dtype=np.int32)
+        tp = np.array([t[1] for t in terms], dtype=np.int32)
+        tw = np.array([t[2] for t in terms], dtype=np.float64)
+        om = np.ascontiguousarray(omega, dtype=np.float64)
+        n_series = int(ts.max()) + 1 if ts.size else 0
+        self._check(self.lib.fdtd_set_dft(self.h, n_series, int(ts.size), _ptr(ts), _ptr(tp), _ptr(tw),
+                                          int(om.size), _ptr(om)))
+        self.n_series, self.n_freq = n_series, int(om.size)
+
+    def compile(self) -> dict:
+        """Build the material table on the host (no GPU needed)."""
+        n = ctypes.c_int()
+        e = ctypes.c_int64()
+        h = ctypes.c_int64()
+        self._check(self.lib.fdtd_compile(self.h, ctypes.byref(n), ctypes.byref(e), ctypes.byref(h)))
+        return dict(n_rows=n.value, e_split_cells=e.value, h_split_cells=h.value)
+
+    def material_table(self):
+        """(ids [nx, ny, nz] uint16, rows [n_rows, 32] uint32) of the compiled table."""
+        info = self.compile()
+        ids = np.empty(self.shape, dtype=np.uint16)
+        rows = np.empty((info["n_rows"], 32), dtype=np.uint32)
+        self._check(self.lib.fdtd_get_material_table(self.h, _ptr(ids), int(ids.size), _ptr(rows),
+                                                     info["n_rows"]))
+        return ids, rows
+
+    def set_stream(self, stream_ptr: int):
+        self._check(self.lib.fdtd_set_stream(self.h, ctypes.c_void_p(int(stream_ptr))))
+
+    def run(self, nt: int):
+        self._check(self.lib.fdtd_run(self.h, int(nt)))
+        self.nt = int(nt)
+
+    def run_async(self, nt: int):
+        self._check(self.lib.fdtd_run_async(self.h, int(nt)))
+        self.nt = int(nt)
+
+    def synchronize(self):
+        self._check(self.lib.fdtd_synchronize(self.h))
+
+    def probe_values(self) -> np.ndarray:
+        out = np.empty((self.n_probes, self.nt), dtype=np.float32)
+        self._check(self.lib.fdtd_get_probe_values(self.h, _ptr(out), self.n_probes, self.nt))
+        return out
+
+    def dft(self) -> np.ndarray:
+        out = np.empty((self.n_series, self.n_freq, 2), dtype=np.float64)
+        self._check(self.lib.fdtd_get_dft(self.h, _ptr(out), self.n_series, self.n_freq))
+        return out[..., 0] + 1j * out[..., 1]
+
+    def monitor(self, m: int) -> np.ndarray:
+        info = self.monitors[m]
+        if info["n_freq"]:
+            out = np.empty((info["n_freq"], info["n1"], info["n2"]), dtype=np.complex64)
+        else:
+            out = np.empty((self.nt // info["n_step"] + 1, info["n1"], info["n2"]), dtype=np.float32)
+        self._check(self.lib.fdtd_get_monitor(self.h, int(m), _ptr(out), int(out.nbytes)))
+        return out
+
+    def stats(self) -> dict:
+        st = FdtdStats()
+        self._check(self.lib.fdtd_get_stats(self.h, ctypes.byref(st)))
+        return st.as_dict()
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.fdtd_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Batch:
+    """Several simulations stepped together by one kernel launch per step."""
+
+    def __init__(self, sims):
+        self.lib = load()
+        self.sims = list(sims)
+        arr = (ctypes.c_void_p * len(self.sims))(*[s.h.value for s in self.sims])
+        h = ctypes.c_void_p()
+        rc = self.lib.fdtd_batch_create(arr, len(self.sims), ctypes.byref(h))
+        if rc:
+            raise ValueError(self.lib.fdtd_global_error().decode())
+        self.h = h
+
+    def run(self, nt: int):
+        rc = self.lib.fdtd_batch_run(self.h, int(nt))
+        if rc:
+            raise FdtdError(f"{FDTD_ERRORS.get(rc, rc)}: {self.lib.fdtd_batch_last_error(self.h).decode()}")
+        for s in self.sims:
+            s.nt = int(nt)
+
+    def set_stream(self, stream_ptr: int):
+        self.lib.fdtd_batch_set_stream(self.h, ctypes.c_void_p(int(stream_ptr)))
+
+    def stats(self) -> dict:
+        st = FdtdStats()
+        self.lib.fdtd_batch_get_stats(self.h, ctypes.byref(st))
+        return st.as_dict()
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.fdtd_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

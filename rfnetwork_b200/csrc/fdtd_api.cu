@@ -1,0 +1,763 @@
+// C ABI and runtime of the B200 FDTD engine (declarations in include/fdtd.h).
+//
+// Replaces SolverFDTD::solver_run_cu (rfnetwork/core/src/solver.cu:546-1143):
+// instead of 48 device arrays and four kernel launches per step on the
+// default stream, each simulation keeps its fields double-buffered in an
+// x-fastest layout, its coefficients as a 16-bit material index plus a row
+// table, and the whole time loop is one kernel launch per step (plus a DFT
+// pass every kDftChunk steps), captured once into a CUDA graph and replayed.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "../../include/fdtd.h"
+#include "fdtd_compile.h"
+#include "fdtd_kernels.cuh"
+
+using namespace rfn;
+
+namespace {
+
+constexpr int kDftChunk = 256;  // steps between DFT accumulation passes
+constexpr int kMaxProbes = 1 << 20;
+constexpr int kMaxMonitors = 50;  // MAX_MONITORS, rfnetwork/core/inc/solver.h:15
+
+std::string g_error;
+
+struct CudaError {
+  cudaError_t code;
+  std::string where;
+};
+
+#define CK(call)                                                   \
+  do {                                                             \
+    cudaError_t e_ = (call);                                       \
+    if (e_ != cudaSuccess) throw CudaError{e_, #call};             \
+  } while (0)
+
+struct ArgError {
+  int code;
+  std::string msg;
+};
+
+template <typename T>
+struct DevBuf {
+  T* p = nullptr;
+  size_t n = 0;
+  void alloc(size_t count) {
+    free();
+    if (count) CK(cudaMalloc(&p, count * sizeof(T)));
+    n = count;
+  }
+  void free() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+  ~DevBuf() { free(); }
+  DevBuf() = default;
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+};
+
+struct Monitor {
+  int field, axis, position, n_step, n_freq;
+  std::vector<float> phase;  // interleaved complex64 rows
+  int n_phase_rows;
+  int n1, n2;
+  size_t out_bytes(int nt) const {
+    const size_t plane = size_t(n1) * n2;
+    return n_freq ? plane * n_freq * 8 : plane * size_t(nt / n_step + 1) * 4;
+  }
+};
+
+int threads_for_host() {
+  unsigned h = std::thread::hardware_concurrency();
+  return int(std::max(1u, std::min(h, 32u)));
+}
+
+}  // namespace
+
+struct Engine;
+
+struct fdtd_sim {
+  int nx, ny, nz;
+  std::vector<float> coef[kNumCoef];
+  bool have_coef[kNumCoef] = {};
+  std::vector<ProbeSpec> probes;
+  std::vector<std::vector<float>> probe_values;
+  std::vector<Monitor> monitors;
+  // DFT specification
+  int n_series = 0, n_freq = 0;
+  std::vector<int> series_start, term_probe;
+  std::vector<double> term_weight, omega;
+
+  // device state (valid when prepared)
+  bool compiled = false;
+  bool prepared = false;
+  int prepared_nt = -1;
+  int pitch = 0;
+  size_t cells_padded = 0;
+  CompiledGrid grid;
+  DevBuf<float> fields;        // 2 x 6 field arrays
+  DevBuf<float> splits;        // 2 x 12 split arrays (only when split cells exist)
+  DevBuf<uint16_t> mat;
+  DevBuf<float4> rows;
+  DevBuf<int2> cell_probes;
+  DevBuf<float> src, rec;
+  DevBuf<int> is_src;
+  DevBuf<int> d_series_start, d_term_probe;
+  DevBuf<double> d_term_weight, d_omega;
+  DevBuf<double2> dft_X;
+  DevBuf<MonDev> d_mons;
+  std::vector<std::unique_ptr<DevBuf<char>>> mon_out;
+  std::vector<std::unique_ptr<DevBuf<float2>>> mon_phase;
+  SimDev dev{};
+  DevBuf<SimDev> d_dev;  // this simulation's descriptor alone (monitor kernel)
+
+  std::unique_ptr<Engine> engine;  // batch of one for fdtd_run
+  cudaStream_t ext_stream = nullptr;
+  std::string err;
+  fdtd_stats stats{};
+};
+
+struct Engine {
+  std::vector<fdtd_sim*> sims;
+  DevBuf<SimDev> d_sims;
+  DevBuf<int4> d_tiles;
+  int n_tiles = 0;
+  cudaStream_t own_stream = nullptr;
+  cudaStream_t ext_stream = nullptr;
+  cudaGraphExec_t graph = nullptr;
+  int graph_nt = -1;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  int64_t step_launches = 0, dft_launches = 0;
+  double last_ms = 0;
+  bool timing_pending = false;
+
+  cudaStream_t stream() const { return ext_stream ? ext_stream : own_stream; }
+
+  void init() {
+    if (!own_stream) CK(cudaStreamCreateWithFlags(&own_stream, cudaStreamNonBlocking));
+    if (!ev0) CK(cudaEventCreate(&ev0));
+    if (!ev1) CK(cudaEventCreate(&ev1));
+  }
+  ~Engine() {
+    if (graph) cudaGraphExecDestroy(graph);
+    if (ev0) cudaEventDestroy(ev0);
+    if (ev1) cudaEventDestroy(ev1);
+    if (own_stream) cudaStreamDestroy(own_stream);
+  }
+
+  void build_tiles() {
+    std::vector<int4> tiles;
+    std::vector<SimDev> devs;
+    // xy tiles of all simulations first, then cut z into chunks so one step
+    // has enough blocks to fill 148 SMs several times over.
+    int64_t xy_tiles = 0;
+    for (auto* s : sims) xy_tiles += int64_t((s->nx + kTileX - 1) / kTileX) * ((s->ny + kTileY - 1) / kTileY);
+    int dev = 0, n_sm = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
+    const int64_t want = int64_t(n_sm) * 8;
+    for (size_t i = 0; i < sims.size(); ++i) {
+      fdtd_sim* s = sims[i];
+      devs.push_back(s->dev);
+      int chunks = int(std::max<int64_t>(1, (want + xy_tiles - 1) / std::max<int64_t>(xy_tiles, 1)));
+      chunks = std::min(chunks, std::max(1, s->nz / 8));
+      const int zlen = (s->nz + chunks - 1) / chunks;
+      for (int z0 = 0; z0 < s->nz; z0 += zlen)
+        for (int y0 = 0; y0 < s->ny; y0 += kTileY)
+          for (int x0 = 0; x0 < s->nx; x0 += kTileX) {
+            const int z1 = std::min(s->nz, z0 + zlen);
+            tiles.push_back(make_int4(int(i), x0 | (y0 << 16), z0 | (z1 << 16), 0));
+          }
+    }
+    d_sims.alloc(devs.size());
+    CK(cudaMemcpy(d_sims.p, devs.data(), devs.size() * sizeof(SimDev), cudaMemcpyHostToDevice));
+    d_tiles.alloc(tiles.size());
+    CK(cudaMemcpy(d_tiles.p, tiles.data(), tiles.size() * sizeof(int4), cudaMemcpyHostToDevice));
+    n_tiles = int(tiles.size());
+  }
+
+  // Enqueue one full run of nt steps on stream st (used for capture and for
+  // direct launches alike).
+  void enqueue(cudaStream_t st, int nt) {
+    step_launches = dft_launches = 0;
+    for (auto* s : sims) {
+      CK(cudaMemsetAsync(s->fields.p, 0, s->fields.n * sizeof(float), st));
+      if (s->splits.n) CK(cudaMemsetAsync(s->splits.p, 0, s->splits.n * sizeof(float), st));
+      if (s->dft_X.n) CK(cudaMemsetAsync(s->dft_X.p, 0, s->dft_X.n * sizeof(double2), st));
+      for (size_t m = 0; m < s->monitors.size(); ++m)
+        CK(cudaMemsetAsync(s->mon_out[m]->p, 0, s->mon_out[m]->n, st));
+    }
+    const dim3 block(32, kBlockY);
+    int dft_from = 0;
+    for (int n = 0; n < nt; ++n) {
+      fdtd_step_kernel<kTileY><<<n_tiles, block, 0, st>>>(d_sims.p, d_tiles.p, n);
+      CK(cudaGetLastError());
+      ++step_launches;
+      for (auto* s : sims)
+        if (!s->monitors.empty()) {
+          monitor_kernel<<<64, 256, 0, st>>>(s->d_dev.p, s->d_mons.p, int(s->monitors.size()), n, (n + 1) & 1);
+          CK(cudaGetLastError());
+        }
+      if ((n + 1) % kDftChunk == 0 || n + 1 == nt) {
+        for (auto* s : sims)
+          if (s->n_series > 0 && s->n_freq > 0) {
+            DftDev d{s->n_series, s->n_freq, nt, s->d_series_start.p, s->d_term_probe.p, s->d_term_weight.p,
+                     s->d_omega.p, s->rec.p, s->dft_X.p};
+            dft_accumulate_kernel<<<dim3(s->n_freq, s->n_series), 256, 0, st>>>(d, dft_from, n + 1);
+            CK(cudaGetLastError());
+            ++dft_launches;
+          }
+        dft_from = n + 1;
+      }
+    }
+  }
+
+  void run_async(int nt) {
+    init();
+    cudaStream_t st = stream();
+    if (graph_nt != nt) {
+      if (graph) {
+        cudaGraphExecDestroy(graph);
+        graph = nullptr;
+      }
+      cudaStream_t cap;
+      CK(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
+      cudaGraph_t g = nullptr;
+      try {
+        CK(cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal));
+        enqueue(cap, nt);
+        CK(cudaStreamEndCapture(cap, &g));
+        CK(cudaGraphInstantiate(&graph, g, 0));
+      } catch (...) {
+        cudaGraph_t dummy;
+        cudaStreamEndCapture(cap, &dummy);
+        if (dummy) cudaGraphDestroy(dummy);
+        if (g) cudaGraphDestroy(g);
+        cudaStreamDestroy(cap);
+        throw;
+      }
+      cudaGraphDestroy(g);
+      cudaStreamDestroy(cap);
+      graph_nt = nt;
+    }
+    CK(cudaEventRecord(ev0, st));
+    CK(cudaGraphLaunch(graph, st));
+    CK(cudaEventRecord(ev1, st));
+    timing_pending = true;
+  }
+
+  void sync() {
+    CK(cudaStreamSynchronize(stream()));
+    if (timing_pending) {
+      float ms = 0;
+      CK(cudaEventElapsedTime(&ms, ev0, ev1));
+      last_ms = ms;
+      timing_pending = false;
+    }
+  }
+};
+
+namespace {
+
+void compile_host(fdtd_sim* s) {
+  if (s->compiled) return;
+  for (int i = 0; i < kNumCoef; ++i)
+    if (!s->have_coef[i]) throw ArgError{FDTD_ERR_STATE, std::string("Coefficient not set: ") + kCoefNames[i]};
+  const float* cp[kNumCoef];
+  for (int i = 0; i < kNumCoef; ++i) cp[i] = s->coef[i].data();
+  std::string err;
+  if (!compile_grid(s->nx, s->ny, s->nz, cp, s->probes, threads_for_host(), s->grid, err))
+    throw ArgError{FDTD_ERR_LIMIT, err};
+  s->compiled = true;
+}
+
+void prepare(fdtd_sim* s, int nt) {
+  if (s->prepared && s->prepared_nt == nt) return;
+  for (size_t p = 0; p < s->probe_values.size(); ++p)
+    if (s->probes[p].is_source && int(s->probe_values[p].size()) < nt)
+      throw ArgError{FDTD_ERR_ARG, "Invalid data source array shape. Expected shape greater or equal to " +
+                                       std::to_string(nt)};
+  const int nx = s->nx, ny = s->ny, nz = s->nz;
+  if (!s->prepared) {
+    compile_host(s);
+    s->pitch = ((nx + 31) / 32) * 32;
+    s->cells_padded = size_t(nz) * ny * s->pitch;
+    if (s->cells_padded >= (size_t(1) << 31) - size_t(2) * ny * s->pitch)
+      throw ArgError{FDTD_ERR_LIMIT, "Grid too large for 32-bit cell offsets."};
+    const size_t N = s->cells_padded;
+    s->fields.alloc(12 * N);
+    const bool any_split = s->grid.e_split_cells > 0 || s->grid.h_split_cells > 0;
+    s->splits.alloc(any_split ? 24 * N : 0);
+    // material index: upload in reference order, transpose on the device
+    {
+      DevBuf<uint16_t> tmp;
+      tmp.alloc(s->grid.ids.size());
+      CK(cudaMemcpy(tmp.p, s->grid.ids.data(), s->grid.ids.size() * 2, cudaMemcpyHostToDevice));
+      s->mat.alloc(N);
+      CK(cudaMemset(s->mat.p, 0, N * 2));
+      transpose_ids_kernel<<<1024, 256>>>(tmp.p, s->mat.p, nx, ny, nz, s->pitch);
+      CK(cudaGetLastError());
+      CK(cudaDeviceSynchronize());
+    }
+    s->rows.alloc(s->grid.rows.size() * 8);
+    CK(cudaMemcpy(s->rows.p, s->grid.rows.data(), s->grid.rows.size() * sizeof(Row), cudaMemcpyHostToDevice));
+    s->cell_probes.alloc(std::max<size_t>(1, s->grid.cell_probes.size()));
+    if (!s->grid.cell_probes.empty())
+      CK(cudaMemcpy(s->cell_probes.p, s->grid.cell_probes.data(), s->grid.cell_probes.size() * sizeof(int2),
+                    cudaMemcpyHostToDevice));
+    std::vector<int> srcflag(std::max<size_t>(1, s->probes.size()), 0);
+    for (size_t p = 0; p < s->probes.size(); ++p) srcflag[p] = s->probes[p].is_source;
+    s->is_src.alloc(srcflag.size());
+    CK(cudaMemcpy(s->is_src.p, srcflag.data(), srcflag.size() * sizeof(int), cudaMemcpyHostToDevice));
+    s->prepared = true;
+  }
+  // per-nt buffers: source amplitudes, records, DFT, monitors
+  const size_t P = s->probes.size();
+  s->src.alloc(std::max<size_t>(1, P * size_t(nt)));
+  s->rec.alloc(std::max<size_t>(1, P * size_t(nt)));
+  {
+    std::vector<float> host(std::max<size_t>(1, P * size_t(nt)), 0.f);
+    for (size_t p = 0; p < P; ++p)
+      if (s->probes[p].is_source)
+        std::memcpy(&host[p * nt], s->probe_values[p].data(), size_t(nt) * sizeof(float));
+    CK(cudaMemcpy(s->src.p, host.data(), host.size() * sizeof(float), cudaMemcpyHostToDevice));
+  }
+  if (s->n_series > 0) {
+    s->d_series_start.alloc(s->series_start.size());
+    CK(cudaMemcpy(s->d_series_start.p, s->series_start.data(), s->series_start.size() * 4, cudaMemcpyHostToDevice));
+    s->d_term_probe.alloc(std::max<size_t>(1, s->term_probe.size()));
+    if (!s->term_probe.empty())
+      CK(cudaMemcpy(s->d_term_probe.p, s->term_probe.data(), s->term_probe.size() * 4, cudaMemcpyHostToDevice));
+    s->d_term_weight.alloc(std::max<size_t>(1, s->term_weight.size()));
+    if (!s->term_weight.empty())
+      CK(cudaMemcpy(s->d_term_weight.p, s->term_weight.data(), s->term_weight.size() * 8, cudaMemcpyHostToDevice));
+    s->d_omega.alloc(s->omega.size());
+    CK(cudaMemcpy(s->d_omega.p, s->omega.data(), s->omega.size() * 8, cudaMemcpyHostToDevice));
+    s->dft_X.alloc(size_t(s->n_series) * s->n_freq);
+  }
+  std::vector<MonDev> mdev;
+  s->mon_out.clear();
+  s->mon_phase.clear();
+  for (auto& m : s->monitors) {
+    if (m.n_freq && m.n_phase_rows < nt / m.n_step + 1)
+      throw ArgError{FDTD_ERR_ARG, "Monitor phase table has fewer rows than nt/n_step + 1."};
+    auto out = std::make_unique<DevBuf<char>>();
+    out->alloc(m.out_bytes(nt));
+    auto ph = std::make_unique<DevBuf<float2>>();
+    if (m.n_freq) {
+      ph->alloc(m.phase.size() / 2);
+      CK(cudaMemcpy(ph->p, m.phase.data(), m.phase.size() * 4, cudaMemcpyHostToDevice));
+    }
+    mdev.push_back(MonDev{m.field, m.axis, m.position, m.n_step, m.n_freq, m.n1, m.n2, out->p, ph->p});
+    s->mon_out.push_back(std::move(out));
+    s->mon_phase.push_back(std::move(ph));
+  }
+  s->d_mons.alloc(mdev.size());
+  if (!mdev.empty())
+    CK(cudaMemcpy(s->d_mons.p, mdev.data(), mdev.size() * sizeof(MonDev), cudaMemcpyHostToDevice));
+
+  // descriptor
+  SimDev& d = s->dev;
+  const size_t N = s->cells_padded;
+  d.nx = nx; d.ny = ny; d.nz = nz; d.pitch = s->pitch; d.plane = ny * s->pitch; d.nt = nt;
+  for (int b = 0; b < 2; ++b) {
+    for (int c = 0; c < 3; ++c) {
+      d.E[b][c] = s->fields.p + (size_t(b) * 6 + c) * N;
+      d.H[b][c] = s->fields.p + (size_t(b) * 6 + 3 + c) * N;
+    }
+    for (int c = 0; c < 6; ++c) {
+      d.Es[b][c] = s->splits.n ? s->splits.p + (size_t(b) * 12 + c) * N : nullptr;
+      d.Hs[b][c] = s->splits.n ? s->splits.p + (size_t(b) * 12 + 6 + c) * N : nullptr;
+    }
+  }
+  d.mat = s->mat.p;
+  d.rows = s->rows.p;
+  d.cell_probes = s->cell_probes.p;
+  d.src = s->src.p;
+  d.rec = s->rec.p;
+  d.is_src = s->is_src.p;
+  s->d_dev.alloc(1);
+  CK(cudaMemcpy(s->d_dev.p, &d, sizeof(SimDev), cudaMemcpyHostToDevice));
+  s->prepared_nt = nt;
+}
+
+void fill_stats(fdtd_sim* s, const Engine* e) {
+  fdtd_stats& st = s->stats;
+  st.nx = s->nx; st.ny = s->ny; st.nz = s->nz; st.nt = s->prepared_nt;
+  st.n_rows = int(s->grid.rows.size());
+  st.id_bytes = 2;
+  st.e_split_cells = s->grid.e_split_cells;
+  st.h_split_cells = s->grid.h_split_cells;
+  st.compile_ms = s->grid.compile_ms;
+  if (e) {
+    st.n_tiles = e->n_tiles;
+    st.step_launches = e->step_launches;
+    st.dft_launches = e->dft_launches;
+    st.last_run_ms = e->last_ms;
+  }
+}
+
+template <typename F>
+int guarded(std::string* err, F&& f) {
+  try {
+    f();
+    return FDTD_OK;
+  } catch (const ArgError& a) {
+    if (err) *err = a.msg;
+    return a.code;
+  } catch (const CudaError& c) {
+    if (err) *err = c.where + ": " + cudaGetErrorString(c.code);
+    return FDTD_ERR_CUDA;
+  } catch (const std::bad_alloc&) {
+    if (err) *err = "host allocation failed";
+    return FDTD_ERR_LIMIT;
+  } catch (const std::exception& e) {
+    if (err) *err = e.what();
+    return FDTD_ERR_ARG;
+  }
+}
+
+int coef_index(const char* name) {
+  for (int i = 0; i < kNumCoef; ++i)
+    if (std::strcmp(name, kCoefNames[i]) == 0) return i;
+  return -1;
+}
+
+}  // namespace
+
+struct fdtd_batch {
+  std::vector<fdtd_sim*> sims;
+  Engine engine;
+  std::string err;
+  fdtd_stats stats{};
+};
+
+extern "C" {
+
+int fdtd_create(int nx, int ny, int nz, fdtd_sim** out) {
+  if (!out) {
+    g_error = "fdtd_create: null output pointer";
+    return FDTD_ERR_ARG;
+  }
+  *out = nullptr;
+  if (nx < 2 || ny < 2 || nz < 2 || nx > 65535 || ny > 65535 || nz > 65535) {
+    g_error = "Grid dimensions must be between 2 and 65535 cells.";
+    return FDTD_ERR_ARG;
+  }
+  auto* s = new (std::nothrow) fdtd_sim();
+  if (!s) {
+    g_error = "host allocation failed";
+    return FDTD_ERR_LIMIT;
+  }
+  s->nx = nx;
+  s->ny = ny;
+  s->nz = nz;
+  *out = s;
+  return FDTD_OK;
+}
+
+int fdtd_set_coefficient(fdtd_sim* s, const char* name, const float* data, int nx, int ny, int nz) {
+  if (!s) return FDTD_ERR_ARG;
+  return guarded(&s->err, [&] {
+    const int i = name ? coef_index(name) : -1;
+    if (i < 0) throw ArgError{FDTD_ERR_ARG, std::string("Unknown coefficient array ") + (name ? name : "(null)")};
+    const int expect[3] = {s->nx, s->ny, s->nz}, got[3] = {nx, ny, nz};
+    for (int a = 0; a < 3; ++a)
+      if (expect[a] != got[a])
+        throw ArgError{FDTD_ERR_ARG, std::string("Invalid data array ") + name + ". Expected shape on axis " +
+                                         std::to_string(a) + " of " + std::to_string(expect[a])};
+    if (!data) throw ArgError{FDTD_ERR_ARG, "null coefficient data"};
+    s->coef[i].assign(data, data + size_t(nx) * ny * nz);
+    s->have_coef[i] = true;
+    s->prepared = false;
+    s->compiled = false;
+  });
+}
+
+int fdtd_add_probe(fdtd_sim* s, int field, int i, int j, int k, int is_source, const float* values, int n_values,
+                   int* index) {
+  if (!s) return FDTD_ERR_ARG;
+  return guarded(&s->err, [&] {
+    if (field < 0 || field > 5) throw ArgError{FDTD_ERR_ARG, "Invalid probe field type."};
+    if (int(s->probes.size()) >= kMaxProbes) throw ArgError{FDTD_ERR_LIMIT, "Exceeded maximum number of probes."};
+    if (is_source && (!values || n_values < 0)) throw ArgError{FDTD_ERR_ARG, "Source probe needs values."};
+    s->probes.push_back(ProbeSpec{field, i, j, k, is_source ? 1 : 0});
+    s->probe_values.emplace_back();
+    if (values && n_values > 0) s->probe_values.back().assign(values, values + n_values);
+    if (index) *index = int(s->probes.size()) - 1;
+    s->prepared = false;
+    s->compiled = false;
+  });
+}
+
+int fdtd_add_monitor(fdtd_sim* s, int field, int axis, int position, int n_step, int n_freq, const float* phase,
+                     int n_phase_rows, int* index) {
+  if (!s) return FDTD_ERR_ARG;
+  return guarded(&s->err, [&] {
+    if (int(s->monitors.size()) >= kMaxMonitors)
+      throw ArgError{FDTD_ERR_LIMIT, "Exceeded maximum number of monitors."};
+    if (field < 0 || field > 5 || axis < 0 || axis > 2 || n_step < 1 || n_freq < 0)
+      throw ArgError{FDTD_ERR_ARG, "Invalid monitor field, axis, n_step or n_frequencies."};
+    Monitor m{};
+    m.field = field;
+    m.axis = axis;
+    m.n_step = n_step;
+    m.n_freq = n_freq;
+    // GPU-layout position shift of solver_init_monitors (solver.cpp:394-441, gpu = 1)
+    int pos = position;
+    if (axis == 0 && (field == 3 || field == 1 || field == 2)) pos -= 1;
+    if (axis == 1 && (field == 4 || field == 0 || field == 2)) pos -= 1;
+    if (axis == 2 && (field == 5 || field == 0 || field == 1)) pos -= 1;
+    m.position = pos;
+    m.n1 = axis == 0 ? s->ny : s->nx;
+    m.n2 = axis == 2 ? s->ny : s->nz;
+    if (n_freq) {
+      if (!phase || n_phase_rows < 1) throw ArgError{FDTD_ERR_ARG, "Phasor monitor needs a dtft_phase table."};
+      m.phase.assign(phase, phase + size_t(n_phase_rows) * n_freq * 2);
+      m.n_phase_rows = n_phase_rows;
+    }
+    s->monitors.push_back(std::move(m));
+    if (index) *index = int(s->monitors.size()) - 1;
+    s->prepared_nt = -1;
+  });
+}
+
+int fdtd_set_dft(fdtd_sim* s, int n_series, int n_terms, const int* term_series, const int* term_probe,
+                 const double* term_weight, int n_freq, const double* omega) {
+  if (!s) return FDTD_ERR_ARG;
+  return guarded(&s->err, [&] {
+    if (n_series < 0 || n_terms < 0 || n_freq < 0) throw ArgError{FDTD_ERR_ARG, "Negative DFT size."};
+    if (n_series > 0 && n_freq > 0 && (!omega || (n_terms > 0 && (!term_series || !term_probe || !term_weight))))
+      throw ArgError{FDTD_ERR_ARG, "null DFT array"};
+    std::vector<std::vector<std::pair<int, double>>> per(n_series);
+    for (int t = 0; t < n_terms; ++t) {
+      if (term_series[t] < 0 || term_series[t] >= n_series)
+        throw ArgError{FDTD_ERR_ARG, "DFT term refers to a series out of range."};
+      if (term_probe[t] < 0 || term_probe[t] >= int(s->probes.size()))
+        throw ArgError{FDTD_ERR_ARG, "DFT term refers to a probe out of range (add probes first)."};
+      per[term_series[t]].emplace_back(term_probe[t], term_weight[t]);
+    }
+    s->n_series = n_series;
+    s->n_freq = n_freq;
+    s->series_start.assign(1, 0);
+    s->term_probe.clear();
+    s->term_weight.clear();
+    for (auto& v : per) {
+      for (auto& pw : v) {
+        s->term_probe.push_back(pw.first);
+        s->term_weight.push_back(pw.second);
+      }
+      s->series_start.push_back(int(s->term_probe.size()));
+    }
+    s->omega.assign(omega, omega + n_freq);
+    s->prepared_nt = -1;
+  });
+}
+
+int fdtd_compile(fdtd_sim* s, int* n_rows, int64_t* e_split_cells, int64_t* h_split_cells) {
+  if (!s) return FDTD_ERR_ARG;
+  return guarded(&s->err, [&] {
+    compile_host(s);
+    if (n_rows) *n_rows = int(s->grid.rows.size());
+    if (e_split_cells) *e_split_cells = s->grid.e_split_cells;
+    if (h_split_cells) *h_split_cells = s->grid.h_split_cells;
+  });
+}
+
+int fdtd_get_material_table(fdtd_sim* s, uint16_t* ids, int64_t n_ids, uint32_t* rows, int n_rows) {
+  if (!s) return FDTD_ERR_ARG;
+  return guarded(&s->err, [&] {
+    if (!s->compiled) throw ArgError{FDTD_ERR_STATE, "Material table not compiled."};
+    if (ids) {
+      if (size_t(n_ids) != s->grid.ids.size()) throw ArgError{FDTD_ERR_ARG, "ids size mismatch."};
+      std::memcpy(ids, s->grid.ids.data(), s->grid.ids.size() * 2);
+    }
+    if (rows) {
+      if (size_t(n_rows) != s->grid.rows.size()) throw ArgError{FDTD_ERR_ARG, "rows size mismatch."};
+      std::memcpy(rows, s->grid.rows.data(), s->grid.rows.size() * sizeof(Row));
+    }
+  });
+}
+
+int fdtd_set_stream(fdtd_sim* s, void* stream) {
+  if (!s) return FDTD_ERR_ARG;
+  s->ext_stream = static_cast<cudaStream_t>(stream);
+  if (s->engine) s->engine->ext_stream = s->ext_stream;
+  return FDTD_OK;
+}
+
+int fdtd_run_async(fdtd_sim* s, int nt) {
+  if (!s) return FDTD_ERR_ARG;
+  return guarded(&s->err, [&] {
+    if (nt < 1) throw ArgError{FDTD_ERR_ARG, "nt must be positive."};
+    const bool rebuild = !s->prepared || s->prepared_nt != nt || !s->engine;
+    prepare(s, nt);
+    if (rebuild) {
+      s->engine = std::make_unique<Engine>();
+      s->engine->sims = {s};
+      s->engine->ext_stream = s->ext_stream;
+      s->engine->build_tiles();
+    }
+    s->engine->run_async(nt);
+    fill_stats(s, s->engine.get());
+  });
+}
+
+int fdtd_synchronize(fdtd_sim* s) {
+  if (!s) return FDTD_ERR_ARG;
+  return guarded(&s->err, [&] {
+    if (!s->engine) throw ArgError{FDTD_ERR_STATE, "No run in flight."};
+    s->engine->sync();
+    fill_stats(s, s->engine.get());
+  });
+}
+
+int fdtd_run(fdtd_sim* s, int nt) {
+  int rc = fdtd_run_async(s, nt);
+  if (rc) return rc;
+  return fdtd_synchronize(s);
+}
+
+int fdtd_get_probe_values(fdtd_sim* s, float* out, int n_probes, int nt) {
+  if (!s) return FDTD_ERR_ARG;
+  return guarded(&s->err, [&] {
+    if (!s->prepared || s->prepared_nt < 0) throw ArgError{FDTD_ERR_STATE, "No completed run."};
+    if (n_probes != int(s->probes.size()) || nt != s->prepared_nt)
+      throw ArgError{FDTD_ERR_ARG, "Probe output size does not match the last run."};
+    if (n_probes == 0) return;
+    CK(cudaMemcpy(out, s->rec.p, size_t(n_probes) * nt * sizeof(float), cudaMemcpyDeviceToHost));
+  });
+}
+
+int fdtd_get_dft(fdtd_sim* s, double* out, int n_series, int n_freq) {
+  if (!s) return FDTD_ERR_ARG;
+  return guarded(&s->err, [&] {
+    if (n_series != s->n_series || n_freq != s->n_freq) throw ArgError{FDTD_ERR_ARG, "DFT size mismatch."};
+    if (!s->dft_X.n) throw ArgError{FDTD_ERR_STATE, "No DFT configured."};
+    CK(cudaMemcpy(out, s->dft_X.p, s->dft_X.n * sizeof(double2), cudaMemcpyDeviceToHost));
+  });
+}
+
+int fdtd_get_monitor(fdtd_sim* s, int m, void* out, int64_t n_bytes) {
+  if (!s) return FDTD_ERR_ARG;
+  return guarded(&s->err, [&] {
+    if (m < 0 || m >= int(s->mon_out.size())) throw ArgError{FDTD_ERR_ARG, "Monitor index out of range."};
+    if (size_t(n_bytes) != s->mon_out[m]->n) throw ArgError{FDTD_ERR_ARG, "Monitor output size mismatch."};
+    CK(cudaMemcpy(out, s->mon_out[m]->p, size_t(n_bytes), cudaMemcpyDeviceToHost));
+  });
+}
+
+int fdtd_get_stats(const fdtd_sim* s, fdtd_stats* out) {
+  if (!s || !out) return FDTD_ERR_ARG;
+  *out = s->stats;
+  return FDTD_OK;
+}
+
+const char* fdtd_last_error(const fdtd_sim* s) { return s ? s->err.c_str() : g_error.c_str(); }
+
+void fdtd_destroy(fdtd_sim* s) {
+  if (!s) return;
+  if (s->engine) {
+    cudaStreamSynchronize(s->engine->stream());
+    s->engine.reset();
+  }
+  delete s;
+}
+
+int fdtd_batch_create(fdtd_sim* const* sims, int n_sims, fdtd_batch** out) {
+  if (!out || !sims || n_sims < 1) {
+    g_error = "fdtd_batch_create: invalid arguments";
+    return FDTD_ERR_ARG;
+  }
+  *out = nullptr;
+  auto* b = new (std::nothrow) fdtd_batch();
+  if (!b) {
+    g_error = "host allocation failed";
+    return FDTD_ERR_LIMIT;
+  }
+  for (int i = 0; i < n_sims; ++i) {
+    if (!sims[i]) {
+      delete b;
+      g_error = "fdtd_batch_create: null simulation";
+      return FDTD_ERR_ARG;
+    }
+    b->sims.push_back(sims[i]);
+  }
+  b->engine.sims = b->sims;
+  *out = b;
+  return FDTD_OK;
+}
+
+int fdtd_batch_set_stream(fdtd_batch* b, void* stream) {
+  if (!b) return FDTD_ERR_ARG;
+  b->engine.ext_stream = static_cast<cudaStream_t>(stream);
+  return FDTD_OK;
+}
+
+int fdtd_batch_run(fdtd_batch* b, int nt) {
+  if (!b) return FDTD_ERR_ARG;
+  return guarded(&b->err, [&] {
+    if (nt < 1) throw ArgError{FDTD_ERR_ARG, "nt must be positive."};
+    bool rebuild = b->engine.graph_nt != nt || b->engine.n_tiles == 0;
+    for (auto* s : b->sims) {
+      if (!s->prepared || s->prepared_nt != nt) rebuild = true;
+      try {
+        prepare(s, nt);
+      } catch (ArgError& a) {
+        a.msg = "batch member: " + a.msg;
+        throw;
+      }
+    }
+    if (rebuild) {
+      b->engine.graph_nt = -1;
+      b->engine.build_tiles();
+    }
+    b->engine.run_async(nt);
+    b->engine.sync();
+    for (auto* s : b->sims) fill_stats(s, &b->engine);
+    fdtd_stats& st = b->stats;
+    st = fdtd_stats{};
+    st.nt = nt;
+    st.n_tiles = b->engine.n_tiles;
+    st.step_launches = b->engine.step_launches;
+    st.dft_launches = b->engine.dft_launches;
+    st.last_run_ms = b->engine.last_ms;
+    for (auto* s : b->sims) {
+      st.e_split_cells += s->grid.e_split_cells;
+      st.h_split_cells += s->grid.h_split_cells;
+      st.n_rows += int(s->grid.rows.size());
+      st.compile_ms += s->grid.compile_ms;
+    }
+    st.id_bytes = 2;
+  });
+}
+
+int fdtd_batch_get_stats(const fdtd_batch* b, fdtd_stats* out) {
+  if (!b || !out) return FDTD_ERR_ARG;
+  *out = b->stats;
+  return FDTD_OK;
+}
+
+const char* fdtd_batch_last_error(const fdtd_batch* b) { return b ? b->err.c_str() : g_error.c_str(); }
+
+void fdtd_batch_destroy(fdtd_batch* b) {
+  if (!b) return;
+  cudaStreamSynchronize(b->engine.stream());
+  delete b;
+}
+
+const char* fdtd_global_error(void) { return g_error.c_str(); }
+
+}  // extern "C"

@@ -1,0 +1,265 @@
+// Host-side compilation of per-component coefficient arrays into a material
+// index + coefficient-row table (see fdtd_compile.h).
+//
+// The reference CUDA engine reads 30 float arrays per cell and step
+// (rfnetwork/core/src/solver.cu:116-437). Almost all cells share a handful of
+// distinct coefficient tuples, so the engine stores one 16-bit row index per
+// cell instead, and the kernels fetch the row from a table. Compilation folds
+// three reference behaviours into the rows so the kernels need no special
+// cases:
+//  1. the x-max PEC wall: solver_init_fields zeroes the last x plane of the
+//     Cy, Cz and Dx arrays (rfnetwork/core/src/solver.cpp:294-328);
+//  2. the update guards of efield_update_kernel (solver.cu:152-185): a split
+//     on the y-max / z-max / x-max boundary is not updated, i.e. keeps its
+//     value. A split that is never updated and never receives a source stays
+//     exactly zero, so it can take its partner split's Ca with Cb = 0 without
+//     changing any result; only a guarded split carrying a source keeps the
+//     literal (Ca = 1, Cb = 0) "keep" row;
+//  3. split-field storage: a cell whose two splits of some component have
+//     different Ca (E) or Da (H) -- the PML slabs -- or that carries a soft
+//     source, is flagged for split storage. Every other cell is advanced in
+//     unsplit form, f' = Ca f + Cb1 d1 + Cb2 d2, which is the same algebra.
+#include "fdtd_compile.h"
+
+#include <algorithm>
+#include <chrono>
+#include <cstring>
+#include <thread>
+#include <unordered_map>
+
+namespace rfn {
+
+const char* const kCoefNames[kNumCoef] = {
+    "Ca_ex_y", "Ca_ex_z", "Cb_ex_y", "Cb_ex_z", "Ca_ey_z", "Ca_ey_x", "Cb_ey_z", "Cb_ey_x",
+    "Ca_ez_x", "Ca_ez_y", "Cb_ez_x", "Cb_ez_y", "Da_hx_y", "Da_hx_z", "Db_hx_y1", "Db_hx_y2",
+    "Db_hx_z1", "Db_hx_z2", "Da_hy_z", "Da_hy_x", "Db_hy_z1", "Db_hy_z2", "Db_hy_x1", "Db_hy_x2",
+    "Da_hz_x", "Da_hz_y", "Db_hz_x1", "Db_hz_x2", "Db_hz_y1", "Db_hz_y2"};
+
+namespace {
+
+// kCoefNames index -> row slot.
+constexpr int kSlotOf[kNumCoef] = {
+    R_CA_EX_Y, R_CA_EX_Z, R_CB_EX_Y, R_CB_EX_Z, R_CA_EY_Z, R_CA_EY_X, R_CB_EY_Z, R_CB_EY_X,
+    R_CA_EZ_X, R_CA_EZ_Y, R_CB_EZ_X, R_CB_EZ_Y, R_DA_HX_Y, R_DA_HX_Z, R_DB1_HX_Y, R_DB2_HX_Y,
+    R_DB1_HX_Z, R_DB2_HX_Z, R_DA_HY_Z, R_DA_HY_X, R_DB1_HY_Z, R_DB2_HY_Z, R_DB1_HY_X, R_DB2_HY_X,
+    R_DA_HZ_X, R_DA_HZ_Y, R_DB1_HZ_X, R_DB2_HZ_X, R_DB1_HZ_Y, R_DB2_HZ_Y};
+
+inline uint32_t fbits(float f) {
+  uint32_t u;
+  std::memcpy(&u, &f, 4);
+  return u;
+}
+
+struct RowHash {
+  size_t operator()(const Row& r) const {
+    uint64_t h = 0x9E3779B97F4A7C15ull;
+    for (int i = 0; i < kRowWords; ++i) {
+      h ^= r.w[i] + 0x9E3779B97F4A7C15ull + (h << 6) + (h >> 2);
+      h *= 0xBF58476D1CE4E5B9ull;
+    }
+    return size_t(h ^ (h >> 31));
+  }
+};
+struct RowEq {
+  bool operator()(const Row& a, const Row& b) const { return std::memcmp(a.w, b.w, sizeof(a.w)) == 0; }
+};
+using RowMap = std::unordered_map<Row, uint32_t, RowHash, RowEq>;
+
+}  // namespace
+
+float row_coefficient(const Row& r, int c) {
+  float f;
+  std::memcpy(&f, &r.w[kSlotOf[c]], 4);
+  return f;
+}
+
+bool compile_grid(int nx, int ny, int nz, const float* const* coef, const std::vector<ProbeSpec>& probes,
+                  int n_threads, CompiledGrid& out, std::string& err) {
+  auto t0 = std::chrono::steady_clock::now();
+  if (nx < 2 || ny < 2 || nz < 2) {
+    err = "Grid must have at least 2 cells along each axis.";
+    return false;
+  }
+  for (int i = 0; i < kNumCoef; ++i)
+    if (!coef[i]) {
+      err = std::string("Missing coefficient array ") + kCoefNames[i];
+      return false;
+    }
+  const int64_t ncell = int64_t(nx) * ny * nz;
+  out = CompiledGrid();
+  out.nx = nx;
+  out.ny = ny;
+  out.nz = nz;
+
+  // ---- probes: Yee shift and per-cell grouping (solver.cpp:503-525)
+  std::vector<std::pair<int64_t, int>> by_cell;  // (cell, probe)
+  out.probe_cell.resize(probes.size());
+  for (size_t p = 0; p < probes.size(); ++p) {
+    const ProbeSpec& q = probes[p];
+    if (q.field < 0 || q.field > 5) {
+      err = "Invalid probe field type.";
+      return false;
+    }
+    int x = q.i, y = q.j, z = q.k;
+    if (q.field == 1 || q.field == 2 || q.field == 3) x -= 1;
+    if (q.field == 0 || q.field == 2 || q.field == 4) y -= 1;
+    if (q.field == 0 || q.field == 1 || q.field == 5) z -= 1;
+    if (x < 0 || y < 0 || z < 0) {
+      err = "Source cannot be placed on grid edge";
+      return false;
+    }
+    if (x >= nx || y >= ny || z >= nz) {
+      err = "Probe index outside the solver grid";
+      return false;
+    }
+    const int64_t cell = (int64_t(x) * ny + y) * nz + z;
+    out.probe_cell[p] = cell;
+    by_cell.emplace_back(cell, int(p));
+  }
+  std::stable_sort(by_cell.begin(), by_cell.end(),
+                   [](const auto& a, const auto& b) { return a.first < b.first; });
+  // cell -> (first entry, count, source-field mask)
+  struct CellInfo {
+    int first, count;
+    unsigned src_mask;
+  };
+  std::unordered_map<int64_t, CellInfo> cell_info;
+  for (size_t e = 0; e < by_cell.size(); ++e) {
+    const int p = by_cell[e].second;
+    out.cell_probes.push_back({p, probes[p].field});
+    auto it = cell_info.find(by_cell[e].first);
+    if (it == cell_info.end()) it = cell_info.emplace(by_cell[e].first, CellInfo{int(e), 0, 0u}).first;
+    it->second.count += 1;
+    if (probes[p].is_source) it->second.src_mask |= 1u << probes[p].field;
+  }
+  for (auto& kv : cell_info)
+    if (kv.second.count > 0xFFFF) {
+      err = "Too many probes on one cell.";
+      return false;
+    }
+
+  // ---- rows, built per x slab in parallel with thread-local dedup
+  n_threads = std::max(1, std::min(n_threads, nx));
+  std::vector<RowMap> local_maps(n_threads);
+  std::vector<std::vector<Row>> local_rows(n_threads);
+  std::vector<uint32_t> local_ids(static_cast<size_t>(ncell));
+  std::vector<int64_t> e_split(n_threads, 0), h_split(n_threads, 0);
+  auto work = [&](int t, int xa, int xb) {
+    RowMap& map = local_maps[t];
+    std::vector<Row>& rows = local_rows[t];
+    Row prev;
+    uint32_t prev_id = UINT32_MAX;
+    for (int x = xa; x < xb; ++x)
+      for (int y = 0; y < ny; ++y)
+        for (int z = 0; z < nz; ++z) {
+          const int64_t cell = (int64_t(x) * ny + y) * nz + z;
+          Row r;
+          for (int c = 0; c < kNumCoef; ++c) r.w[kSlotOf[c]] = fbits(coef[c][cell]);
+          if (x == nx - 1)  // solver_init_fields zeroes the last x plane of Cy, Cz, Dx
+            for (int s = R_CA_EY_Z; s <= R_DB2_HX_Z; ++s) r.w[s] = 0u;
+          unsigned src_mask = 0;
+          int probe_first = -1, probe_count = 0;
+          if (!cell_info.empty()) {
+            auto it = cell_info.find(cell);
+            if (it != cell_info.end()) {
+              src_mask = it->second.src_mask;
+              probe_first = it->second.first;
+              probe_count = it->second.count;
+            }
+          }
+          // guarded (never updated) E splits: ex_y, ez_y at y max; ex_z, ey_z at
+          // z max; ey_x, ez_x at x max (solver.cu:152-185)
+          const bool frozen[6] = {y == ny - 1, z == nz - 1, z == nz - 1, x == nx - 1, x == nx - 1, y == ny - 1};
+          for (int s = 0; s < 6; ++s) {
+            if (!frozen[s]) continue;
+            const int comp = s / 2, partner = s ^ 1;
+            if (src_mask & (1u << comp)) {
+              r.w[2 * s] = fbits(1.0f);
+              r.w[2 * s + 1] = 0u;
+            } else {
+              r.w[2 * s] = frozen[partner] ? 0u : r.w[2 * partner];
+              r.w[2 * s + 1] = 0u;
+            }
+          }
+          uint32_t flags = 0;
+          if (r.w[R_CA_EX_Y] != r.w[R_CA_EX_Z] || r.w[R_CA_EY_Z] != r.w[R_CA_EY_X] ||
+              r.w[R_CA_EZ_X] != r.w[R_CA_EZ_Y] || (src_mask & 7u))
+            flags |= kFlagESplit;
+          if (r.w[R_DA_HX_Y] != r.w[R_DA_HX_Z] || r.w[R_DA_HY_Z] != r.w[R_DA_HY_X] ||
+              r.w[R_DA_HZ_X] != r.w[R_DA_HZ_Y] || (src_mask & 0x38u))
+            flags |= kFlagHSplit;
+          flags |= uint32_t(probe_count) << 16;
+          e_split[t] += (flags & kFlagESplit) ? 1 : 0;
+          h_split[t] += (flags & kFlagHSplit) ? 1 : 0;
+          r.w[R_FLAGS] = flags;
+          r.w[R_PROBE] = uint32_t(probe_first);
+          uint32_t id;
+          if (prev_id != UINT32_MAX && RowEq()(r, prev)) {
+            id = prev_id;
+          } else {
+            auto ins = map.emplace(r, uint32_t(rows.size()));
+            if (ins.second) rows.push_back(r);
+            id = ins.first->second;
+            prev = r;
+            prev_id = id;
+          }
+          local_ids[size_t(cell)] = id;
+        }
+  };
+  {
+    std::vector<std::thread> pool;
+    const int base = nx / n_threads, rem = nx % n_threads;
+    int xa = 0;
+    for (int t = 0; t < n_threads; ++t) {
+      const int xb = xa + base + (t < rem ? 1 : 0);
+      pool.emplace_back(work, t, xa, xb);
+      xa = xb;
+    }
+    for (auto& th : pool) th.join();
+  }
+
+  // ---- merge the thread-local tables; row 0 is the all-zero row
+  RowMap global;
+  Row zero;
+  std::memset(zero.w, 0, sizeof(zero.w));
+  zero.w[R_PROBE] = uint32_t(-1);
+  global.emplace(zero, 0u);
+  out.rows.push_back(zero);
+  std::vector<std::vector<uint32_t>> remap(n_threads);
+  for (int t = 0; t < n_threads; ++t) {
+    remap[t].resize(local_rows[t].size());
+    for (size_t i = 0; i < local_rows[t].size(); ++i) {
+      auto ins = global.emplace(local_rows[t][i], uint32_t(out.rows.size()));
+      if (ins.second) out.rows.push_back(local_rows[t][i]);
+      remap[t][i] = ins.first->second;
+    }
+  }
+  if (out.rows.size() > 65536) {
+    err = "The coefficient arrays hold " + std::to_string(out.rows.size()) +
+          " distinct cell rows; the material table holds at most 65536.";
+    return false;
+  }
+  out.ids.resize(size_t(ncell));
+  {
+    std::vector<std::thread> pool;
+    const int base = nx / n_threads, rem = nx % n_threads;
+    int xa = 0;
+    for (int t = 0; t < n_threads; ++t) {
+      const int xb = xa + base + (t < rem ? 1 : 0);
+      pool.emplace_back([&, t, xa, xb] {
+        const size_t a = size_t(xa) * ny * nz, b = size_t(xb) * ny * nz;
+        for (size_t c = a; c < b; ++c) out.ids[c] = uint16_t(remap[t][local_ids[c]]);
+      });
+      xa = xb;
+    }
+    for (auto& th : pool) th.join();
+  }
+  for (int t = 0; t < n_threads; ++t) {
+    out.e_split_cells += e_split[t];
+    out.h_split_cells += h_split[t];
+  }
+  out.compile_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  return true;
+}
+
+}  // namespace rfn

@@ -1,0 +1,71 @@
+// Host-side compilation of the reference's 30 per-component coefficient
+// arrays into a per-cell material index plus a table of distinct coefficient
+// rows, the form the B200 kernels read.
+#pragma once
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+namespace rfn {
+
+constexpr int kNumCoef = 30;
+
+// Coefficient names in the key order of the dict built at
+// rfnetwork/solver.py:1473-1518.
+extern const char* const kCoefNames[kNumCoef];
+
+// Position of each coefficient inside a table row (the kernel's order).
+enum RowSlot : int {
+  // E: (Ca, Cb) per split, splits ordered as in solver.h:20-39
+  R_CA_EX_Y = 0, R_CB_EX_Y, R_CA_EX_Z, R_CB_EX_Z,
+  R_CA_EY_Z, R_CB_EY_Z, R_CA_EY_X, R_CB_EY_X,
+  R_CA_EZ_X, R_CB_EZ_X, R_CA_EZ_Y, R_CB_EZ_Y,
+  // H: (Da, Db1, Db2) per split, solver.h:41-79
+  R_DA_HX_Y = 12, R_DB1_HX_Y, R_DB2_HX_Y, R_DA_HX_Z, R_DB1_HX_Z, R_DB2_HX_Z,
+  R_DA_HY_Z, R_DB1_HY_Z, R_DB2_HY_Z, R_DA_HY_X, R_DB1_HY_X, R_DB2_HY_X,
+  R_DA_HZ_X, R_DB1_HZ_X, R_DB2_HZ_X, R_DA_HZ_Y, R_DB1_HZ_Y, R_DB2_HZ_Y,
+  R_FLAGS = 30,  // bit 0: E split storage, bit 1: H split storage, bits 16..31: probe entries
+  R_PROBE = 31,  // first entry of this cell in the per-cell probe list (-1 if none)
+  kRowWords = 32
+};
+constexpr uint32_t kFlagESplit = 1u;
+constexpr uint32_t kFlagHSplit = 2u;
+
+struct Row {
+  uint32_t w[kRowWords];
+};
+
+struct ProbeSpec {
+  int field;          // 0..5
+  int i, j, k;        // full-grid component index
+  int is_source;
+};
+
+// One entry of the per-cell probe list: probe index and its field code.
+struct CellProbe {
+  int probe;
+  int field;
+};
+
+struct CompiledGrid {
+  int nx = 0, ny = 0, nz = 0;
+  std::vector<Row> rows;                 // distinct rows; row 0 is all zero
+  std::vector<uint16_t> ids;             // per cell, reference order [x][y][z]
+  std::vector<CellProbe> cell_probes;    // grouped per probe cell
+  std::vector<int64_t> probe_cell;       // per probe: cell index (x*ny + y)*nz + z
+  int64_t e_split_cells = 0, h_split_cells = 0;
+  double compile_ms = 0;
+};
+
+// Builds the table. coef[i] points to kCoefNames[i]'s (nx, ny, nz) array.
+// Returns false with `err` set on invalid input or when more than 65535
+// distinct rows are needed.
+bool compile_grid(int nx, int ny, int nz, const float* const* coef, const std::vector<ProbeSpec>& probes,
+                  int n_threads, CompiledGrid& out, std::string& err);
+
+// Expands a row back to the coefficient the reference kernel would apply to
+// split `c` (coefficient index into kCoefNames) -- used by tests.
+float row_coefficient(const Row& r, int c);
+
+}  // namespace rfn

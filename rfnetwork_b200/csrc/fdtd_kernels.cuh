@@ -1,0 +1,361 @@
+// sm_100a kernels of the FDTD time loop.
+//
+// One launch of `fdtd_step_kernel` advances every cell of every simulation in
+// a batch by one full Yee step: E^{n} -> E^{n+1} (efield_update_kernel,
+// rfnetwork/core/src/solver.cu:116-191), soft sources / E probes
+// (e_probe_update_kernel, solver.cu:439-490), H^{n} -> H^{n+1}
+// (hfield_update_kernel, solver.cu:278-356) and H sources / probes
+// (h_probe_update_kernel, solver.cu:492-543) -- four launches per step in the
+// reference, one here.
+//
+// Layout in HBM (per simulation, GPU index space of the reference):
+//   fields   float32 [z][y][x], x fastest, row pitch a multiple of 32 floats;
+//            two buffers per field (step n reads buffer n&1, writes the other),
+//            so a block can recompute its halo from consistent step-n data
+//            while neighbours already write step n+1.
+//   splits   the two split components of E (ex_y, ex_z, ...) and H, same
+//            layout, read and written only for cells flagged in the material
+//            table (PML slabs, source cells); unsplit cells never touch them.
+//   material uint16 [z][y][x] row index into a table of 32-word rows: the
+//            cell's 30 update coefficients + flags + probe-list offset.
+//
+// Work decomposition: a block owns a tile of 31 (x) by TY (y) cells and a
+// z range, with one warp per y row plus one halo row below (y0-1) and lane 0
+// on the halo column (x0-1). It streams up through z: at plane z every lane
+// computes E^{n+1}(z) for its column, trades x neighbours by warp shuffle and
+// y neighbours through shared memory, then the owned cells compute
+// H^{n+1}(z) from E^{n+1}(z) and E^{n+1}(z-1) (kept in registers). The halo
+// row / column recompute E so no second sweep over memory is needed.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace rfn {
+
+constexpr int kTileX = 31;        // cells owned per tile along x (lane 0 is the halo column)
+constexpr int kTileY = 7;         // rows owned per tile along y (warp 0 is the halo row)
+constexpr int kBlockY = kTileY + 1;
+
+constexpr uint32_t kESplit = 1u, kHSplit = 2u;
+
+struct SimDev {
+  int nx, ny, nz, pitch;  // cells; pitch = floats per x row
+  int plane;              // ny * pitch
+  int nt;
+  float* E[2][3];         // [buffer][ex, ey, ez]
+  float* H[2][3];         // [buffer][hx, hy, hz]
+  float* Es[2][6];        // [buffer][ex_y, ex_z, ey_z, ey_x, ez_x, ez_y]
+  float* Hs[2][6];        // [buffer][hx_y, hx_z, hy_z, hy_x, hz_x, hz_y]
+  const uint16_t* mat;    // [z][y][pitch]
+  const float4* rows;     // 8 float4 per row
+  const int2* cell_probes;  // (probe, field) grouped per probe cell
+  const float* src;       // [P][nt] soft-source amplitudes
+  float* rec;             // [P][nt] recorded field values
+  const int* is_src;      // [P]
+};
+
+__device__ __forceinline__ float ldf(const float* p, int i, bool ok) { return ok ? __ldg(p + i) : 0.0f; }
+
+template <int TY>
+__global__ void __launch_bounds__(32 * (TY + 1))
+fdtd_step_kernel(const SimDev* __restrict__ sims, const int4* __restrict__ tiles, int n) {
+  const int4 t = tiles[blockIdx.x];
+  const SimDev& S = sims[t.x];
+  const int x0 = t.y & 0xffff, y0 = int(unsigned(t.y) >> 16), z0 = t.z & 0xffff, z1 = int(unsigned(t.z) >> 16);
+  const int lane = threadIdx.x, w = threadIdx.y;
+  const int c = x0 - 1 + lane;  // this lane's column
+  const int r = y0 - 1 + w;     // this warp's row
+  const int nx = S.nx, ny = S.ny, nz = S.nz, pitch = S.pitch, plane = S.plane;
+  const bool in_xy = c >= 0 && c < nx && r >= 0 && r < ny;
+  const bool own = in_xy && lane >= 1 && w >= 1;  // tile cells this thread stores
+  const bool has_yn = in_xy && r + 1 < ny;
+  const bool has_xn = (c + 1) >= 0 && (c + 1) < nx && r >= 0 && r < ny;
+  const int cur = n & 1, nxt = cur ^ 1;
+
+  const float* __restrict__ Ex = S.E[cur][0];
+  const float* __restrict__ Ey = S.E[cur][1];
+  const float* __restrict__ Ez = S.E[cur][2];
+  const float* __restrict__ Hx = S.H[cur][0];
+  const float* __restrict__ Hy = S.H[cur][1];
+  const float* __restrict__ Hz = S.H[cur][2];
+
+  __shared__ float s_ex[2][TY + 1][32];
+  __shared__ float s_ez[2][TY + 1][32];
+
+  const int col = r * pitch + c;  // offset inside a z plane (valid when in_xy)
+  float hx_c = 0.f, hy_c = 0.f;   // H^n at (c, r, z), carried from the look-ahead
+  float ex_p = 0.f, ey_p = 0.f;   // E^{n+1} at (c, r, z-1)
+  {
+    const int zp = z0 - 1;
+    const bool ok = in_xy && zp >= 0;
+    hx_c = ldf(Hx, zp * plane + col, ok);
+    hy_c = ldf(Hy, zp * plane + col, ok);
+  }
+
+  for (int z = z0 - 1; z < z1; ++z) {
+    const bool zin = z >= 0 && z < nz;
+    const bool live = in_xy && zin;
+    const int idx = z * plane + col;
+    const int buf = z & 1;
+
+    // ---- H^n around (c, r, z)
+    const float hz_c = ldf(Hz, idx, live);
+    const bool zn_ok = in_xy && z + 1 < nz && z + 1 >= 0;
+    const float hx_n = ldf(Hx, idx + plane, zn_ok);
+    const float hy_n = ldf(Hy, idx + plane, zn_ok);
+    const float hz_yn = ldf(Hz, idx + pitch, has_yn && zin);
+    const float hx_yn = ldf(Hx, idx + pitch, has_yn && zin);
+    float hz_xn = __shfl_down_sync(0xffffffffu, hz_c, 1);
+    float hy_xn = __shfl_down_sync(0xffffffffu, hy_c, 1);
+    if (lane == 31) {
+      hz_xn = ldf(Hz, idx + 1, has_xn && zin);
+      hy_xn = ldf(Hy, idx + 1, has_xn && zin);
+    }
+
+    // ---- E^{n+1}(c, r, z)
+    float ex = 0.f, ey = 0.f, ez = 0.f;
+    float4 rw7 = make_float4(0.f, 0.f, 0.f, 0.f);
+    int id = 0;
+    uint32_t flags = 0;
+    if (live) {
+      id = __ldg(S.mat + idx);
+      const float4* row = S.rows + 8 * id;
+      const float4 a = __ldg(row + 0), b = __ldg(row + 1), d = __ldg(row + 2);
+      rw7 = __ldg(row + 7);
+      flags = __float_as_uint(rw7.z);
+      const float dhz_y = hz_yn - hz_c, dhy_z = hy_n - hy_c;
+      const float dhx_z = hx_n - hx_c, dhz_x = hz_xn - hz_c;
+      const float dhy_x = hy_xn - hy_c, dhx_y = hx_yn - hx_c;
+      if (!(flags & kESplit)) {
+        // interior: both splits share Ca, so f' = Ca f + Cb1 d1 + Cb2 d2
+        ex = a.x * __ldg(Ex + idx) + a.y * dhz_y + a.w * dhy_z;
+        ey = b.x * __ldg(Ey + idx) + b.y * dhx_z + b.w * dhz_x;
+        ez = d.x * __ldg(Ez + idx) + d.y * dhy_x + d.w * dhx_y;
+      } else {
+        const float* const* Es = S.Es[cur];
+        float s0 = a.x * __ldg(Es[0] + idx) + a.y * dhz_y;  // ex_y
+        float s1 = a.z * __ldg(Es[1] + idx) + a.w * dhy_z;  // ex_z
+        float s2 = b.x * __ldg(Es[2] + idx) + b.y * dhx_z;  // ey_z
+        float s3 = b.z * __ldg(Es[3] + idx) + b.w * dhz_x;  // ey_x
+        float s4 = d.x * __ldg(Es[4] + idx) + d.y * dhy_x;  // ez_x
+        float s5 = d.z * __ldg(Es[5] + idx) + d.w * dhx_y;  // ez_y
+        const int np = int(flags >> 16);
+        if (np) {
+          // soft sources: s1 += v; s2 += v; f = s1 + s2 (solver.cu:459-488)
+          const int first = __float_as_int(rw7.w);
+          for (int e = 0; e < np; ++e) {
+            const int2 pe = __ldg(S.cell_probes + first + e);
+            if (pe.y < 3 && __ldg(S.is_src + pe.x)) {
+              const float v = __ldg(S.src + (size_t)pe.x * S.nt + n);
+              if (pe.y == 0) { s0 += v; s1 += v; }
+              if (pe.y == 1) { s2 += v; s3 += v; }
+              if (pe.y == 2) { s4 += v; s5 += v; }
+            }
+          }
+        }
+        ex = s0 + s1;
+        ey = s2 + s3;
+        ez = s4 + s5;
+        if (own && z >= z0) {
+          float* const* Eo = S.Es[nxt];
+          Eo[0][idx] = s0; Eo[1][idx] = s1; Eo[2][idx] = s2;
+          Eo[3][idx] = s3; Eo[4][idx] = s4; Eo[5][idx] = s5;
+        }
+      }
+    }
+
+    // ---- neighbour exchange of E^{n+1}
+    s_ex[buf][w][lane] = ex;
+    s_ez[buf][w][lane] = ez;
+    const float ey_xm = __shfl_up_sync(0xffffffffu, ey, 1);
+    const float ez_xm = __shfl_up_sync(0xffffffffu, ez, 1);
+    __syncthreads();
+
+    if (own && z >= z0 && zin) {
+      const float ex_ym = s_ex[buf][w - 1][lane];
+      const float ez_ym = s_ez[buf][w - 1][lane];
+      if (!(flags & kESplit)) {
+        S.E[nxt][0][idx] = ex;
+        S.E[nxt][1][idx] = ey;
+        S.E[nxt][2][idx] = ez;
+      }
+      const float4* row = S.rows + 8 * id;
+      const float4 p = __ldg(row + 3), q = __ldg(row + 4), u = __ldg(row + 5), v6 = __ldg(row + 6);
+      // slots 12..29: (Da, Db1, Db2) for hx_y, hx_z, hy_z, hy_x, hz_x, hz_y
+      const float da_xy = p.x, b1_xy = p.y, b2_xy = p.z, da_xz = p.w;
+      const float b1_xz = q.x, b2_xz = q.y, da_yz = q.z, b1_yz = q.w;
+      const float b2_yz = u.x, da_yx = u.y, b1_yx = u.z, b2_yx = u.w;
+      const float da_zx = v6.x, b1_zx = v6.y, b2_zx = v6.z, da_zy = v6.w;
+      const float b1_zy = rw7.x, b2_zy = rw7.y;
+      const float gxy = b2_xy * ez - b1_xy * ez_ym;
+      const float gxz = b2_xz * ey - b1_xz * ey_p;
+      const float gyz = b2_yz * ex - b1_yz * ex_p;
+      const float gyx = b2_yx * ez - b1_yx * ez_xm;
+      const float gzx = b2_zx * ey - b1_zx * ey_xm;
+      const float gzy = b2_zy * ex - b1_zy * ex_ym;
+      float hx, hy, hz;
+      if (!(flags & kHSplit)) {
+        hx = da_xy * hx_c + gxy + gxz;
+        hy = da_yz * hy_c + gyz + gyx;
+        hz = da_zx * hz_c + gzx + gzy;
+      } else {
+        const float* const* Hs = S.Hs[cur];
+        float s0 = da_xy * __ldg(Hs[0] + idx) + gxy;
+        float s1 = da_xz * __ldg(Hs[1] + idx) + gxz;
+        float s2 = da_yz * __ldg(Hs[2] + idx) + gyz;
+        float s3 = da_yx * __ldg(Hs[3] + idx) + gyx;
+        float s4 = da_zx * __ldg(Hs[4] + idx) + gzx;
+        float s5 = da_zy * __ldg(Hs[5] + idx) + gzy;
+        const int np = int(flags >> 16);
+        if (np) {
+          const int first = __float_as_int(rw7.w);
+          for (int e = 0; e < np; ++e) {
+            const int2 pe = __ldg(S.cell_probes + first + e);
+            if (pe.y >= 3 && __ldg(S.is_src + pe.x)) {
+              const float v = __ldg(S.src + (size_t)pe.x * S.nt + n);
+              if (pe.y == 3) { s0 += v; s1 += v; }
+              if (pe.y == 4) { s2 += v; s3 += v; }
+              if (pe.y == 5) { s4 += v; s5 += v; }
+            }
+          }
+        }
+        hx = s0 + s1;
+        hy = s2 + s3;
+        hz = s4 + s5;
+        float* const* Ho = S.Hs[nxt];
+        Ho[0][idx] = s0; Ho[1][idx] = s1; Ho[2][idx] = s2;
+        Ho[3][idx] = s3; Ho[4][idx] = s4; Ho[5][idx] = s5;
+      }
+      S.H[nxt][0][idx] = hx;
+      S.H[nxt][1][idx] = hy;
+      S.H[nxt][2][idx] = hz;
+      const int np = int(flags >> 16);
+      if (np) {  // record probes of this cell (solver.cu:467, 521)
+        const int first = __float_as_int(rw7.w);
+        for (int e = 0; e < np; ++e) {
+          const int2 pe = __ldg(S.cell_probes + first + e);
+          const float val = pe.y == 0 ? ex : pe.y == 1 ? ey : pe.y == 2 ? ez : pe.y == 3 ? hx : pe.y == 4 ? hy : hz;
+          S.rec[(size_t)pe.x * S.nt + n] = val;
+        }
+      }
+    }
+    ex_p = ex;
+    ey_p = ey;
+    hx_c = hx_n;
+    hy_c = hy_n;
+  }
+}
+
+// Ids arrive in the reference order [x][y][z]; the kernels read [z][y][pitch].
+__global__ void transpose_ids_kernel(const uint16_t* __restrict__ in, uint16_t* __restrict__ out, int nx, int ny,
+                                     int nz, int pitch) {
+  const int64_t total = int64_t(nx) * ny * nz;
+  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < total; i += int64_t(gridDim.x) * blockDim.x) {
+    const int z = int(i % nz);
+    const int64_t xy = i / nz;
+    const int y = int(xy % ny), x = int(xy / ny);
+    out[(int64_t(z) * ny + y) * pitch + x] = in[i];
+  }
+}
+
+// ------------------------------------------------------------------ DFT
+struct DftDev {
+  int n_series, n_freq, nt;
+  const int* series_start;   // n_series + 1
+  const int* term_probe;
+  const double* term_weight;
+  const double* omega;       // radians per step
+  const float* rec;          // [P][nt]
+  double2* X;                // [n_series][n_freq]
+};
+
+// X[s][f] += sum_{n0 <= n < n1} series_s[n] e^{-j omega_f n}. One block per
+// (f, s); fixed-order block reduction, so results are deterministic.
+__global__ void __launch_bounds__(256) dft_accumulate_kernel(DftDev d, int n0, int n1) {
+  const int f = blockIdx.x, s = blockIdx.y;
+  const double om = d.omega[f];
+  const int t0 = d.series_start[s], t1 = d.series_start[s + 1];
+  double re = 0.0, im = 0.0;
+  for (int n = n0 + threadIdx.x; n < n1; n += blockDim.x) {
+    double v = 0.0;
+    for (int t = t0; t < t1; ++t) v += d.term_weight[t] * double(d.rec[size_t(d.term_probe[t]) * d.nt + n]);
+    double sn, cs;
+    sincos(om * double(n), &sn, &cs);
+    re += v * cs;
+    im -= v * sn;
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    re += __shfl_down_sync(0xffffffffu, re, o);
+    im += __shfl_down_sync(0xffffffffu, im, o);
+  }
+  __shared__ double sre[8], sim[8];
+  const int wid = threadIdx.x >> 5, ln = threadIdx.x & 31;
+  if (ln == 0) {
+    sre[wid] = re;
+    sim[wid] = im;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double a = 0.0, b = 0.0;
+    for (int i = 0; i < int(blockDim.x >> 5); ++i) {
+      a += sre[i];
+      b += sim[i];
+    }
+    double2 x = d.X[s * d.n_freq + f];
+    x.x += a;
+    x.y += b;
+    d.X[s * d.n_freq + f] = x;
+  }
+}
+
+// -------------------------------------------------------------- monitors
+struct MonDev {
+  int field, axis, position, n_step, n_freq, n1, n2;
+  void* out;                 // float [Nm][n1][n2] or float2 [n_freq][n1][n2]
+  const float2* phase;       // [Nm][n_freq]
+};
+
+// Samples the fields after step n (E and H of the new buffer), i.e. after the
+// sources of the step are applied, as the CPU engine does (solver.cpp:1129-1161).
+__global__ void monitor_kernel(const SimDev* __restrict__ sim, const MonDev* __restrict__ mons, int n_mon, int n,
+                               int buf) {
+  const SimDev& S = *sim;
+  for (int m = 0; m < n_mon; ++m) {
+    const MonDev M = mons[m];
+    if (n > 0 && (n % M.n_step) != 0) continue;
+    const int mn = n / M.n_step;
+    const int total = M.n1 * M.n2;
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < total; e += gridDim.x * blockDim.x) {
+      const int a = e / M.n2, b = e % M.n2;
+      int x, y, z;
+      if (M.axis == 0) { x = M.position; y = a; z = b; }
+      else if (M.axis == 1) { x = a; y = M.position; z = b; }
+      else { x = a; y = b; z = M.position; }
+      if (x < 0 || y < 0 || z < 0 || x >= S.nx || y >= S.ny || z >= S.nz) continue;
+      const int idx = z * S.plane + y * S.pitch + x;
+      const uint32_t flags = __float_as_uint(S.rows[8 * S.mat[idx] + 7].z);
+      float v;
+      if (M.field < 3) {
+        v = (flags & kESplit) ? S.Es[buf][2 * M.field][idx] + S.Es[buf][2 * M.field + 1][idx]
+                              : S.E[buf][M.field][idx];
+      } else {
+        v = S.H[buf][M.field - 3][idx];
+      }
+      if (M.n_freq == 0) {
+        static_cast<float*>(M.out)[size_t(mn) * total + e] = v;
+      } else {
+        float2* o = static_cast<float2*>(M.out);
+        for (int f = 0; f < M.n_freq; ++f) {
+          const float2 ph = M.phase[size_t(mn) * M.n_freq + f];
+          float2 acc = o[size_t(f) * total + e];
+          acc.x += v * ph.x;
+          acc.y += v * ph.y;
+          o[size_t(f) * total + e] = acc;
+        }
+      }
+    }
+  }
+}
+
+}  // namespace rfn

@@ -1,0 +1,104 @@
+"""Engine library checks that need no GPU: it loads, exports every declared
+entry point, validates arguments, and its host-side material-table compiler
+reproduces the oracle's arithmetic (replayed through tests/kernel_model.py)."""
+import re
+
+import numpy as np
+import pytest
+
+import kernel_model as km
+import make_setup_golden as mg
+from helpers import rel_l2, run_oracle
+from rfnetwork_b200 import _lib, configs
+from rfnetwork_b200 import geometry as geo
+from rfnetwork_b200 import solver as S
+from rfnetwork_b200.solver_constants import COEFF_NAMES
+
+HEADER = mg.HERE.parent.parent / "include" / "fdtd.h"
+
+
+def declared_functions():
+    text = HEADER.read_text()
+    return sorted(set(re.findall(r"^\s*(?:int|void|const char\*)\s+(fdtd_\w+)\s*\(", text, flags=re.M)))
+
+
+def test_exports_every_declared_symbol(engine_lib):
+    names = declared_functions()
+    assert len(names) >= 20
+    for n in names:
+        assert hasattr(engine_lib, n), n
+    assert set(names) == set(_lib.EXPORTED)
+
+
+def test_argument_errors(engine_lib):
+    with pytest.raises(ValueError):
+        _lib.Simulation(1, 4, 4)
+    sim = _lib.Simulation(4, 5, 6)
+    with pytest.raises(ValueError, match="Expected shape on axis 2"):
+        sim.set_coefficient("Ca_ex_y", np.zeros((4, 5, 7), np.float32))
+    with pytest.raises(ValueError, match="Unknown coefficient"):
+        sim.set_coefficient("Ca_xx", np.zeros((4, 5, 6), np.float32))
+    with pytest.raises(_lib.FdtdError, match="Coefficient not set"):
+        sim.compile()
+    for name in COEFF_NAMES:
+        sim.set_coefficient(name, np.ones((4, 5, 6), np.float32))
+    sim.add_probe(2, (1, 1, 0))           # ez at x=1, y=1 -> cell (0, 0, 0)
+    assert sim.compile()["n_rows"] >= 2
+    sim.add_probe(0, (0, 0, 3))           # ex at y=0 lies on the PEC edge
+    with pytest.raises(_lib.FdtdError, match="Source cannot be placed on grid edge"):
+        sim.compile()
+
+
+@pytest.fixture(scope="module")
+def small():
+    return mg.build_model(S.FDTD_Solver, geo.Box, geo.Rectangle, geo.Line, mg.grid_edges(),
+                          lambda s, e: s.generate_mesh(grid=e))
+
+
+def _table(s):
+    co, pr, mo, mem, Nx, Ny, Nz, Nt = s.pack_inputs(gpu=True)
+    sim = _lib.Simulation(Nx, Ny, Nz)
+    sim.set_coefficients(co)
+    for p in pr:
+        sim.add_probe(p["field"], p["idx"], p["is_source"], p["values"] if p["is_source"] else None)
+    ids, rows = sim.material_table()
+    return ids, rows, pr, Nt
+
+
+def test_table_reproduces_coefficients(engine_lib, small):
+    """Every non-boundary cell's row holds exactly the reference coefficients."""
+    ids, rows, pr, Nt = _table(small)
+    co = small.pack_inputs(gpu=True)[0]
+    slot = dict(zip(COEFF_NAMES, [0, 2, 1, 3, 4, 6, 5, 7, 8, 10, 9, 11, 12, 15, 13, 14, 16, 17,
+                                   18, 21, 19, 20, 22, 23, 24, 27, 25, 26, 28, 29]))
+    inner = (slice(0, -1), slice(0, -1), slice(0, -1))
+    for name, arr in co.items():
+        got = rows[:, slot[name]].view(np.float32)[ids]
+        assert np.array_equal(got[inner].view(np.uint32), arr[inner].view(np.uint32)), name
+    assert rows[0].view(np.float32)[:30].tolist() == [0.0] * 30
+
+
+def test_kernel_arithmetic_model_matches_oracle(engine_lib, oracle_lib, small):
+    ids, rows, pr, Nt = _table(small)
+    src = np.array([p["values"] for p in pr])
+    rec = km.run_model(ids, rows, None, km.shifted_probes(pr), src, Nt)
+    _, ref = run_oracle(small)
+    assert rel_l2(rec, ref) < 1e-6
+
+
+def test_split_flags_cover_pml(engine_lib):
+    s = configs.microstrip(n=(24, 24, 20), n_pml=4, nt=10)
+    co, pr, mo, mem, Nx, Ny, Nz, Nt = s.pack_inputs(gpu=True)
+    sim = _lib.Simulation(Nx, Ny, Nz)
+    sim.set_coefficients(co)
+    ids, rows = sim.material_table()
+    esplit = (rows[:, 30] & 1)[ids] != 0
+    # cells where the two E splits of a component have different Ca must be split
+    for a, b in (("Ca_ex_y", "Ca_ex_z"), ("Ca_ey_z", "Ca_ey_x"), ("Ca_ez_x", "Ca_ez_y")):
+        diff = co[a] != co[b]
+        diff[-1] = False          # x-max plane is zeroed (solver.cpp:294-311)
+        diff[:, -1] = False       # guarded planes (solver.cu:152-185)
+        diff[:, :, -1] = False
+        assert not np.any(diff & ~esplit), a
+    # the deep interior is unsplit
+    assert not esplit[8:-8, 8:-8, 8:-8].any()
