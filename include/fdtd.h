@@ -55,6 +55,11 @@ typedef struct fdtd_stats {
   int64_t dft_launches;  /* DFT kernel launches issued by the last run */
   double last_run_ms;    /* device time of the last run (CUDA events) */
   double compile_ms;     /* host time spent building the material table */
+  int variant;           /* step kernel: 0 plain loads, 1 TMA-pipelined */
+  int tile_y;            /* tile height (rows) of the step kernel */
+  int stages;            /* shared-memory pipeline stages (TMA kernel) */
+  int zchunk;            /* z planes per tile */
+  int grid;              /* blocks launched per step */
 } fdtd_stats;
 
 /* --------------------------------------------------------------- one grid */
@@ -110,6 +115,13 @@ int fdtd_run(fdtd_sim* s, int nt);
 int fdtd_run_async(fdtd_sim* s, int nt);
 int fdtd_synchronize(fdtd_sim* s);
 
+/* Step-kernel selection: variant 0 = plain loads (1 cell per thread, 31 x 7
+ * tiles), 1 = TMA-pipelined (64 x tile_y tiles, `stages` plane buffers).
+ * zchunk = z planes per tile (0: derived from the grid). The default comes from
+ * RFN_FDTD_KERNEL / RFN_FDTD_TY / RFN_FDTD_STAGES / RFN_FDTD_ZCHUNK or is
+ * (1, 8, 4, 0). The reference has one fixed 8x8x8 launch shape (solver.cu:549-557). */
+int fdtd_set_kernel(fdtd_sim* s, int variant, int tile_y, int stages, int zchunk);
+
 /* Launch on a caller stream (cudaStream_t passed as void*); NULL = own stream. */
 int fdtd_set_stream(fdtd_sim* s, void* stream);
 
@@ -134,6 +146,7 @@ void fdtd_destroy(fdtd_sim* s);
  * coefficients, probes and DFT; results are read per member after the run. */
 int fdtd_batch_create(fdtd_sim* const* sims, int n_sims, fdtd_batch** out);
 int fdtd_batch_run(fdtd_batch* b, int nt);
+int fdtd_batch_set_kernel(fdtd_batch* b, int variant, int tile_y, int stages, int zchunk);
 int fdtd_batch_set_stream(fdtd_batch* b, void* stream);
 int fdtd_batch_get_stats(const fdtd_batch* b, fdtd_stats* out);
 const char* fdtd_batch_last_error(const fdtd_batch* b);

@@ -18,6 +18,7 @@ EXPORTED = (
     "fdtd_create", "fdtd_set_coefficient", "fdtd_add_probe", "fdtd_add_monitor", "fdtd_set_dft",
     "fdtd_compile", "fdtd_get_material_table",
     "fdtd_run", "fdtd_run_async", "fdtd_synchronize", "fdtd_set_stream", "fdtd_get_probe_values",
+    "fdtd_set_kernel", "fdtd_batch_set_kernel",
     "fdtd_get_dft", "fdtd_get_monitor", "fdtd_get_stats", "fdtd_last_error", "fdtd_destroy",
     "fdtd_batch_create", "fdtd_batch_run", "fdtd_batch_set_stream", "fdtd_batch_get_stats",
     "fdtd_batch_last_error", "fdtd_batch_destroy", "fdtd_global_error",
@@ -31,6 +32,8 @@ class FdtdStats(ctypes.Structure):
         ("e_split_cells", ctypes.c_int64), ("h_split_cells", ctypes.c_int64),
         ("n_tiles", ctypes.c_int), ("step_launches", ctypes.c_int64), ("dft_launches", ctypes.c_int64),
         ("last_run_ms", ctypes.c_double), ("compile_ms", ctypes.c_double),
+        ("variant", ctypes.c_int), ("tile_y", ctypes.c_int), ("stages", ctypes.c_int), ("zchunk", ctypes.c_int),
+        ("grid", ctypes.c_int),
     ]
 
     def as_dict(self):
@@ -59,6 +62,8 @@ def load():
         "fdtd_set_dft": ([vp, ip, ip, vp, vp, vp, ip, vp], ip),
         "fdtd_compile": ([vp, ctypes.POINTER(ip), ctypes.POINTER(i64), ctypes.POINTER(i64)], ip),
         "fdtd_get_material_table": ([vp, vp, i64, vp, ip], ip),
+        "fdtd_set_kernel": ([vp, ip, ip, ip, ip], ip),
+        "fdtd_batch_set_kernel": ([vp, ip, ip, ip, ip], ip),
         "fdtd_run": ([vp, ip], ip),
         "fdtd_run_async": ([vp, ip], ip),
         "fdtd_synchronize": ([vp], ip),
@@ -190,6 +195,10 @@ class Simulation:
                                                      info["n_rows"]))
         return ids, rows
 
+    def set_kernel(self, variant: int = 1, tile_y: int = 8, stages: int = 4, zchunk: int = 0):
+        """Pick the step kernel (0 plain, 1 TMA) and its tile shape."""
+        self._check(self.lib.fdtd_set_kernel(self.h, int(variant), int(tile_y), int(stages), int(zchunk)))
+
     def set_stream(self, stream_ptr: int):
         self._check(self.lib.fdtd_set_stream(self.h, ctypes.c_void_p(int(stream_ptr))))
 
@@ -259,6 +268,11 @@ class Batch:
             raise FdtdError(f"{FDTD_ERRORS.get(rc, rc)}: {self.lib.fdtd_batch_last_error(self.h).decode()}")
         for s in self.sims:
             s.nt = int(nt)
+
+    def set_kernel(self, variant: int = 1, tile_y: int = 8, stages: int = 4, zchunk: int = 0):
+        rc = self.lib.fdtd_batch_set_kernel(self.h, int(variant), int(tile_y), int(stages), int(zchunk))
+        if rc:
+            raise ValueError(self.lib.fdtd_batch_last_error(self.h).decode())
 
     def set_stream(self, stream_ptr: int):
         self.lib.fdtd_batch_set_stream(self.h, ctypes.c_void_p(int(stream_ptr)))

@@ -93,7 +93,8 @@ def boxes(n=(256, 256, 128), n_pml=8, n_boxes=64, nt=5000, seed=2, n_ports=4, n_
         face = geo.Rectangle([(px * D, py * D, (pz + 4) * D), (px * D, (py + 4) * D, (pz + 4) * D),
                               (px * D, (py + 4) * D, pz * D)])
         s.add_lumped_port(k + 1, face, integration_line="z+")
-    s.assign_PML_boundaries("x-", "x+", "y-", "y+", "z-", "z+", n_pml=n_pml)
+    if n_pml:
+        s.assign_PML_boundaries("x-", "x+", "y-", "y+", "z-", "z+", n_pml=n_pml)
     s.generate_mesh(grid=_grid(n))
     for k in range(n_probes):
         idx = [int(rng.integers(lo[a] + 1, hi[a] - 1)) for a in range(3)]

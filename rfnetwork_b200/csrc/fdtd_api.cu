@@ -11,6 +11,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <memory>
@@ -21,6 +22,8 @@
 #include "../../include/fdtd.h"
 #include "fdtd_compile.h"
 #include "fdtd_kernels.cuh"
+#include "fdtd_step_tma.cuh"
+#include <cudaTypedefs.h>
 
 using namespace rfn;
 
@@ -86,6 +89,24 @@ int threads_for_host() {
 
 }  // namespace
 
+// Kernel selection of an engine: the plain-load kernel (one cell per thread)
+// or the TMA-pipelined kernel with its tile height, stage count and z chunk.
+struct KernelConfig {
+  int variant = 0;  // 0 plain, 1 tma
+  int ty = 7;
+  int stages = 4;
+  int zchunk = 0;   // 0: pick from the grid size
+};
+
+KernelConfig default_config() {
+  KernelConfig c;
+  if (const char* v = std::getenv("RFN_FDTD_KERNEL")) c.variant = (std::string(v) == "tma") ? 1 : 0;
+  if (const char* v = std::getenv("RFN_FDTD_TY")) c.ty = std::atoi(v);
+  if (const char* v = std::getenv("RFN_FDTD_STAGES")) c.stages = std::atoi(v);
+  if (const char* v = std::getenv("RFN_FDTD_ZCHUNK")) c.zchunk = std::atoi(v);
+  return c;
+}
+
 struct Engine;
 
 struct fdtd_sim {
@@ -124,16 +145,116 @@ struct fdtd_sim {
   DevBuf<SimDev> d_dev;  // this simulation's descriptor alone (monitor kernel)
 
   std::unique_ptr<Engine> engine;  // batch of one for fdtd_run
+  KernelConfig cfg = default_config();
   cudaStream_t ext_stream = nullptr;
   std::string err;
   fdtd_stats stats{};
 };
 
+using TmaKernelFn = void (*)(const SimDev*, const TileDesc*, int, int, unsigned*, unsigned, int*);
+
+// One instantiation of the TMA step kernel.
+struct TmaVariant {
+  int tx, ty, stages, mode;
+  int smem, threads;
+  TmaKernelFn fn;
+};
+
+template <int TX, int TY, int S, int MODE>
+TmaVariant tma_variant() {
+  return TmaVariant{TX, TY, S, MODE, tma_smem_bytes<TX, TY, S, MODE>(), TmaGeom<TX, TY, MODE>::THREADS,
+                    &fdtd_step_tma_kernel<TX, TY, S, MODE>};
+}
+
+const std::vector<TmaVariant>& tma_variants() {
+  static const std::vector<TmaVariant> v = {
+      tma_variant<64, 7, 4, MODE_WINDOW>(),  tma_variant<64, 8, 4, MODE_WINDOW>(),
+      tma_variant<64, 16, 3, MODE_WINDOW>(), tma_variant<64, 4, 6, MODE_WINDOW>(),
+      tma_variant<64, 8, 3, MODE_WINDOW>(),  tma_variant<64, 4, 4, MODE_FULL>()};
+  return v;
+}
+
+const TmaVariant* find_variant(int tx, int ty, int stages, int mode) {
+  for (auto& v : tma_variants())
+    if (v.tx == tx && v.ty == ty && v.stages == stages && v.mode == mode) return &v;
+  return nullptr;
+}
+
+PFN_cuTensorMapEncodeTiled_v12000 get_encode_fn() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  if (!fn) {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    CK(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q));
+    if (q != cudaDriverEntryPointSuccess || !p) throw ArgError{FDTD_ERR_CUDA, "cuTensorMapEncodeTiled unavailable"};
+    fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  }
+  return fn;
+}
+
+// Tiled tensor map over a field group of simulation s: dims (x, y, z) and,
+// for rank 5, (component, buffer) with the given element strides.
+void encode_map(CUtensorMap* m, const void* base, CUtensorMapDataType type, int elem, const fdtd_sim* s, int rank,
+                int box_x, int box_y, int ncomp, size_t comp_stride, size_t buf_stride) {
+  const cuuint64_t dims[5] = {cuuint64_t(s->pitch), cuuint64_t(s->ny), cuuint64_t(s->nz), cuuint64_t(ncomp), 2};
+  const cuuint64_t strides[4] = {cuuint64_t(s->pitch) * elem, cuuint64_t(s->pitch) * s->ny * elem,
+                                 cuuint64_t(comp_stride) * elem, cuuint64_t(buf_stride) * elem};
+  const cuuint32_t box[5] = {cuuint32_t(box_x), cuuint32_t(box_y), 1, cuuint32_t(ncomp), 1};
+  const cuuint32_t estr[5] = {1, 1, 1, 1, 1};
+  CUresult r = get_encode_fn()(m, type, cuuint32_t(rank), const_cast<void*>(base), dims, strides, box, estr,
+                               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                               CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) throw ArgError{FDTD_ERR_CUDA, "cuTensorMapEncodeTiled failed: " + std::to_string(int(r))};
+}
+
+void encode_maps(TmaMaps& m, const fdtd_sim* s, const TmaVariant& v) {
+  std::memset(&m, 0, sizeof(m));
+  const auto F = CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
+  const int tx = v.tx, ty = v.ty;
+  const int sew = v.mode == MODE_FULL ? tx + 4 : kSplitWin, shw = v.mode == MODE_FULL ? tx : kSplitWin;
+  const size_t N = s->cells_padded;
+  // fields: [buffer][ex ey ez hx hy hz][cells]; splits: [buffer][6 E splits, 6 H splits][cells]
+  encode_map(&m.E, s->fields.p, F, 4, s, 5, tx + 4, ty + 1, 3, N, 6 * N);
+  encode_map(&m.H, s->fields.p + 3 * N, F, 4, s, 5, tx + 8, ty + 2, 3, N, 6 * N);
+  if (s->splits.n) {
+    encode_map(&m.Es, s->splits.p, F, 4, s, 5, sew, ty + 1, 6, N, 12 * N);
+    encode_map(&m.Hs, s->splits.p + 6 * N, F, 4, s, 5, shw, ty, 6, N, 12 * N);
+  }
+  encode_map(&m.ids, s->mat.p, CU_TENSOR_MAP_DATA_TYPE_UINT16, 2, s, 3, tx + 8, ty + 1, 1, 0, 0);
+}
+
+// Tiles of one kernel class with everything one launch of that class needs.
+struct TileClass {
+  const TmaVariant* v = nullptr;
+  std::vector<TileDesc> host_tiles;
+  std::vector<TmaMaps> host_maps;
+  DevBuf<TmaMaps> d_maps;
+  DevBuf<SimDev> d_sims;
+  DevBuf<TileDesc> d_tiles;
+  DevBuf<unsigned> d_counter;
+  int n_tiles = 0, grid = 0;
+  void reset() {
+    v = nullptr;
+    host_tiles.clear();
+    host_maps.clear();
+    d_maps.free();
+    d_sims.free();
+    d_tiles.free();
+    d_counter.free();
+    n_tiles = grid = 0;
+  }
+};
+
 struct Engine {
   std::vector<fdtd_sim*> sims;
-  DevBuf<SimDev> d_sims;
-  DevBuf<int4> d_tiles;
+  KernelConfig cfg;
+  TileClass cls[2];        // 0: ordinary tiles (x-PML in split windows), 1: y/z-PML slabs (all split)
+  DevBuf<SimDev> d_sims;   // plain kernel
+  DevBuf<int4> d_tiles;    // plain kernel
+  DevBuf<int> d_err;
   int n_tiles = 0;
+  int grid = 0;
+  int zchunk_used = 0;
   cudaStream_t own_stream = nullptr;
   cudaStream_t ext_stream = nullptr;
   cudaGraphExec_t graph = nullptr;
@@ -157,23 +278,145 @@ struct Engine {
     if (own_stream) cudaStreamDestroy(own_stream);
   }
 
+  void reset_graph() {
+    if (graph) cudaGraphExecDestroy(graph);
+    graph = nullptr;
+    graph_nt = -1;
+  }
+
+  // Cut [x0,x1) x [y0,y1) x [z0,z1) of simulation `si` into tiles of (tx, ty, zc).
+  static void tile_region(std::vector<TileDesc>& out, int si, int x0, int x1, int y0, int y1, int z0, int z1, int tx,
+                          int ty, int zc) {
+    for (int z = z0; z < z1; z += zc)
+      for (int y = y0; y < y1; y += ty)
+        for (int x = x0; x < x1; x += tx)
+          out.push_back(TileDesc{si, x, y, z, std::min(z1, z + zc), std::min(x1, x + tx), std::min(y1, y + ty), -1});
+  }
+
   void build_tiles() {
-    std::vector<int4> tiles;
+    reset_graph();
+    int dev = 0, n_sm = 148;
+    CK(cudaGetDevice(&dev));
+    CK(cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev));
+    if (!d_err.n) {
+      d_err.alloc(1);
+      CK(cudaMemset(d_err.p, 0, sizeof(int)));
+    }
+    if (cfg.variant == 1) {
+      const TmaVariant* vv[2] = {find_variant(64, cfg.ty, cfg.stages, MODE_WINDOW), find_variant(64, 4, 4, MODE_FULL)};
+      if (!vv[0]) throw ArgError{FDTD_ERR_ARG, "No TMA kernel instantiated for this tile height / stage count."};
+      int per_sm[2];
+      for (int k = 0; k < 2; ++k) {
+        cls[k].reset();
+        cls[k].v = vv[k];
+        CK(cudaFuncSetAttribute(reinterpret_cast<const void*>(vv[k]->fn),
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, vv[k]->smem));
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[k], reinterpret_cast<const void*>(vv[k]->fn),
+                                                         vv[k]->threads, vv[k]->smem));
+        if (per_sm[k] < 1) throw ArgError{FDTD_ERR_LIMIT, "TMA kernel does not fit on an SM."};
+      }
+      const int ty = cfg.ty;
+      std::vector<Box3> cores(sims.size());
+      std::vector<std::unique_ptr<GradedIndex>> gidx(sims.size());
+      int64_t cols = 0;
+      for (size_t i = 0; i < sims.size(); ++i) {
+        gidx[i] = std::make_unique<GradedIndex>(sims[i]->grid);
+        cores[i] = core_box(*gidx[i], 4, 8);
+        const int nyc = cores[i].empty() ? 0 : cores[i].y1 - cores[i].y0;
+        cols += int64_t((sims[i]->nx + 63) / 64) * ((nyc + ty - 1) / ty);
+      }
+      const int64_t slots = int64_t(per_sm[0]) * n_sm;
+      zchunk_used = 1 << 30;
+      for (size_t i = 0; i < sims.size(); ++i) {
+        fdtd_sim* s = sims[i];
+        const Box3& c = cores[i];
+        const GradedIndex& gi = *gidx[i];
+        int zc = cfg.zchunk;
+        if (zc <= 0) {
+          // about 8 tiles per resident block, chunks of at least 8 planes
+          const int64_t chunks = std::max<int64_t>(1, (slots * 8 + std::max<int64_t>(cols, 1) - 1) /
+                                                           std::max<int64_t>(cols, 1));
+          zc = int(std::max<int64_t>(8, ((c.empty() ? s->nz : c.z1 - c.z0) + chunks - 1) / chunks));
+        }
+        zchunk_used = std::min(zchunk_used, zc);
+        const int si = int(i);
+        for (int k = 0; k < 2; ++k) {
+          cls[k].host_maps.emplace_back();
+          encode_maps(cls[k].host_maps.back(), s, *vv[k]);
+        }
+        if (c.empty()) {
+          tile_region(cls[1].host_tiles, si, 0, s->nx, 0, s->ny, 0, s->nz, 64, 4, zc);
+          continue;
+        }
+        // ordinary tiles over all x; graded cells of their E region (the x-PML)
+        // must fit one 16-column window, otherwise the tile goes to the full class
+        std::vector<TileDesc> ord;
+        tile_region(ord, si, 0, s->nx, c.y0, c.y1, c.z0, c.z1, 64, ty, zc);
+        for (TileDesc t : ord) {
+          int gmin = 1 << 30, gmax = -1;
+          if (gi.count(t.x0 - 4, t.x0 + 64, t.y0 - 1, t.y1, t.z0 - 1, t.z1) > 0)
+            for (int x = std::max(0, t.x0 - 4); x < std::min(s->nx, t.x0 + 64); ++x)
+              if (gi.count(x, x + 1, t.y0 - 1, t.y1, t.z0 - 1, t.z1) > 0) {
+                gmin = std::min(gmin, x);
+                gmax = std::max(gmax, x);
+              }
+          if (gmax < 0) {
+            t.wx0 = -1;
+            cls[0].host_tiles.push_back(t);
+          } else {
+            const int w0 = gmin / 4 * 4;
+            if (gmax < w0 + kSplitWin) {
+              t.wx0 = w0;
+              cls[0].host_tiles.push_back(t);
+            } else {
+              tile_region(cls[1].host_tiles, si, t.x0, t.x1, t.y0, t.y1, t.z0, t.z1, 64, 4, zc);
+            }
+          }
+        }
+        // y- and z-PML slabs
+        tile_region(cls[1].host_tiles, si, 0, s->nx, 0, s->ny, 0, c.z0, 64, 4, zc);
+        tile_region(cls[1].host_tiles, si, 0, s->nx, 0, s->ny, c.z1, s->nz, 64, 4, zc);
+        tile_region(cls[1].host_tiles, si, 0, s->nx, 0, c.y0, c.z0, c.z1, 64, 4, zc);
+        tile_region(cls[1].host_tiles, si, 0, s->nx, c.y1, s->ny, c.z0, c.z1, 64, 4, zc);
+      }
+      n_tiles = 0;
+      grid = 0;
+      for (int k = 0; k < 2; ++k) {
+        TileClass& t = cls[k];
+        t.n_tiles = int(t.host_tiles.size());
+        if (!t.n_tiles) continue;
+        t.d_maps.alloc(t.host_maps.size());
+        CK(cudaMemcpy(t.d_maps.p, t.host_maps.data(), t.host_maps.size() * sizeof(TmaMaps), cudaMemcpyHostToDevice));
+        std::vector<SimDev> devs;
+        for (size_t i = 0; i < sims.size(); ++i) {
+          devs.push_back(sims[i]->dev);
+          devs.back().maps = t.d_maps.p + i;
+        }
+        t.d_sims.alloc(devs.size());
+        CK(cudaMemcpy(t.d_sims.p, devs.data(), devs.size() * sizeof(SimDev), cudaMemcpyHostToDevice));
+        t.d_tiles.alloc(t.host_tiles.size());
+        CK(cudaMemcpy(t.d_tiles.p, t.host_tiles.data(), t.host_tiles.size() * sizeof(TileDesc),
+                      cudaMemcpyHostToDevice));
+        t.d_counter.alloc(1);
+        t.grid = int(std::min<int64_t>(t.n_tiles, int64_t(per_sm[k]) * n_sm));
+        n_tiles += t.n_tiles;
+        grid += t.grid;
+      }
+      return;
+    }
+    // plain kernel: 31 x 7 tiles, z cut into chunks
     std::vector<SimDev> devs;
-    // xy tiles of all simulations first, then cut z into chunks so one step
-    // has enough blocks to fill 148 SMs several times over.
+    for (auto* s : sims) devs.push_back(s->dev);
+    std::vector<int4> tiles;
     int64_t xy_tiles = 0;
     for (auto* s : sims) xy_tiles += int64_t((s->nx + kTileX - 1) / kTileX) * ((s->ny + kTileY - 1) / kTileY);
-    int dev = 0, n_sm = 148;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
     const int64_t want = int64_t(n_sm) * 8;
     for (size_t i = 0; i < sims.size(); ++i) {
       fdtd_sim* s = sims[i];
-      devs.push_back(s->dev);
       int chunks = int(std::max<int64_t>(1, (want + xy_tiles - 1) / std::max<int64_t>(xy_tiles, 1)));
       chunks = std::min(chunks, std::max(1, s->nz / 8));
-      const int zlen = (s->nz + chunks - 1) / chunks;
+      const int zlen = cfg.zchunk > 0 ? cfg.zchunk : (s->nz + chunks - 1) / chunks;
+      zchunk_used = zlen;
       for (int z0 = 0; z0 < s->nz; z0 += zlen)
         for (int y0 = 0; y0 < s->ny; y0 += kTileY)
           for (int x0 = 0; x0 < s->nx; x0 += kTileX) {
@@ -181,11 +424,28 @@ struct Engine {
             tiles.push_back(make_int4(int(i), x0 | (y0 << 16), z0 | (z1 << 16), 0));
           }
     }
+    grid = int(tiles.size());
     d_sims.alloc(devs.size());
     CK(cudaMemcpy(d_sims.p, devs.data(), devs.size() * sizeof(SimDev), cudaMemcpyHostToDevice));
     d_tiles.alloc(tiles.size());
     CK(cudaMemcpy(d_tiles.p, tiles.data(), tiles.size() * sizeof(int4), cudaMemcpyHostToDevice));
     n_tiles = int(tiles.size());
+  }
+
+  void launch_step(cudaStream_t st, int n) {
+    if (cfg.variant == 1) {
+      for (int k = 0; k < 2; ++k) {
+        TileClass& t = cls[k];
+        if (!t.n_tiles) continue;
+        const unsigned base = unsigned(n) * unsigned(t.n_tiles + t.grid);
+        t.v->fn<<<t.grid, t.v->threads, t.v->smem, st>>>(t.d_sims.p, t.d_tiles.p, t.n_tiles, n, t.d_counter.p, base,
+                                                          d_err.p);
+        CK(cudaGetLastError());
+      }
+    } else {
+      fdtd_step_kernel<kTileY><<<n_tiles, dim3(32, kBlockY), 0, st>>>(d_sims.p, d_tiles.p, n);
+      CK(cudaGetLastError());
+    }
   }
 
   // Enqueue one full run of nt steps on stream st (used for capture and for
@@ -199,11 +459,11 @@ struct Engine {
       for (size_t m = 0; m < s->monitors.size(); ++m)
         CK(cudaMemsetAsync(s->mon_out[m]->p, 0, s->mon_out[m]->n, st));
     }
-    const dim3 block(32, kBlockY);
+    for (auto& t : cls)
+      if (t.d_counter.n) CK(cudaMemsetAsync(t.d_counter.p, 0, sizeof(unsigned), st));
     int dft_from = 0;
     for (int n = 0; n < nt; ++n) {
-      fdtd_step_kernel<kTileY><<<n_tiles, block, 0, st>>>(d_sims.p, d_tiles.p, n);
-      CK(cudaGetLastError());
+      launch_step(st, n);
       ++step_launches;
       for (auto* s : sims)
         if (!s->monitors.empty()) {
@@ -228,10 +488,7 @@ struct Engine {
     init();
     cudaStream_t st = stream();
     if (graph_nt != nt) {
-      if (graph) {
-        cudaGraphExecDestroy(graph);
-        graph = nullptr;
-      }
+      reset_graph();
       cudaStream_t cap;
       CK(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
       cudaGraph_t g = nullptr;
@@ -241,7 +498,7 @@ struct Engine {
         CK(cudaStreamEndCapture(cap, &g));
         CK(cudaGraphInstantiate(&graph, g, 0));
       } catch (...) {
-        cudaGraph_t dummy;
+        cudaGraph_t dummy = nullptr;
         cudaStreamEndCapture(cap, &dummy);
         if (dummy) cudaGraphDestroy(dummy);
         if (g) cudaGraphDestroy(g);
@@ -265,6 +522,15 @@ struct Engine {
       CK(cudaEventElapsedTime(&ms, ev0, ev1));
       last_ms = ms;
       timing_pending = false;
+    }
+    if (d_err.n) {
+      int e = 0;
+      CK(cudaMemcpy(&e, d_err.p, sizeof(int), cudaMemcpyDeviceToHost));
+      if (e) {
+        CK(cudaMemset(d_err.p, 0, sizeof(int)));
+        throw ArgError{FDTD_ERR_DEVICE, "step kernel gave up waiting for a TMA plane load (code " +
+                                            std::to_string(e) + ")"};
+      }
     }
   }
 };
@@ -402,6 +668,11 @@ void fill_stats(fdtd_sim* s, const Engine* e) {
   st.h_split_cells = s->grid.h_split_cells;
   st.compile_ms = s->grid.compile_ms;
   if (e) {
+    st.variant = e->cfg.variant;
+    st.tile_y = e->cfg.variant == 1 ? e->cfg.ty : kTileY;
+    st.stages = e->cfg.variant == 1 ? e->cfg.stages : 0;
+    st.zchunk = e->zchunk_used;
+    st.grid = e->grid;
     st.n_tiles = e->n_tiles;
     st.step_launches = e->step_launches;
     st.dft_launches = e->dft_launches;
@@ -440,6 +711,7 @@ int coef_index(const char* name) {
 struct fdtd_batch {
   std::vector<fdtd_sim*> sims;
   Engine engine;
+  bool dirty = true;
   std::string err;
   fdtd_stats stats{};
 };
@@ -591,6 +863,25 @@ int fdtd_get_material_table(fdtd_sim* s, uint16_t* ids, int64_t n_ids, uint32_t*
   });
 }
 
+int fdtd_set_kernel(fdtd_sim* s, int variant, int tile_y, int stages, int zchunk) {
+  if (!s) return FDTD_ERR_ARG;
+  return guarded(&s->err, [&] {
+    if (variant != 0 && variant != 1) throw ArgError{FDTD_ERR_ARG, "variant must be 0 (plain) or 1 (tma)"};
+    KernelConfig c;
+    c.variant = variant;
+    c.ty = tile_y;
+    c.stages = stages;
+    c.zchunk = zchunk;
+    if (variant == 1) {
+      bool found = false;
+      found = find_variant(64, tile_y, stages, MODE_WINDOW) != nullptr;
+      if (!found) throw ArgError{FDTD_ERR_ARG, "No TMA kernel instantiated for this tile height / stage count."};
+    }
+    s->cfg = c;
+    s->engine.reset();
+  });
+}
+
 int fdtd_set_stream(fdtd_sim* s, void* stream) {
   if (!s) return FDTD_ERR_ARG;
   s->ext_stream = static_cast<cudaStream_t>(stream);
@@ -607,6 +898,7 @@ int fdtd_run_async(fdtd_sim* s, int nt) {
     if (rebuild) {
       s->engine = std::make_unique<Engine>();
       s->engine->sims = {s};
+      s->engine->cfg = s->cfg;
       s->engine->ext_stream = s->ext_stream;
       s->engine->build_tiles();
     }
@@ -696,8 +988,26 @@ int fdtd_batch_create(fdtd_sim* const* sims, int n_sims, fdtd_batch** out) {
     b->sims.push_back(sims[i]);
   }
   b->engine.sims = b->sims;
+  b->engine.cfg = default_config();
   *out = b;
   return FDTD_OK;
+}
+
+int fdtd_batch_set_kernel(fdtd_batch* b, int variant, int tile_y, int stages, int zchunk) {
+  if (!b) return FDTD_ERR_ARG;
+  return guarded(&b->err, [&] {
+    if (variant != 0 && variant != 1) throw ArgError{FDTD_ERR_ARG, "variant must be 0 (plain) or 1 (tma)"};
+    if (variant == 1) {
+      bool found = false;
+      found = find_variant(64, tile_y, stages, MODE_WINDOW) != nullptr;
+      if (!found) throw ArgError{FDTD_ERR_ARG, "No TMA kernel instantiated for this tile height / stage count."};
+    }
+    b->engine.cfg.variant = variant;
+    b->engine.cfg.ty = tile_y;
+    b->engine.cfg.stages = stages;
+    b->engine.cfg.zchunk = zchunk;
+    b->dirty = true;
+  });
 }
 
 int fdtd_batch_set_stream(fdtd_batch* b, void* stream) {
@@ -710,7 +1020,8 @@ int fdtd_batch_run(fdtd_batch* b, int nt) {
   if (!b) return FDTD_ERR_ARG;
   return guarded(&b->err, [&] {
     if (nt < 1) throw ArgError{FDTD_ERR_ARG, "nt must be positive."};
-    bool rebuild = b->engine.graph_nt != nt || b->engine.n_tiles == 0;
+    bool rebuild = b->engine.graph_nt != nt || b->engine.n_tiles == 0 || b->dirty;
+    b->dirty = false;
     for (auto* s : b->sims) {
       if (!s->prepared || s->prepared_nt != nt) rebuild = true;
       try {
@@ -730,6 +1041,11 @@ int fdtd_batch_run(fdtd_batch* b, int nt) {
     fdtd_stats& st = b->stats;
     st = fdtd_stats{};
     st.nt = nt;
+    st.variant = b->engine.cfg.variant;
+    st.tile_y = b->engine.cfg.variant == 1 ? b->engine.cfg.ty : kTileY;
+    st.stages = b->engine.cfg.variant == 1 ? b->engine.cfg.stages : 0;
+    st.zchunk = b->engine.zchunk_used;
+    st.grid = b->engine.grid;
     st.n_tiles = b->engine.n_tiles;
     st.step_launches = b->engine.step_launches;
     st.dft_launches = b->engine.dft_launches;

@@ -67,6 +67,64 @@ using RowMap = std::unordered_map<Row, uint32_t, RowHash, RowEq>;
 
 }  // namespace
 
+GradedIndex::GradedIndex(const CompiledGrid& g) : nx(g.nx), ny(g.ny), nz(g.nz) {
+  // summed-volume table of graded cells, indexed [x][y][z] with a zero border
+  sy_ = nz + 1;
+  sx_ = int64_t(ny + 1) * sy_;
+  sv_.assign(size_t(nx + 1) * sx_, 0);
+  for (int x = 0; x < nx; ++x)
+    for (int y = 0; y < ny; ++y)
+      for (int z = 0; z < nz; ++z) {
+        const uint32_t f = g.rows[g.ids[(size_t(x) * ny + y) * nz + z]].w[R_FLAGS];
+        const int32_t v = (f & kFlagGraded) ? 1 : 0;
+        const int64_t i = (x + 1) * sx_ + (y + 1) * sy_ + (z + 1);
+        sv_[i] = v + sv_[i - sx_] + sv_[i - sy_] + sv_[i - 1] - sv_[i - sx_ - sy_] - sv_[i - sx_ - 1] -
+                 sv_[i - sy_ - 1] + sv_[i - sx_ - sy_ - 1];
+      }
+}
+
+int64_t GradedIndex::count(int x0, int x1, int y0, int y1, int z0, int z1) const {
+  x0 = std::max(x0, 0); y0 = std::max(y0, 0); z0 = std::max(z0, 0);
+  x1 = std::min(x1, nx); y1 = std::min(y1, ny); z1 = std::min(z1, nz);
+  if (x1 <= x0 || y1 <= y0 || z1 <= z0) return 0;
+  auto at = [&](int x, int y, int z) { return int64_t(sv_[x * sx_ + y * sy_ + z]); };
+  return at(x1, y1, z1) - at(x0, y1, z1) - at(x1, y0, z1) - at(x1, y1, z0) + at(x0, y0, z1) + at(x0, y1, z0) +
+         at(x1, y0, z0) - at(x0, y0, z0);
+}
+
+Box3 core_box(const GradedIndex& gi, int halo_x, int align) {
+  const int nx = gi.nx, ny = gi.ny, nz = gi.nz;
+  auto count = [&](int x0, int x1, int y0, int y1, int z0, int z1) { return gi.count(x0, x1, y0, y1, z0, z1); };
+  Box3 b{0, nx, 0, ny, 0, nz};
+  for (;;) {
+    const int ex0 = b.x0 - halo_x, ey0 = b.y0 - 1, ez0 = b.z0 - 1;
+    if (b.empty()) return Box3{};
+    if (count(ex0, b.x1, ey0, b.y1, ez0, b.z1) == 0) break;
+    // shrink the face whose outermost layer of the extended box holds most
+    // graded cells (layers clipped to the grid)
+    const int lx = std::max(ex0, 0), ly = std::max(ey0, 0), lz = std::max(ez0, 0);
+    const int64_t c[6] = {
+        count(lx, lx + 1, ey0, b.y1, ez0, b.z1), count(b.x1 - 1, b.x1, ey0, b.y1, ez0, b.z1),
+        count(ex0, b.x1, ly, ly + 1, ez0, b.z1), count(ex0, b.x1, b.y1 - 1, b.y1, ez0, b.z1),
+        count(ex0, b.x1, ey0, b.y1, lz, lz + 1), count(ex0, b.x1, ey0, b.y1, b.z1 - 1, b.z1)};
+    int best = 0;
+    for (int k = 1; k < 6; ++k)
+      if (c[k] > c[best]) best = k;
+    switch (best) {
+      case 0: b.x0 += 1; break;
+      case 1: b.x1 -= 1; break;
+      case 2: b.y0 += 1; break;
+      case 3: b.y1 -= 1; break;
+      case 4: b.z0 += 1; break;
+      default: b.z1 -= 1; break;
+    }
+  }
+  b.x0 = (b.x0 + align - 1) / align * align;
+  if (b.x1 != nx) b.x1 = b.x1 / align * align;
+  if (b.empty()) return Box3{};
+  return b;
+}
+
 float row_coefficient(const Row& r, int c) {
   float f;
   std::memcpy(&f, &r.w[kSlotOf[c]], 4);
@@ -182,12 +240,13 @@ bool compile_grid(int nx, int ny, int nz, const float* const* coef, const std::v
             }
           }
           uint32_t flags = 0;
-          if (r.w[R_CA_EX_Y] != r.w[R_CA_EX_Z] || r.w[R_CA_EY_Z] != r.w[R_CA_EY_X] ||
-              r.w[R_CA_EZ_X] != r.w[R_CA_EZ_Y] || (src_mask & 7u))
-            flags |= kFlagESplit;
-          if (r.w[R_DA_HX_Y] != r.w[R_DA_HX_Z] || r.w[R_DA_HY_Z] != r.w[R_DA_HY_X] ||
-              r.w[R_DA_HZ_X] != r.w[R_DA_HZ_Y] || (src_mask & 0x38u))
-            flags |= kFlagHSplit;
+          const bool e_diff = r.w[R_CA_EX_Y] != r.w[R_CA_EX_Z] || r.w[R_CA_EY_Z] != r.w[R_CA_EY_X] ||
+                              r.w[R_CA_EZ_X] != r.w[R_CA_EZ_Y];
+          const bool h_diff = r.w[R_DA_HX_Y] != r.w[R_DA_HX_Z] || r.w[R_DA_HY_Z] != r.w[R_DA_HY_X] ||
+                              r.w[R_DA_HZ_X] != r.w[R_DA_HZ_Y];
+          if (e_diff || (src_mask & 7u)) flags |= kFlagESplit;
+          if (h_diff || (src_mask & 0x38u)) flags |= kFlagHSplit;
+          if (e_diff || h_diff) flags |= kFlagGraded;
           flags |= uint32_t(probe_count) << 16;
           e_split[t] += (flags & kFlagESplit) ? 1 : 0;
           h_split[t] += (flags & kFlagHSplit) ? 1 : 0;

@@ -31,6 +31,9 @@ enum RowSlot : int {
 };
 constexpr uint32_t kFlagESplit = 1u;
 constexpr uint32_t kFlagHSplit = 2u;
+// the cell's split coefficients differ (a PML cell), as opposed to a cell that
+// is split only because it carries a soft source
+constexpr uint32_t kFlagGraded = 4u;
 
 struct Row {
   uint32_t w[kRowWords];
@@ -67,5 +70,30 @@ bool compile_grid(int nx, int ny, int nz, const float* const* coef, const std::v
 // Expands a row back to the coefficient the reference kernel would apply to
 // split `c` (coefficient index into kCoefNames) -- used by tests.
 float row_coefficient(const Row& r, int c);
+
+struct Box3 {
+  int x0 = 0, x1 = 0, y0 = 0, y1 = 0, z0 = 0, z1 = 0;
+  bool empty() const { return x1 <= x0 || y1 <= y0 || z1 <= z0; }
+};
+
+// Counts graded (PML) split cells in boxes of a compiled grid in O(1) through
+// a summed-volume table.
+class GradedIndex {
+ public:
+  explicit GradedIndex(const CompiledGrid& g);
+  // cells with the graded flag in [x0,x1) x [y0,y1) x [z0,z1), clipped to the grid
+  int64_t count(int x0, int x1, int y0, int y1, int z0, int z1) const;
+  int nx, ny, nz;
+
+ private:
+  std::vector<int32_t> sv_;
+  int64_t sx_, sy_;
+};
+
+// The "core" of a grid: a box whose cells, together with the halo the fused
+// kernel recomputes (x0-halo_x .. x0-1, y0-1, z0-1), hold no graded (PML)
+// split cell. x0 is a multiple of `align`, x1 one too unless it is nx.
+// Everything outside it is the PML shell. Empty when no such box exists.
+Box3 core_box(const GradedIndex& gi, int halo_x, int align);
 
 }  // namespace rfn

@@ -39,7 +39,10 @@ constexpr int kBlockY = kTileY + 1;
 
 constexpr uint32_t kESplit = 1u, kHSplit = 2u;
 
+struct TmaMaps;
+
 struct SimDev {
+  const TmaMaps* maps;    // tensor maps of the TMA kernel (set per engine)
   int nx, ny, nz, pitch;  // cells; pitch = floats per x row
   int plane;              // ny * pitch
   int nt;
@@ -56,6 +59,28 @@ struct SimDev {
 };
 
 __device__ __forceinline__ float ldf(const float* p, int i, bool ok) { return ok ? __ldg(p + i) : 0.0f; }
+
+// The update arithmetic with its rounding order fixed by intrinsics, so every
+// kernel variant produces the same bits (the compiler may otherwise contract
+// a*b + c*d either way).
+//   E split      s' = Ca s + Cb d                    (solver.cu:154-184)
+//   E unsplit    f' = (Ca f + Cb1 d1) + Cb2 d2        (sum of the two splits)
+//   H term       g  = Db2 e2 - Db1 e1                  (solver.cu:329-350)
+//   H split      s' = Da s + g
+//   H unsplit    f' = (Da f + g1) + g2
+__device__ __forceinline__ float upd_e_split(float ca, float s, float cb, float d) {
+  return __fmaf_rn(cb, d, __fmul_rn(ca, s));
+}
+__device__ __forceinline__ float upd_e(float ca, float f, float cb1, float d1, float cb2, float d2) {
+  return __fmaf_rn(cb2, d2, __fmaf_rn(cb1, d1, __fmul_rn(ca, f)));
+}
+__device__ __forceinline__ float h_term(float b2, float e2, float b1, float e1) {
+  return __fmaf_rn(b2, e2, -__fmul_rn(b1, e1));
+}
+__device__ __forceinline__ float upd_h_split(float da, float s, float g) { return __fmaf_rn(da, s, g); }
+__device__ __forceinline__ float upd_h(float da, float f, float g1, float g2) {
+  return __fadd_rn(__fmaf_rn(da, f, g1), g2);
+}
 
 template <int TY>
 __global__ void __launch_bounds__(32 * (TY + 1))
@@ -129,17 +154,17 @@ fdtd_step_kernel(const SimDev* __restrict__ sims, const int4* __restrict__ tiles
       const float dhy_x = hy_xn - hy_c, dhx_y = hx_yn - hx_c;
       if (!(flags & kESplit)) {
         // interior: both splits share Ca, so f' = Ca f + Cb1 d1 + Cb2 d2
-        ex = a.x * __ldg(Ex + idx) + a.y * dhz_y + a.w * dhy_z;
-        ey = b.x * __ldg(Ey + idx) + b.y * dhx_z + b.w * dhz_x;
-        ez = d.x * __ldg(Ez + idx) + d.y * dhy_x + d.w * dhx_y;
+        ex = upd_e(a.x, __ldg(Ex + idx), a.y, dhz_y, a.w, dhy_z);
+        ey = upd_e(b.x, __ldg(Ey + idx), b.y, dhx_z, b.w, dhz_x);
+        ez = upd_e(d.x, __ldg(Ez + idx), d.y, dhy_x, d.w, dhx_y);
       } else {
         const float* const* Es = S.Es[cur];
-        float s0 = a.x * __ldg(Es[0] + idx) + a.y * dhz_y;  // ex_y
-        float s1 = a.z * __ldg(Es[1] + idx) + a.w * dhy_z;  // ex_z
-        float s2 = b.x * __ldg(Es[2] + idx) + b.y * dhx_z;  // ey_z
-        float s3 = b.z * __ldg(Es[3] + idx) + b.w * dhz_x;  // ey_x
-        float s4 = d.x * __ldg(Es[4] + idx) + d.y * dhy_x;  // ez_x
-        float s5 = d.z * __ldg(Es[5] + idx) + d.w * dhx_y;  // ez_y
+        float s0 = upd_e_split(a.x, __ldg(Es[0] + idx), a.y, dhz_y);  // ex_y
+        float s1 = upd_e_split(a.z, __ldg(Es[1] + idx), a.w, dhy_z);  // ex_z
+        float s2 = upd_e_split(b.x, __ldg(Es[2] + idx), b.y, dhx_z);  // ey_z
+        float s3 = upd_e_split(b.z, __ldg(Es[3] + idx), b.w, dhz_x);  // ey_x
+        float s4 = upd_e_split(d.x, __ldg(Es[4] + idx), d.y, dhy_x);  // ez_x
+        float s5 = upd_e_split(d.z, __ldg(Es[5] + idx), d.w, dhx_y);  // ez_y
         const int np = int(flags >> 16);
         if (np) {
           // soft sources: s1 += v; s2 += v; f = s1 + s2 (solver.cu:459-488)
@@ -148,15 +173,15 @@ fdtd_step_kernel(const SimDev* __restrict__ sims, const int4* __restrict__ tiles
             const int2 pe = __ldg(S.cell_probes + first + e);
             if (pe.y < 3 && __ldg(S.is_src + pe.x)) {
               const float v = __ldg(S.src + (size_t)pe.x * S.nt + n);
-              if (pe.y == 0) { s0 += v; s1 += v; }
-              if (pe.y == 1) { s2 += v; s3 += v; }
-              if (pe.y == 2) { s4 += v; s5 += v; }
+              if (pe.y == 0) { s0 = __fadd_rn(s0, v); s1 = __fadd_rn(s1, v); }
+              if (pe.y == 1) { s2 = __fadd_rn(s2, v); s3 = __fadd_rn(s3, v); }
+              if (pe.y == 2) { s4 = __fadd_rn(s4, v); s5 = __fadd_rn(s5, v); }
             }
           }
         }
-        ex = s0 + s1;
-        ey = s2 + s3;
-        ez = s4 + s5;
+        ex = __fadd_rn(s0, s1);
+        ey = __fadd_rn(s2, s3);
+        ez = __fadd_rn(s4, s5);
         if (own && z >= z0) {
           float* const* Eo = S.Es[nxt];
           Eo[0][idx] = s0; Eo[1][idx] = s1; Eo[2][idx] = s2;
@@ -188,25 +213,25 @@ fdtd_step_kernel(const SimDev* __restrict__ sims, const int4* __restrict__ tiles
       const float b2_yz = u.x, da_yx = u.y, b1_yx = u.z, b2_yx = u.w;
       const float da_zx = v6.x, b1_zx = v6.y, b2_zx = v6.z, da_zy = v6.w;
       const float b1_zy = rw7.x, b2_zy = rw7.y;
-      const float gxy = b2_xy * ez - b1_xy * ez_ym;
-      const float gxz = b2_xz * ey - b1_xz * ey_p;
-      const float gyz = b2_yz * ex - b1_yz * ex_p;
-      const float gyx = b2_yx * ez - b1_yx * ez_xm;
-      const float gzx = b2_zx * ey - b1_zx * ey_xm;
-      const float gzy = b2_zy * ex - b1_zy * ex_ym;
+      const float gxy = h_term(b2_xy, ez, b1_xy, ez_ym);
+      const float gxz = h_term(b2_xz, ey, b1_xz, ey_p);
+      const float gyz = h_term(b2_yz, ex, b1_yz, ex_p);
+      const float gyx = h_term(b2_yx, ez, b1_yx, ez_xm);
+      const float gzx = h_term(b2_zx, ey, b1_zx, ey_xm);
+      const float gzy = h_term(b2_zy, ex, b1_zy, ex_ym);
       float hx, hy, hz;
       if (!(flags & kHSplit)) {
-        hx = da_xy * hx_c + gxy + gxz;
-        hy = da_yz * hy_c + gyz + gyx;
-        hz = da_zx * hz_c + gzx + gzy;
+        hx = upd_h(da_xy, hx_c, gxy, gxz);
+        hy = upd_h(da_yz, hy_c, gyz, gyx);
+        hz = upd_h(da_zx, hz_c, gzx, gzy);
       } else {
         const float* const* Hs = S.Hs[cur];
-        float s0 = da_xy * __ldg(Hs[0] + idx) + gxy;
-        float s1 = da_xz * __ldg(Hs[1] + idx) + gxz;
-        float s2 = da_yz * __ldg(Hs[2] + idx) + gyz;
-        float s3 = da_yx * __ldg(Hs[3] + idx) + gyx;
-        float s4 = da_zx * __ldg(Hs[4] + idx) + gzx;
-        float s5 = da_zy * __ldg(Hs[5] + idx) + gzy;
+        float s0 = upd_h_split(da_xy, __ldg(Hs[0] + idx), gxy);
+        float s1 = upd_h_split(da_xz, __ldg(Hs[1] + idx), gxz);
+        float s2 = upd_h_split(da_yz, __ldg(Hs[2] + idx), gyz);
+        float s3 = upd_h_split(da_yx, __ldg(Hs[3] + idx), gyx);
+        float s4 = upd_h_split(da_zx, __ldg(Hs[4] + idx), gzx);
+        float s5 = upd_h_split(da_zy, __ldg(Hs[5] + idx), gzy);
         const int np = int(flags >> 16);
         if (np) {
           const int first = __float_as_int(rw7.w);
@@ -214,15 +239,15 @@ fdtd_step_kernel(const SimDev* __restrict__ sims, const int4* __restrict__ tiles
             const int2 pe = __ldg(S.cell_probes + first + e);
             if (pe.y >= 3 && __ldg(S.is_src + pe.x)) {
               const float v = __ldg(S.src + (size_t)pe.x * S.nt + n);
-              if (pe.y == 3) { s0 += v; s1 += v; }
-              if (pe.y == 4) { s2 += v; s3 += v; }
-              if (pe.y == 5) { s4 += v; s5 += v; }
+              if (pe.y == 3) { s0 = __fadd_rn(s0, v); s1 = __fadd_rn(s1, v); }
+              if (pe.y == 4) { s2 = __fadd_rn(s2, v); s3 = __fadd_rn(s3, v); }
+              if (pe.y == 5) { s4 = __fadd_rn(s4, v); s5 = __fadd_rn(s5, v); }
             }
           }
         }
-        hx = s0 + s1;
-        hy = s2 + s3;
-        hz = s4 + s5;
+        hx = __fadd_rn(s0, s1);
+        hy = __fadd_rn(s2, s3);
+        hz = __fadd_rn(s4, s5);
         float* const* Ho = S.Hs[nxt];
         Ho[0][idx] = s0; Ho[1][idx] = s1; Ho[2][idx] = s2;
         Ho[3][idx] = s3; Ho[4][idx] = s4; Ho[5][idx] = s5;

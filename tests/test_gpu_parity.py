@@ -123,3 +123,27 @@ def test_no_nan_after_long_run(engine_lib):
     se, pe = run_engine(s)
     assert np.isfinite(pe).all()
     assert np.abs(pe).max() > 0
+
+
+def _engine_probe_matrix(s, variant, **kw):
+    co, pr, mo, mem, Nx, Ny, Nz, Nt = s.pack_inputs(gpu=True)
+    sim = _lib.Simulation(Nx, Ny, Nz)
+    sim.set_kernel(variant, **kw)
+    sim.set_coefficients(co)
+    for p in pr:
+        sim.add_probe(p["field"], p["idx"], p["is_source"], p["values"] if p["is_source"] else None)
+    sim.run(Nt)
+    out = sim.probe_values()
+    st = sim.stats()
+    sim.close()
+    return out, st
+
+
+@pytest.mark.parametrize("ty,stages,zchunk", [(7, 4, 0), (8, 3, 5), (4, 6, 0), (16, 3, 7)])
+def test_tma_kernel_bitwise_equals_plain(engine_lib, ty, stages, zchunk):
+    """The TMA-pipelined kernel evaluates the same expressions as the plain one."""
+    s = configs.microstrip(n=(72, 40, 30), n_pml=5, nt=150)
+    a, sa = _engine_probe_matrix(s, 0)
+    b, sb = _engine_probe_matrix(s, 1, tile_y=ty, stages=stages, zchunk=zchunk)
+    assert sa["variant"] == 0 and sb["variant"] == 1
+    assert np.array_equal(a, b)
