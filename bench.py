@@ -1,0 +1,365 @@
+#!/usr/bin/env python
+"""Throughput of the B200 FDTD engine on the bandwidth model.
+
+Workload: 256 x 256 x 128 cells, 8-cell split-field PML on all faces, 64
+seeded dielectric boxes, 4 lumped ports driven by a Gaussian pulse, 16 Ez
+point probes and an FP64 running DFT at 51 frequencies of the port voltages,
+port currents and probes; 5000 Yee time steps. One bench "step" is one full
+simulation of that model (all 5000 time steps).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Prints one JSON line (rank 0). ``value`` is Mcell-updates/s with the model
+resident on the device (the time loop replayed as a CUDA graph on a stream of
+this script, CUDA events around the K simulations, max over ranks);
+``e2e`` is the same metric through the reference-facing call
+(``rfnetwork_b200.cuda_func.solver_run_dft`` on host numpy arrays: coefficient
+compilation, host-to-device copies, the run and the read-back of probes and
+DFT inside the timed region). ``--impl reference`` times the CPU restatement
+of the reference's threaded C++ solver on the host cores instead.
+
+With N > 1 (torchrun) every rank runs its own replica of the model (the
+solver has no cross-GPU exchange); ``value`` is the sum over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import copy
+import datetime
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+GRID = (256, 256, 128)
+N_PML = 8
+NT = 5000
+N_FREQ = 51
+WORKLOAD = "boxes 256x256x128, 8-cell PML, 64 dielectric boxes, 4 ports, 16 Ez probes, 51-freq DFT, 5000 steps"
+METRIC = "Yee Mcell-updates/s"
+UNIT = "Mcell-updates/s"
+FALLBACK_HBM_GBS = 6650.0
+
+SMI_FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+
+def parse_args():
+    ap = argparse.ArgumentParser(description=__doc__.split("\n\n")[0])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
+    ap.add_argument("--nt", type=int, default=NT, help="time steps per simulation")
+    ap.add_argument("--e2e-steps", type=int, default=None, help="end-to-end calls timed (default: --steps)")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+# --------------------------------------------------------------------- model
+
+def build_model(nt: int):
+    from rfnetwork_b200 import configs
+    return configs.boxes(n=GRID, n_pml=N_PML, nt=nt)
+
+
+def dft_spec(s, pr):
+    """Port V/I series of the S-parameter post-processing plus one series per point probe."""
+    from rfnetwork_b200 import configs
+    names, terms = s.dft_series()
+    n_lead = len(pr) - len(s.probes)
+    for i, k in enumerate(s.probes.keys()):
+        if k.startswith("port_"):
+            continue
+        terms.append((len(names), n_lead + i, 1.0))
+        names.append(k)
+    omega = s.dft_omega(configs.boxes_frequencies(N_FREQ))
+    return names, terms, omega
+
+
+def peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return FALLBACK_HBM_GBS, "fallback"
+
+
+# ------------------------------------------------------------------- clocks
+
+class ClockSampler:
+    """nvidia-smi samples of one GPU every 200 ms while the timed region runs."""
+
+    def __init__(self, device_index: int):
+        self.dev = str(device_index)
+        try:  # the physical GPU behind a CUDA_VISIBLE_DEVICES remapping
+            import torch
+            u = str(torch.cuda.get_device_properties(device_index).uuid)
+            self.dev = u if u.startswith("GPU-") else "GPU-" + u
+        except Exception:
+            pass
+        self.proc = None
+        self.path = Path(os.environ.get("TMPDIR", "/tmp")) / f"rfn_clocks_{os.getpid()}.csv"
+
+    def __enter__(self):
+        try:
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={SMI_FIELDS}", "--format=csv,noheader,nounits", "-lms", "200",
+                 "-i", self.dev], stdout=self.fh, stderr=subprocess.DEVNULL)
+        except (OSError, ValueError):
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+            self.fh.close()
+
+    def summary(self):
+        if self.proc is None or not self.path.exists():
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        sm, mx, reasons = [], None, set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for line in self.path.read_text().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for name, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(name)
+        try:
+            self.path.unlink()
+        except OSError:
+            pass
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------- our arm
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+    from rfnetwork_b200 import _lib, configs, cuda_func
+
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local_rank))
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(v: float) -> float:
+        if dist is None:
+            return v
+        t = torch.tensor([v], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    nt = args.nt
+    s = build_model(nt)
+    co, pr, mo, mem, Nx, Ny, Nz, Nt = s.pack_inputs(gpu=True)
+    names, terms, omega = dft_spec(s, pr)
+    cells = Nx * Ny * Nz
+    alg_bytes_step = configs.algorithmic_bytes((Nx, Ny, Nz), N_PML)
+
+    # ---- device-resident arm: the model compiled once, the time loop replayed
+    sim = _lib.Simulation(Nx, Ny, Nz)
+    sim.set_coefficients(co)
+    for p in pr:
+        src = bool(p["is_source"])
+        sim.add_probe(int(p["field"]), p["idx"], src, p["values"][:Nt] if src else None)
+    sim.set_dft(terms, omega)
+    stream = torch.cuda.Stream()
+    sim.set_stream(stream.cuda_stream)
+    for _ in range(max(args.warmup, 0)):
+        sim.run_async(Nt)
+        sim.synchronize()
+    st = sim.stats()
+
+    barrier()
+    evs = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
+    with ClockSampler(local_rank) as clk:
+        evs[0].record(stream)
+        for k in range(args.steps):
+            sim.run_async(Nt)
+            evs[k + 1].record(stream)
+        sim.synchronize()
+        torch.cuda.synchronize()
+    barrier()
+    per_sim_ms = [evs[k].elapsed_time(evs[k + 1]) for k in range(args.steps)]
+    total_ms = max_over_ranks(sum(per_sim_ms))
+    st = sim.stats()
+    launches_per_sim = int(st["step_launches"] + st["dft_launches"])
+    rec = sim.probe_values()
+    finite = bool(np.isfinite(rec).all())
+    sim.close()
+
+    # ---- end to end through the reference-facing call, host arrays in and out
+    e2e_steps = args.e2e_steps if args.e2e_steps is not None else args.steps
+    e2e_s, info = 0.0, {}
+    if e2e_steps > 0:
+        pr_h = copy.deepcopy(pr)
+        cuda_func.solver_run_dft(co, pr_h, mo, Nx, Ny, Nz, Nt, terms, omega)  # warm-up (driver, allocator)
+        barrier()
+        t0 = time.perf_counter()
+        for _ in range(e2e_steps):
+            pr_h = copy.deepcopy(pr)
+            cuda_func.solver_run_dft(co, pr_h, mo, Nx, Ny, Nz, Nt, terms, omega)
+        torch.cuda.synchronize()
+        e2e_s = max_over_ranks(time.perf_counter() - t0)
+        info = cuda_func.last_run_info()
+
+    out = None
+    if rank == 0:
+        hbm, peak_kind = peaks()
+        mean_sim_ms = statistics.fmean(per_sim_ms)
+        step_ms = mean_sim_ms / Nt  # one step-kernel launch per time step (+ the DFT every 256 steps)
+        achieved = alg_bytes_step / (step_ms * 1e-3) / 1e9
+        traffic = None
+        tp = ROOT / "profiles" / "traffic.json"
+        if tp.exists():
+            tj = json.loads(tp.read_text())
+            key = f"variant{st['variant']}"
+            if key in tj:
+                traffic = tj[key]["bytes_per_launch"]
+        value = world * cells * Nt * args.steps / (total_ms * 1e-3) / 1e6
+        out = {
+            "metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(total_ms / args.steps, 3),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic: seeded 64-box dielectric model (eps_r~U[1,10], sigma~U[0,0.05] S/m), "
+                    "Gaussian-pulse ports",
+            "config": {"workload": WORKLOAD, "grid": list(GRID), "n_pml": N_PML, "time_steps": Nt,
+                       "dft_frequencies": N_FREQ, "dft_series": len(names), "probes": len(pr),
+                       "step": f"one full simulation ({Nt} Yee time steps)",
+                       "l2": "inputs larger than L2 (fields+splits+index %.2f GB per replica)"
+                             % ((cells * (48 + 96) + cells * 2) / 1e9),
+                       "parallelism": f"replicas{world}" if world > 1 else "single",
+                       "kernel": {k: st[k] for k in ("variant", "tile_y", "stages", "zchunk", "grid", "n_tiles")}},
+            "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s",
+                         "frac": round(achieved / hbm, 4), "traffic": traffic,
+                         "peak_source": peak_kind,
+                         "algorithmic_bytes_per_launch": alg_bytes_step,
+                         "launch_ms": round(step_ms, 5),
+                         "launch_ms_source": "CUDA events over the timed simulations / time steps"},
+            "e2e": None if e2e_steps <= 0 else {
+                "value": round(world * cells * Nt * e2e_steps / e2e_s / 1e6, 1), "unit": UNIT,
+                "h2d_bytes_per_step": int(info.get("h2d_bytes", 0)),
+                "d2h_bytes_per_step": int(info.get("d2h_bytes", 0)),
+                "s_per_step": round(e2e_s / e2e_steps, 3), "call": "cuda_func.solver_run_dft",
+                "compile_ms": round(float(info.get("compile_ms", 0.0)), 1)},
+            "gpu_launches": launches_per_sim * args.steps,
+            "clocks": clk.summary(),
+            "finite": finite,
+        }
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return out
+
+
+# ----------------------------------------------------------- CPU baseline
+
+def cpu_sample(nt_sample: int, n_threads: int):
+    """Run the CPU restatement of the reference solver on the full grid for nt_sample steps.
+
+    Returns (Mcell-updates/s, seconds)."""
+    from oracle import cpu_engine
+    s = build_model(nt_sample)
+    co, pr, mo, mem, Nx, Ny, Nz, Nt = s.pack_inputs(gpu=False)
+    cpu_engine.build()
+    t0 = time.perf_counter()
+    cpu_engine.solver_run(co, pr, mo, mem, Nx, Ny, Nz, Nt, n_threads, 0)
+    dt = time.perf_counter() - t0
+    return Nx * Ny * Nz * Nt / dt / 1e6, dt
+
+
+def sample_steps(n_threads: int, seconds: float = 10.0) -> int:
+    """Time steps of the full grid that take about `seconds` on the CPU (8..256)."""
+    v, _ = cpu_sample(2, n_threads)
+    cells = GRID[0] * GRID[1] * GRID[2]
+    return int(min(256, max(8, seconds * v * 1e6 / cells)))
+
+
+def cpu_baseline_entry():
+    from oracle import cpu_engine
+    n = cpu_engine.default_threads()
+    nt_sample = sample_steps(n)
+    v, dt = cpu_sample(nt_sample, n)
+    return {"value": round(v, 2), "unit": UNIT, "cores": n, "kind": "port",
+            "sample": f"{nt_sample} time steps of the {GRID[0]}x{GRID[1]}x{GRID[2]} model ({dt:.1f} s)"}
+
+
+def run_reference(args, rank, world):
+    """CPU restatement of the reference's threaded C++ solver (solver.cpp), all usable host threads."""
+    if rank != 0:
+        return None
+    from oracle import cpu_engine
+    n = cpu_engine.default_threads()
+    for _ in range(max(args.warmup, 0)):
+        cpu_sample(2, n)
+    nt_sample = sample_steps(n)
+    vals = []
+    for _ in range(args.steps):
+        v, _dt = cpu_sample(nt_sample, n)
+        vals.append(v)
+    value = statistics.fmean(vals)
+    cells = GRID[0] * GRID[1] * GRID[2]
+    return {
+        "impl": "reference", "metric": METRIC, "value": round(value, 2), "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(cells * args.nt / (value * 1e6) * 1e3, 1),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic: seeded 64-box dielectric model, Gaussian-pulse ports",
+        "config": {"workload": WORKLOAD, "grid": list(GRID), "n_pml": N_PML, "time_steps": args.nt,
+                   "step": f"a sample of {nt_sample} time steps per step; ms_per_step extrapolated to {args.nt}"},
+        "cpu_baseline": {"value": round(value, 2), "unit": UNIT, "cores": n, "kind": "port",
+                         "sample": f"{nt_sample} time steps of the full grid per step"},
+        "e2e": {"value": round(value, 2), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
+def main():
+    args = parse_args()
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    local_rank = int(os.environ.get("LOCAL_RANK", 0))
+    if args.impl == "reference":
+        out = run_reference(args, rank, world)
+    else:
+        out = run_ours(args, rank, world, local_rank)
+        if rank == 0 and world == 1 and not args.no_cpu_baseline:
+            out["cpu_baseline"] = cpu_baseline_entry()
+        elif rank == 0:
+            out["cpu_baseline"] = None
+    if rank == 0 and out is not None:
+        print(json.dumps(out), flush=True)
+
+
+if __name__ == "__main__":
+    main()

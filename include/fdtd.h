@@ -60,6 +60,8 @@ typedef struct fdtd_stats {
   int stages;            /* shared-memory pipeline stages (TMA kernel) */
   int zchunk;            /* z planes per tile */
   int grid;              /* blocks launched per step */
+  int64_t h2d_bytes;     /* host-to-device bytes copied for this simulation so far */
+  int64_t d2h_bytes;     /* device-to-host bytes read back from it so far */
 } fdtd_stats;
 
 /* --------------------------------------------------------------- one grid */

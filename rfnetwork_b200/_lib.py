@@ -33,7 +33,7 @@ class FdtdStats(ctypes.Structure):
         ("n_tiles", ctypes.c_int), ("step_launches", ctypes.c_int64), ("dft_launches", ctypes.c_int64),
         ("last_run_ms", ctypes.c_double), ("compile_ms", ctypes.c_double),
         ("variant", ctypes.c_int), ("tile_y", ctypes.c_int), ("stages", ctypes.c_int), ("zchunk", ctypes.c_int),
-        ("grid", ctypes.c_int),
+        ("grid", ctypes.c_int), ("h2d_bytes", ctypes.c_int64), ("d2h_bytes", ctypes.c_int64),
     ]
 
     def as_dict(self):

@@ -22,6 +22,7 @@
 #include "../../include/fdtd.h"
 #include "fdtd_compile.h"
 #include "fdtd_kernels.cuh"
+#include "fdtd_step_stream.cuh"
 #include "fdtd_step_tma.cuh"
 #include <cudaTypedefs.h>
 
@@ -92,7 +93,7 @@ int threads_for_host() {
 // Kernel selection of an engine: the plain-load kernel (one cell per thread)
 // or the TMA-pipelined kernel with its tile height, stage count and z chunk.
 struct KernelConfig {
-  int variant = 0;  // 0 plain, 1 tma
+  int variant = 0;  // 0 plain, 1 tma (float4 groups), 2 stream (one thread per cell)
   int ty = 7;
   int stages = 4;
   int zchunk = 0;   // 0: pick from the grid size
@@ -100,7 +101,8 @@ struct KernelConfig {
 
 KernelConfig default_config() {
   KernelConfig c;
-  if (const char* v = std::getenv("RFN_FDTD_KERNEL")) c.variant = (std::string(v) == "tma") ? 1 : 0;
+  if (const char* v = std::getenv("RFN_FDTD_KERNEL"))
+    c.variant = std::string(v) == "tma" ? 1 : std::string(v) == "stream" ? 2 : 0;
   if (const char* v = std::getenv("RFN_FDTD_TY")) c.ty = std::atoi(v);
   if (const char* v = std::getenv("RFN_FDTD_STAGES")) c.stages = std::atoi(v);
   if (const char* v = std::getenv("RFN_FDTD_ZCHUNK")) c.zchunk = std::atoi(v);
@@ -149,7 +151,19 @@ struct fdtd_sim {
   cudaStream_t ext_stream = nullptr;
   std::string err;
   fdtd_stats stats{};
+  int64_t h2d_bytes = 0, d2h_bytes = 0;  // bytes copied over PCIe/C2C by this simulation
 };
+
+// Host-to-device copy that counts its bytes on the simulation.
+void h2d(fdtd_sim* s, void* dst, const void* src, size_t bytes) {
+  CK(cudaMemcpy(dst, src, bytes, cudaMemcpyHostToDevice));
+  s->h2d_bytes += int64_t(bytes);
+}
+
+void d2h(fdtd_sim* s, void* dst, const void* src, size_t bytes) {
+  CK(cudaMemcpy(dst, src, bytes, cudaMemcpyDeviceToHost));
+  s->d2h_bytes += int64_t(bytes);
+}
 
 using TmaKernelFn = void (*)(const SimDev*, const TileDesc*, int, int, unsigned*, unsigned, int*);
 
@@ -178,6 +192,41 @@ const TmaVariant* find_variant(int tx, int ty, int stages, int mode) {
   for (auto& v : tma_variants())
     if (v.tx == tx && v.ty == ty && v.stages == stages && v.mode == mode) return &v;
   return nullptr;
+}
+
+using StreamKernelFn = void (*)(const SimDev*, const StreamTile*, int, int, unsigned*, unsigned, int*);
+
+// One instantiation of the streaming step kernel.
+struct StreamVariant {
+  int ty, stages;
+  int smem, threads;
+  StreamKernelFn fn;
+};
+
+template <int TY, int S>
+StreamVariant stream_variant() {
+  return StreamVariant{TY, S, stream_smem_bytes<TY, S>(), StreamGeom<TY>::THREADS, &fdtd_step_stream_kernel<TY, S>};
+}
+
+const std::vector<StreamVariant>& stream_variants() {
+  static const std::vector<StreamVariant> v = {
+      stream_variant<4, 4>(), stream_variant<4, 5>(), stream_variant<6, 3>(), stream_variant<6, 4>(),
+      stream_variant<8, 3>(), stream_variant<8, 4>(), stream_variant<12, 3>()};
+  return v;
+}
+
+const StreamVariant* find_stream_variant(int ty, int stages) {
+  for (auto& v : stream_variants())
+    if (v.ty == ty && v.stages == stages) return &v;
+  return nullptr;
+}
+
+// Whether a (variant, tile height, stages) triple names an instantiated kernel.
+bool kernel_exists(int variant, int ty, int stages) {
+  if (variant == 0) return true;
+  if (variant == 1) return find_variant(64, ty, stages, MODE_WINDOW) != nullptr;
+  if (variant == 2) return find_stream_variant(ty, stages) != nullptr;
+  return false;
 }
 
 PFN_cuTensorMapEncodeTiled_v12000 get_encode_fn() {
@@ -223,6 +272,42 @@ void encode_maps(TmaMaps& m, const fdtd_sim* s, const TmaVariant& v) {
   encode_map(&m.ids, s->mat.p, CU_TENSOR_MAP_DATA_TYPE_UINT16, 2, s, 3, tx + 8, ty + 1, 1, 0, 0);
 }
 
+// Tensor maps of the streaming kernel (box widths of StreamGeom).
+void encode_stream_maps(StreamMaps& m, const fdtd_sim* s, int ty) {
+  std::memset(&m, 0, sizeof(m));
+  const auto F = CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
+  const size_t N = s->cells_padded;
+  encode_map(&m.E, s->fields.p, F, 4, s, 5, 36, ty + 1, 3, N, 6 * N);
+  encode_map(&m.H, s->fields.p + 3 * N, F, 4, s, 5, 40, ty + 2, 3, N, 6 * N);
+  if (s->splits.n) {
+    encode_map(&m.Es, s->splits.p, F, 4, s, 5, 36, ty + 1, 6, N, 12 * N);
+    encode_map(&m.Hs, s->splits.p + 6 * N, F, 4, s, 5, 36, ty, 6, N, 12 * N);
+  }
+  encode_map(&m.ids, s->mat.p, CU_TENSOR_MAP_DATA_TYPE_UINT16, 2, s, 3, 40, ty + 1, 1, 0, 0);
+}
+
+// Everything one launch of the streaming kernel needs.
+struct StreamClass {
+  const StreamVariant* v = nullptr;
+  std::vector<StreamTile> host_tiles;
+  std::vector<StreamMaps> host_maps;
+  DevBuf<StreamMaps> d_maps;
+  DevBuf<SimDev> d_sims;
+  DevBuf<StreamTile> d_tiles;
+  DevBuf<unsigned> d_counter;
+  int n_tiles = 0, grid = 0;
+  void reset() {
+    v = nullptr;
+    host_tiles.clear();
+    host_maps.clear();
+    d_maps.free();
+    d_sims.free();
+    d_tiles.free();
+    d_counter.free();
+    n_tiles = grid = 0;
+  }
+};
+
 // Tiles of one kernel class with everything one launch of that class needs.
 struct TileClass {
   const TmaVariant* v = nullptr;
@@ -249,6 +334,7 @@ struct Engine {
   std::vector<fdtd_sim*> sims;
   KernelConfig cfg;
   TileClass cls[2];        // 0: ordinary tiles (x-PML in split windows), 1: y/z-PML slabs (all split)
+  StreamClass scls;        // streaming kernel
   DevBuf<SimDev> d_sims;   // plain kernel
   DevBuf<int4> d_tiles;    // plain kernel
   DevBuf<int> d_err;
@@ -301,6 +387,10 @@ struct Engine {
     if (!d_err.n) {
       d_err.alloc(1);
       CK(cudaMemset(d_err.p, 0, sizeof(int)));
+    }
+    if (cfg.variant == 2) {
+      build_stream_tiles(n_sm);
+      return;
     }
     if (cfg.variant == 1) {
       const TmaVariant* vv[2] = {find_variant(64, cfg.ty, cfg.stages, MODE_WINDOW), find_variant(64, 4, 4, MODE_FULL)};
@@ -432,7 +522,76 @@ struct Engine {
     n_tiles = int(tiles.size());
   }
 
+  // Streaming kernel: 31 x TY column tiles cut in z chunks of at most 62
+  // planes, each with the mask of its planes that hold split-field cells.
+  void build_stream_tiles(int n_sm) {
+    StreamClass& c = scls;
+    c.reset();
+    c.v = find_stream_variant(cfg.ty, cfg.stages);
+    if (!c.v) throw ArgError{FDTD_ERR_ARG, "No streaming kernel instantiated for this tile height / stage count."};
+    const StreamVariant& v = *c.v;
+    CK(cudaFuncSetAttribute(reinterpret_cast<const void*>(v.fn), cudaFuncAttributeMaxDynamicSharedMemorySize, v.smem));
+    int per_sm = 0;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, reinterpret_cast<const void*>(v.fn), v.threads, v.smem));
+    if (per_sm < 1) throw ArgError{FDTD_ERR_LIMIT, "Streaming kernel does not fit on an SM."};
+    const int ty = v.ty;
+    int64_t cols = 0;
+    for (auto* s : sims) cols += int64_t((s->nx + kStreamOwnX - 1) / kStreamOwnX) * ((s->ny + ty - 1) / ty);
+    const int64_t slots = int64_t(per_sm) * n_sm;
+    zchunk_used = 1 << 30;
+    for (size_t i = 0; i < sims.size(); ++i) {
+      fdtd_sim* s = sims[i];
+      int zc = cfg.zchunk;
+      if (zc <= 0) {
+        // about four tiles per resident block
+        const int64_t chunks = std::max<int64_t>(1, (slots * 4 + cols - 1) / std::max<int64_t>(cols, 1));
+        zc = int((s->nz + chunks - 1) / chunks);
+      }
+      zc = std::max(1, std::min(zc, 62));
+      zchunk_used = std::min(zchunk_used, zc);
+      c.host_maps.emplace_back();
+      encode_stream_maps(c.host_maps.back(), s, ty);
+      const GradedIndex split_idx(s->grid, kFlagESplit | kFlagHSplit);
+      for (int z0 = 0; z0 < s->nz; z0 += zc)
+        for (int y0 = 0; y0 < s->ny; y0 += ty)
+          for (int x0 = 0; x0 < s->nx; x0 += kStreamOwnX) {
+            const int z1 = std::min(s->nz, z0 + zc);
+            uint64_t mask = 0;
+            for (int j = 0; j < z1 - z0 + 1; ++j) {
+              const int z = z0 - 1 + j;
+              if (z >= 0 && split_idx.count(x0 - 1, x0 + kStreamOwnX, y0 - 1, y0 + ty, z, z + 1) > 0)
+                mask |= uint64_t(1) << j;
+            }
+            c.host_tiles.push_back(StreamTile{int(i), x0, y0, z0, z1, 0, uint32_t(mask), uint32_t(mask >> 32)});
+          }
+    }
+    c.n_tiles = int(c.host_tiles.size());
+    c.d_maps.alloc(c.host_maps.size());
+    CK(cudaMemcpy(c.d_maps.p, c.host_maps.data(), c.host_maps.size() * sizeof(StreamMaps), cudaMemcpyHostToDevice));
+    std::vector<SimDev> devs;
+    for (size_t i = 0; i < sims.size(); ++i) {
+      devs.push_back(sims[i]->dev);
+      devs.back().maps = reinterpret_cast<const TmaMaps*>(c.d_maps.p + i);
+    }
+    c.d_sims.alloc(devs.size());
+    CK(cudaMemcpy(c.d_sims.p, devs.data(), devs.size() * sizeof(SimDev), cudaMemcpyHostToDevice));
+    c.d_tiles.alloc(c.host_tiles.size());
+    CK(cudaMemcpy(c.d_tiles.p, c.host_tiles.data(), c.host_tiles.size() * sizeof(StreamTile), cudaMemcpyHostToDevice));
+    c.d_counter.alloc(1);
+    c.grid = int(std::min<int64_t>(c.n_tiles, slots));
+    n_tiles = c.n_tiles;
+    grid = c.grid;
+  }
+
   void launch_step(cudaStream_t st, int n) {
+    if (cfg.variant == 2) {
+      StreamClass& c = scls;
+      const unsigned base = unsigned(n) * unsigned(c.n_tiles + c.grid);
+      c.v->fn<<<c.grid, c.v->threads, c.v->smem, st>>>(c.d_sims.p, c.d_tiles.p, c.n_tiles, n, c.d_counter.p, base,
+                                                        d_err.p);
+      CK(cudaGetLastError());
+      return;
+    }
     if (cfg.variant == 1) {
       for (int k = 0; k < 2; ++k) {
         TileClass& t = cls[k];
@@ -461,6 +620,7 @@ struct Engine {
     }
     for (auto& t : cls)
       if (t.d_counter.n) CK(cudaMemsetAsync(t.d_counter.p, 0, sizeof(unsigned), st));
+    if (scls.d_counter.n) CK(cudaMemsetAsync(scls.d_counter.p, 0, sizeof(unsigned), st));
     int dft_from = 0;
     for (int n = 0; n < nt; ++n) {
       launch_step(st, n);
@@ -570,7 +730,7 @@ void prepare(fdtd_sim* s, int nt) {
     {
       DevBuf<uint16_t> tmp;
       tmp.alloc(s->grid.ids.size());
-      CK(cudaMemcpy(tmp.p, s->grid.ids.data(), s->grid.ids.size() * 2, cudaMemcpyHostToDevice));
+      h2d(s, tmp.p, s->grid.ids.data(), s->grid.ids.size() * 2);
       s->mat.alloc(N);
       CK(cudaMemset(s->mat.p, 0, N * 2));
       transpose_ids_kernel<<<1024, 256>>>(tmp.p, s->mat.p, nx, ny, nz, s->pitch);
@@ -578,15 +738,14 @@ void prepare(fdtd_sim* s, int nt) {
       CK(cudaDeviceSynchronize());
     }
     s->rows.alloc(s->grid.rows.size() * 8);
-    CK(cudaMemcpy(s->rows.p, s->grid.rows.data(), s->grid.rows.size() * sizeof(Row), cudaMemcpyHostToDevice));
+    h2d(s, s->rows.p, s->grid.rows.data(), s->grid.rows.size() * sizeof(Row));
     s->cell_probes.alloc(std::max<size_t>(1, s->grid.cell_probes.size()));
     if (!s->grid.cell_probes.empty())
-      CK(cudaMemcpy(s->cell_probes.p, s->grid.cell_probes.data(), s->grid.cell_probes.size() * sizeof(int2),
-                    cudaMemcpyHostToDevice));
+      h2d(s, s->cell_probes.p, s->grid.cell_probes.data(), s->grid.cell_probes.size() * sizeof(int2));
     std::vector<int> srcflag(std::max<size_t>(1, s->probes.size()), 0);
     for (size_t p = 0; p < s->probes.size(); ++p) srcflag[p] = s->probes[p].is_source;
     s->is_src.alloc(srcflag.size());
-    CK(cudaMemcpy(s->is_src.p, srcflag.data(), srcflag.size() * sizeof(int), cudaMemcpyHostToDevice));
+    h2d(s, s->is_src.p, srcflag.data(), srcflag.size() * sizeof(int));
     s->prepared = true;
   }
   // per-nt buffers: source amplitudes, records, DFT, monitors
@@ -598,19 +757,19 @@ void prepare(fdtd_sim* s, int nt) {
     for (size_t p = 0; p < P; ++p)
       if (s->probes[p].is_source)
         std::memcpy(&host[p * nt], s->probe_values[p].data(), size_t(nt) * sizeof(float));
-    CK(cudaMemcpy(s->src.p, host.data(), host.size() * sizeof(float), cudaMemcpyHostToDevice));
+    h2d(s, s->src.p, host.data(), host.size() * sizeof(float));
   }
   if (s->n_series > 0) {
     s->d_series_start.alloc(s->series_start.size());
-    CK(cudaMemcpy(s->d_series_start.p, s->series_start.data(), s->series_start.size() * 4, cudaMemcpyHostToDevice));
+    h2d(s, s->d_series_start.p, s->series_start.data(), s->series_start.size() * 4);
     s->d_term_probe.alloc(std::max<size_t>(1, s->term_probe.size()));
     if (!s->term_probe.empty())
-      CK(cudaMemcpy(s->d_term_probe.p, s->term_probe.data(), s->term_probe.size() * 4, cudaMemcpyHostToDevice));
+      h2d(s, s->d_term_probe.p, s->term_probe.data(), s->term_probe.size() * 4);
     s->d_term_weight.alloc(std::max<size_t>(1, s->term_weight.size()));
     if (!s->term_weight.empty())
-      CK(cudaMemcpy(s->d_term_weight.p, s->term_weight.data(), s->term_weight.size() * 8, cudaMemcpyHostToDevice));
+      h2d(s, s->d_term_weight.p, s->term_weight.data(), s->term_weight.size() * 8);
     s->d_omega.alloc(s->omega.size());
-    CK(cudaMemcpy(s->d_omega.p, s->omega.data(), s->omega.size() * 8, cudaMemcpyHostToDevice));
+    h2d(s, s->d_omega.p, s->omega.data(), s->omega.size() * 8);
     s->dft_X.alloc(size_t(s->n_series) * s->n_freq);
   }
   std::vector<MonDev> mdev;
@@ -624,7 +783,7 @@ void prepare(fdtd_sim* s, int nt) {
     auto ph = std::make_unique<DevBuf<float2>>();
     if (m.n_freq) {
       ph->alloc(m.phase.size() / 2);
-      CK(cudaMemcpy(ph->p, m.phase.data(), m.phase.size() * 4, cudaMemcpyHostToDevice));
+      h2d(s, ph->p, m.phase.data(), m.phase.size() * 4);
     }
     mdev.push_back(MonDev{m.field, m.axis, m.position, m.n_step, m.n_freq, m.n1, m.n2, out->p, ph->p});
     s->mon_out.push_back(std::move(out));
@@ -632,7 +791,7 @@ void prepare(fdtd_sim* s, int nt) {
   }
   s->d_mons.alloc(mdev.size());
   if (!mdev.empty())
-    CK(cudaMemcpy(s->d_mons.p, mdev.data(), mdev.size() * sizeof(MonDev), cudaMemcpyHostToDevice));
+    h2d(s, s->d_mons.p, mdev.data(), mdev.size() * sizeof(MonDev));
 
   // descriptor
   SimDev& d = s->dev;
@@ -655,7 +814,7 @@ void prepare(fdtd_sim* s, int nt) {
   d.rec = s->rec.p;
   d.is_src = s->is_src.p;
   s->d_dev.alloc(1);
-  CK(cudaMemcpy(s->d_dev.p, &d, sizeof(SimDev), cudaMemcpyHostToDevice));
+  h2d(s, s->d_dev.p, &d, sizeof(SimDev));
   s->prepared_nt = nt;
 }
 
@@ -667,10 +826,12 @@ void fill_stats(fdtd_sim* s, const Engine* e) {
   st.e_split_cells = s->grid.e_split_cells;
   st.h_split_cells = s->grid.h_split_cells;
   st.compile_ms = s->grid.compile_ms;
+  st.h2d_bytes = s->h2d_bytes;
+  st.d2h_bytes = s->d2h_bytes;
   if (e) {
     st.variant = e->cfg.variant;
-    st.tile_y = e->cfg.variant == 1 ? e->cfg.ty : kTileY;
-    st.stages = e->cfg.variant == 1 ? e->cfg.stages : 0;
+    st.tile_y = e->cfg.variant != 0 ? e->cfg.ty : kTileY;
+    st.stages = e->cfg.variant != 0 ? e->cfg.stages : 0;
     st.zchunk = e->zchunk_used;
     st.grid = e->grid;
     st.n_tiles = e->n_tiles;
@@ -866,17 +1027,14 @@ int fdtd_get_material_table(fdtd_sim* s, uint16_t* ids, int64_t n_ids, uint32_t*
 int fdtd_set_kernel(fdtd_sim* s, int variant, int tile_y, int stages, int zchunk) {
   if (!s) return FDTD_ERR_ARG;
   return guarded(&s->err, [&] {
-    if (variant != 0 && variant != 1) throw ArgError{FDTD_ERR_ARG, "variant must be 0 (plain) or 1 (tma)"};
+    if (variant < 0 || variant > 2) throw ArgError{FDTD_ERR_ARG, "variant must be 0 (plain), 1 (tma) or 2 (stream)"};
+    if (!kernel_exists(variant, tile_y, stages))
+      throw ArgError{FDTD_ERR_ARG, "No kernel instantiated for this variant / tile height / stage count."};
     KernelConfig c;
     c.variant = variant;
     c.ty = tile_y;
     c.stages = stages;
     c.zchunk = zchunk;
-    if (variant == 1) {
-      bool found = false;
-      found = find_variant(64, tile_y, stages, MODE_WINDOW) != nullptr;
-      if (!found) throw ArgError{FDTD_ERR_ARG, "No TMA kernel instantiated for this tile height / stage count."};
-    }
     s->cfg = c;
     s->engine.reset();
   });
@@ -929,7 +1087,7 @@ int fdtd_get_probe_values(fdtd_sim* s, float* out, int n_probes, int nt) {
     if (n_probes != int(s->probes.size()) || nt != s->prepared_nt)
       throw ArgError{FDTD_ERR_ARG, "Probe output size does not match the last run."};
     if (n_probes == 0) return;
-    CK(cudaMemcpy(out, s->rec.p, size_t(n_probes) * nt * sizeof(float), cudaMemcpyDeviceToHost));
+    d2h(s, out, s->rec.p, size_t(n_probes) * nt * sizeof(float));
   });
 }
 
@@ -938,7 +1096,7 @@ int fdtd_get_dft(fdtd_sim* s, double* out, int n_series, int n_freq) {
   return guarded(&s->err, [&] {
     if (n_series != s->n_series || n_freq != s->n_freq) throw ArgError{FDTD_ERR_ARG, "DFT size mismatch."};
     if (!s->dft_X.n) throw ArgError{FDTD_ERR_STATE, "No DFT configured."};
-    CK(cudaMemcpy(out, s->dft_X.p, s->dft_X.n * sizeof(double2), cudaMemcpyDeviceToHost));
+    d2h(s, out, s->dft_X.p, s->dft_X.n * sizeof(double2));
   });
 }
 
@@ -947,13 +1105,15 @@ int fdtd_get_monitor(fdtd_sim* s, int m, void* out, int64_t n_bytes) {
   return guarded(&s->err, [&] {
     if (m < 0 || m >= int(s->mon_out.size())) throw ArgError{FDTD_ERR_ARG, "Monitor index out of range."};
     if (size_t(n_bytes) != s->mon_out[m]->n) throw ArgError{FDTD_ERR_ARG, "Monitor output size mismatch."};
-    CK(cudaMemcpy(out, s->mon_out[m]->p, size_t(n_bytes), cudaMemcpyDeviceToHost));
+    d2h(s, out, s->mon_out[m]->p, size_t(n_bytes));
   });
 }
 
 int fdtd_get_stats(const fdtd_sim* s, fdtd_stats* out) {
   if (!s || !out) return FDTD_ERR_ARG;
   *out = s->stats;
+  out->h2d_bytes = s->h2d_bytes;
+  out->d2h_bytes = s->d2h_bytes;
   return FDTD_OK;
 }
 
@@ -996,12 +1156,9 @@ int fdtd_batch_create(fdtd_sim* const* sims, int n_sims, fdtd_batch** out) {
 int fdtd_batch_set_kernel(fdtd_batch* b, int variant, int tile_y, int stages, int zchunk) {
   if (!b) return FDTD_ERR_ARG;
   return guarded(&b->err, [&] {
-    if (variant != 0 && variant != 1) throw ArgError{FDTD_ERR_ARG, "variant must be 0 (plain) or 1 (tma)"};
-    if (variant == 1) {
-      bool found = false;
-      found = find_variant(64, tile_y, stages, MODE_WINDOW) != nullptr;
-      if (!found) throw ArgError{FDTD_ERR_ARG, "No TMA kernel instantiated for this tile height / stage count."};
-    }
+    if (variant < 0 || variant > 2) throw ArgError{FDTD_ERR_ARG, "variant must be 0 (plain), 1 (tma) or 2 (stream)"};
+    if (!kernel_exists(variant, tile_y, stages))
+      throw ArgError{FDTD_ERR_ARG, "No kernel instantiated for this variant / tile height / stage count."};
     b->engine.cfg.variant = variant;
     b->engine.cfg.ty = tile_y;
     b->engine.cfg.stages = stages;
@@ -1042,8 +1199,8 @@ int fdtd_batch_run(fdtd_batch* b, int nt) {
     st = fdtd_stats{};
     st.nt = nt;
     st.variant = b->engine.cfg.variant;
-    st.tile_y = b->engine.cfg.variant == 1 ? b->engine.cfg.ty : kTileY;
-    st.stages = b->engine.cfg.variant == 1 ? b->engine.cfg.stages : 0;
+    st.tile_y = b->engine.cfg.variant != 0 ? b->engine.cfg.ty : kTileY;
+    st.stages = b->engine.cfg.variant != 0 ? b->engine.cfg.stages : 0;
     st.zchunk = b->engine.zchunk_used;
     st.grid = b->engine.grid;
     st.n_tiles = b->engine.n_tiles;

@@ -67,8 +67,8 @@ using RowMap = std::unordered_map<Row, uint32_t, RowHash, RowEq>;
 
 }  // namespace
 
-GradedIndex::GradedIndex(const CompiledGrid& g) : nx(g.nx), ny(g.ny), nz(g.nz) {
-  // summed-volume table of graded cells, indexed [x][y][z] with a zero border
+GradedIndex::GradedIndex(const CompiledGrid& g, uint32_t mask) : nx(g.nx), ny(g.ny), nz(g.nz) {
+  // summed-volume table of flagged cells, indexed [x][y][z] with a zero border
   sy_ = nz + 1;
   sx_ = int64_t(ny + 1) * sy_;
   sv_.assign(size_t(nx + 1) * sx_, 0);
@@ -76,7 +76,7 @@ GradedIndex::GradedIndex(const CompiledGrid& g) : nx(g.nx), ny(g.ny), nz(g.nz) {
     for (int y = 0; y < ny; ++y)
       for (int z = 0; z < nz; ++z) {
         const uint32_t f = g.rows[g.ids[(size_t(x) * ny + y) * nz + z]].w[R_FLAGS];
-        const int32_t v = (f & kFlagGraded) ? 1 : 0;
+        const int32_t v = (f & mask) ? 1 : 0;
         const int64_t i = (x + 1) * sx_ + (y + 1) * sy_ + (z + 1);
         sv_[i] = v + sv_[i - sx_] + sv_[i - sy_] + sv_[i - 1] - sv_[i - sx_ - sy_] - sv_[i - sx_ - 1] -
                  sv_[i - sy_ - 1] + sv_[i - sx_ - sy_ - 1];

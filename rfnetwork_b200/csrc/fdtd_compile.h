@@ -76,12 +76,12 @@ struct Box3 {
   bool empty() const { return x1 <= x0 || y1 <= y0 || z1 <= z0; }
 };
 
-// Counts graded (PML) split cells in boxes of a compiled grid in O(1) through
-// a summed-volume table.
+// Counts the cells of a compiled grid whose row flags intersect `mask`
+// (default: graded PML cells) in boxes, in O(1) through a summed-volume table.
 class GradedIndex {
  public:
-  explicit GradedIndex(const CompiledGrid& g);
-  // cells with the graded flag in [x0,x1) x [y0,y1) x [z0,z1), clipped to the grid
+  explicit GradedIndex(const CompiledGrid& g, uint32_t mask = kFlagGraded);
+  // flagged cells in [x0,x1) x [y0,y1) x [z0,z1), clipped to the grid
   int64_t count(int x0, int x1, int y0, int y1, int z0, int z1) const;
   int nx, ny, nz;
 

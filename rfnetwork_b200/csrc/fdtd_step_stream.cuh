@@ -1,0 +1,387 @@
+// Streaming step kernel for sm_100a: one thread per Yee cell, z planes staged
+// in shared memory by the tensor-memory accelerator (cp.async.bulk.tensor)
+// through a ring of S mbarrier-guarded stages.
+//
+// Same update as fdtd_step_kernel (fdtd_kernels.cuh) through the same
+// rounding-fixed helpers, so the two kernels produce the same bits.
+//
+//   tile      31 (x) by TY (y) owned cells and a z range [z0, z1). The block
+//             has TY + 1 consumer warps, one per row y0-1 .. y0+TY-1; lane l
+//             of a warp sits on column x0-1+l. Row y0-1 and column x0-1 are
+//             the halo whose E^{n+1} the H update needs; they are recomputed
+//             here rather than read back, so one sweep over memory advances
+//             the whole step.
+//   producer  one more warp (lane 0) takes tiles from a global atomic counter
+//             and, per z plane, waits for a free stage ("empty" mbarrier) and
+//             issues the plane's loads onto the stage's "full" mbarrier:
+//               H^n     3 components, rows y0-1 .. y0+TY, 40 columns
+//               E^n     3 components, rows y0-1 .. y0+TY-1, 36 columns
+//               index   16-bit material rows, 40 columns
+//               splits  the 6 E and 6 H split components, only for planes the
+//                       host flagged as holding split-field cells (PML slabs,
+//                       soft sources) -- a 64-bit mask per tile
+//             Every box starts at an x that is a multiple of 16 bytes at or
+//             below x0-1; the consumers index from that offset. Boxes reaching
+//             outside the grid fill with zeros and a zero material index
+//             selects the all-zero coefficient row, so halo and grid edges
+//             need no bounds checks in the arithmetic. The last plane of a
+//             tile (z1) is only the look-ahead of H for dH/dz: H alone.
+//   consumers per plane z: E^{n+1}(z) for every thread's cell from H^n(z),
+//             H^n(z+1) and E^n(z) in shared memory; E x/y neighbours are traded
+//             by warp shuffle and a small double-buffered shared array; one
+//             barrier; then H^{n+1}(z) of the owned cells from E^{n+1}(z) and
+//             E^{n+1}(z-1), which each thread kept from its previous plane.
+//   waits     every mbarrier wait is bounded. A consumer whose wait expires
+//             votes at the next barrier; then all consumers record an error
+//             code and return; the producer gives up on the stage it waits
+//             for, drains its own loads (bounded) and returns.
+#pragma once
+
+#include "fdtd_kernels.cuh"
+#include "tma.cuh"
+
+namespace rfn {
+
+constexpr int kStreamOwnX = 31;           // owned columns per tile (lane 0 is the halo column)
+constexpr uint32_t kStreamWaitLimit = 1u << 20;  // sleeping polls (each <= 2 us) per wait
+constexpr int kStreamErrTimeout = 1;
+constexpr int kStreamBar = 1;             // named barrier of the consumer warps
+
+// Tensor maps of one simulation for the streaming kernel.
+struct StreamMaps {
+  CUtensorMap E, H, ids, Es, Hs;
+};
+
+// One tile: owned [x0, x0+31) x [y0, y0+TY) x [z0, z1); bit j of the mask set
+// when plane z0-1+j holds split-field cells inside the tile's E region.
+struct StreamTile {
+  int sim, x0, y0, z0, z1, pad;
+  uint32_t mask_lo, mask_hi;
+};
+
+template <int TY>
+struct StreamGeom {
+  static constexpr int HW = 40, EW = 36, IW = 40;  // box widths along x
+  static constexpr int HR = TY + 2, ER = TY + 1;   // box heights along y
+  static constexpr int HC = HR * HW;               // floats per H component
+  static constexpr int EC = ER * EW;               // floats per E (and E split) component
+  static constexpr int SHC = TY * EW;              // floats per H split component
+  static constexpr int HB = 3 * HC * 4;
+  static constexpr int EB = 3 * EC * 4;
+  static constexpr int IB = ER * IW * 2;
+  static constexpr int SEB = 6 * EC * 4;
+  static constexpr int SHB = 6 * SHC * 4;
+  static constexpr int A(int b) { return (b + 127) / 128 * 128; }
+  static constexpr int OFF_E = A(HB);
+  static constexpr int OFF_I = OFF_E + A(EB);
+  static constexpr int OFF_ES = OFF_I + A(IB);
+  static constexpr int OFF_HS = OFF_ES + A(SEB);
+  static constexpr int STAGE = OFF_HS + A(SHB);
+  static constexpr uint32_t MAIN_BYTES = HB + EB + IB;
+  static constexpr uint32_t SPLIT_BYTES = SEB + SHB;
+  static constexpr int NCW = TY + 1;               // consumer warps
+  static constexpr int CONSUMERS = 32 * NCW;
+  static constexpr int THREADS = CONSUMERS + 32;   // + the producer warp
+  static constexpr int XCH = 2 * ER * 32 * 4;      // one E neighbour-exchange buffer (ex, ez), bytes
+};
+
+template <int TY, int S>
+constexpr int stream_smem_bytes() {
+  using G = StreamGeom<TY>;
+  return S * G::STAGE + 2 * G::XCH + 16 * S;
+}
+
+__device__ __forceinline__ StreamTile load_stream_tile(const StreamTile* tiles, int i) {
+  const int4* p = reinterpret_cast<const int4*>(tiles + i);
+  const int4 a = __ldg(p), b = __ldg(p + 1);
+  return StreamTile{a.x, a.y, a.z, a.w, b.x, b.y, uint32_t(b.z), uint32_t(b.w)};
+}
+
+// Soft sources of one field group of a cell (solver.cu:459-488, 515-541):
+// s1 += v; s2 += v for every source probe on a component of that group.
+__device__ __forceinline__ void stream_inject(const SimDev& Sd, const float4& r7, uint32_t flags, int n, bool e_side,
+                                              float (&s)[6]) {
+  const int np = int(flags >> 16);
+  const int first = __float_as_int(r7.w);
+  for (int e = 0; e < np; ++e) {
+    const int2 pe = __ldg(Sd.cell_probes + first + e);
+    const bool mine = e_side ? pe.y < 3 : pe.y >= 3;
+    if (mine && __ldg(Sd.is_src + pe.x)) {
+      const float v = __ldg(Sd.src + (size_t)pe.x * Sd.nt + n);
+      const int c = e_side ? pe.y : pe.y - 3;
+#pragma unroll
+      for (int k = 0; k < 3; ++k)
+        if (c == k) {
+          s[2 * k] = __fadd_rn(s[2 * k], v);
+          s[2 * k + 1] = __fadd_rn(s[2 * k + 1], v);
+        }
+    }
+  }
+}
+
+template <int TY, int S>
+__global__ void __launch_bounds__(StreamGeom<TY>::THREADS)
+fdtd_step_stream_kernel(const SimDev* __restrict__ sims, const StreamTile* __restrict__ tiles, int n_tiles, int n,
+                        unsigned* __restrict__ counter, unsigned base, int* __restrict__ err) {
+  using G = StreamGeom<TY>;
+  // a tile streams at least 3 planes, so S <= 7 keeps the producer within
+  // three tiles of the consumers (the s_tq ring holds 4)
+  static_assert(S >= 3 && S <= 7, "stage count out of range");
+  extern __shared__ __align__(128) unsigned char smem[];
+  float* xch = reinterpret_cast<float*>(smem + S * G::STAGE);  // [2][ex, ez][ER][32]
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + S * G::STAGE + 2 * G::XCH);
+  uint64_t* empty = full + S;
+  __shared__ int s_tq[4];
+  const int tid = threadIdx.x;
+  const int cur = n & 1, nxt = cur ^ 1;
+  constexpr int NC = G::CONSUMERS;
+
+  if (tid == 0) {
+    for (int s = 0; s < S; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], G::NCW);
+    }
+    fence_mbar_init();
+  }
+  __syncthreads();
+
+  // =================================================================== producer
+  if (tid >= NC) {
+    if (tid != NC) return;
+    uint32_t q = 0;
+    int k = 0;
+    const StreamMaps* cur_maps = nullptr;
+    bool failed = false;
+    for (;;) {
+      const unsigned v = atomicAdd(counter, 1u) - base;
+      const int t = v < unsigned(n_tiles) ? int(v) : -1;
+      StreamTile td{};
+      int nload = 1;
+      uint64_t mask = 0;
+      const StreamMaps* maps = nullptr;
+      if (t >= 0) {
+        td = load_stream_tile(tiles, t);
+        nload = td.z1 - td.z0 + 2;  // planes z0-1 .. z1
+        mask = uint64_t(td.mask_lo) | (uint64_t(td.mask_hi) << 32);
+        maps = reinterpret_cast<const StreamMaps*>(sims[td.sim].maps);
+        if (maps != cur_maps) {
+          tensormap_acquire(&maps->E);
+          tensormap_acquire(&maps->H);
+          tensormap_acquire(&maps->ids);
+          tensormap_acquire(&maps->Es);
+          tensormap_acquire(&maps->Hs);
+          cur_maps = maps;
+        }
+      }
+      const int xs = (td.x0 - 1) & ~3, xi = (td.x0 - 1) & ~7;
+      for (int j = 0; j < nload; ++j, ++q) {
+        const int s = int(q % S);
+        if (q >= uint32_t(S) && !mbar_wait_bounded(&empty[s], ((q / S) + 1) & 1u, kStreamWaitLimit)) {
+          failed = true;
+          break;
+        }
+        if (j == 0) s_tq[k & 3] = t;
+        if (t < 0) {  // end of the stream: complete the phase without data
+          mbar_arrive(&full[s]);
+          ++q;
+          break;
+        }
+        unsigned char* b = smem + s * G::STAGE;
+        const int zp = td.z0 - 1 + j;
+        const bool last = j == nload - 1;
+        const bool split = !last && ((mask >> j) & 1u);
+        fence_proxy_async();
+        mbar_arrive_expect_tx(&full[s], last ? uint32_t(G::HB) : G::MAIN_BYTES + (split ? G::SPLIT_BYTES : 0u));
+        tma_load_5d(b, &maps->H, xs, td.y0 - 1, zp, 0, cur, &full[s]);
+        if (!last) {
+          tma_load_5d(b + G::OFF_E, &maps->E, xs, td.y0 - 1, zp, 0, cur, &full[s]);
+          tma_load_3d(b + G::OFF_I, &maps->ids, xi, td.y0 - 1, zp, &full[s]);
+          if (split) {
+            tma_load_5d(b + G::OFF_ES, &maps->Es, xs, td.y0 - 1, zp, 0, cur, &full[s]);
+            tma_load_5d(b + G::OFF_HS, &maps->Hs, xs, td.y0, zp, 0, cur, &full[s]);
+          }
+        }
+      }
+      if (failed || t < 0) break;
+      ++k;
+    }
+    if (failed) {
+      atomicExch(err, kStreamErrTimeout);
+      // drain the loads still in flight (bounded)
+      for (uint32_t r = q > uint32_t(S) ? q - S : 0; r < q; ++r)
+        mbar_wait_bounded(&full[r % S], (r / S) & 1u, kStreamWaitLimit);
+    }
+    return;
+  }
+
+  // ================================================================== consumers
+  const int lane = tid & 31, w = tid >> 5;
+  const float4* __restrict__ rows = nullptr;
+  int row_id = -1;
+  float4 ra = {}, rb = {}, rd = {}, rp = {}, rq = {}, ru = {}, rv = {}, r7 = {};
+  uint32_t q0 = 0;  // sequence number of the current tile's first plane
+  for (int k = 0;; ++k) {
+    bool ok = mbar_wait_bounded(&full[q0 % S], (q0 / S) & 1u, kStreamWaitLimit);
+    if (named_bar_or(kStreamBar, NC, !ok)) {
+      if (tid == 0) atomicExch(err, kStreamErrTimeout);
+      return;
+    }
+    const int ti = s_tq[k & 3];
+    if (ti < 0) break;
+    const StreamTile td = load_stream_tile(tiles, ti);
+    const SimDev& Sd = sims[td.sim];
+    if (Sd.rows != rows) {
+      rows = Sd.rows;
+      row_id = -1;
+    }
+    const int x0 = td.x0, y0 = td.y0, z0 = td.z0;
+    const int c = x0 - 1 + lane, r = y0 - 1 + w;
+    const int oh = (x0 - 1) - ((x0 - 1) & ~3), oi = (x0 - 1) - ((x0 - 1) & ~7);
+    const bool own_xy = lane >= 1 && w >= 1 && c < Sd.nx && r < Sd.ny;
+    const int plane = Sd.plane;
+    const int col = r * Sd.pitch + c;  // used for owned cells only
+    const int npl = td.z1 - z0 + 1;     // planes z0-1 .. z1-1 computed
+    const int hb = w * G::HW + oh + lane;
+    const int eb = w * G::EW + oh + lane;
+    const int ib = w * G::IW + oi + lane;
+    const int sb = (w - 1) * G::EW + oh + lane;  // H split box (owned rows)
+
+    float ex_p = 0.f, ey_p = 0.f;  // E^{n+1} of this cell one plane below
+    for (int i = 0; i < npl; ++i) {
+      const int z = z0 - 1 + i;
+      const uint32_t q = q0 + i;
+      if (i > 0) ok = mbar_wait_bounded(&full[q % S], (q / S) & 1u, kStreamWaitLimit);
+      ok = ok && mbar_wait_bounded(&full[(q + 1) % S], ((q + 1) / S) & 1u, kStreamWaitLimit);
+      const unsigned char* st = smem + int(q % S) * G::STAGE;
+      const float* sH = reinterpret_cast<const float*>(st);
+      const float* sE = reinterpret_cast<const float*>(st + G::OFF_E);
+      const uint16_t* sI = reinterpret_cast<const uint16_t*>(st + G::OFF_I);
+      const float* sEs = reinterpret_cast<const float*>(st + G::OFF_ES);
+      const float* sHs = reinterpret_cast<const float*>(st + G::OFF_HS);
+      const float* nH = reinterpret_cast<const float*>(smem + int((q + 1) % S) * G::STAGE);
+      float* xb = xch + (i & 1) * (G::XCH / 4);
+      constexpr int HC = G::HC, EC = G::EC;
+
+      // ------------------------------------------------------------ E phase
+      float ex = 0.f, ey = 0.f, ez = 0.f;
+      float hx_c = 0.f, hy_c = 0.f, hz_c = 0.f;
+      uint32_t flags = 0;
+      if (ok) {
+        hx_c = sH[hb];
+        hy_c = sH[HC + hb];
+        hz_c = sH[2 * HC + hb];
+        const float dhz_y = sH[2 * HC + hb + G::HW] - hz_c, dhy_z = nH[HC + hb] - hy_c;
+        const float dhx_z = nH[hb] - hx_c, dhz_x = sH[2 * HC + hb + 1] - hz_c;
+        const float dhy_x = sH[HC + hb + 1] - hy_c, dhx_y = sH[hb + G::HW] - hx_c;
+        const int id = sI[ib];
+        if (id != row_id) {
+          const float4* row = rows + 8 * id;
+          ra = __ldg(row); rb = __ldg(row + 1); rd = __ldg(row + 2); rp = __ldg(row + 3);
+          rq = __ldg(row + 4); ru = __ldg(row + 5); rv = __ldg(row + 6); r7 = __ldg(row + 7);
+          row_id = id;
+        }
+        flags = __float_as_uint(r7.z);
+        if (!(flags & kESplit)) {
+          // both splits share Ca: f' = Ca f + Cb1 d1 + Cb2 d2
+          ex = upd_e(ra.x, sE[eb], ra.y, dhz_y, ra.w, dhy_z);
+          ey = upd_e(rb.x, sE[EC + eb], rb.y, dhx_z, rb.w, dhz_x);
+          ez = upd_e(rd.x, sE[2 * EC + eb], rd.y, dhy_x, rd.w, dhx_y);
+        } else {
+          float sp[6];
+#pragma unroll
+          for (int m = 0; m < 6; ++m) sp[m] = sEs[m * EC + eb];
+          sp[0] = upd_e_split(ra.x, sp[0], ra.y, dhz_y);  // ex_y
+          sp[1] = upd_e_split(ra.z, sp[1], ra.w, dhy_z);  // ex_z
+          sp[2] = upd_e_split(rb.x, sp[2], rb.y, dhx_z);  // ey_z
+          sp[3] = upd_e_split(rb.z, sp[3], rb.w, dhz_x);  // ey_x
+          sp[4] = upd_e_split(rd.x, sp[4], rd.y, dhy_x);  // ez_x
+          sp[5] = upd_e_split(rd.z, sp[5], rd.w, dhx_y);  // ez_y
+          if (flags >> 16) stream_inject(Sd, r7, flags, n, true, sp);
+          ex = __fadd_rn(sp[0], sp[1]);
+          ey = __fadd_rn(sp[2], sp[3]);
+          ez = __fadd_rn(sp[4], sp[5]);
+          if (own_xy && z >= z0) {
+            const int idx = z * plane + col;
+            float* const* Eo = Sd.Es[nxt];
+#pragma unroll
+            for (int m = 0; m < 6; ++m) Eo[m][idx] = sp[m];
+          }
+        }
+      }
+      xb[w * 32 + lane] = ex;
+      xb[G::ER * 32 + w * 32 + lane] = ez;
+      const float ey_xm = __shfl_up_sync(0xffffffffu, ey, 1);
+      const float ez_xm = __shfl_up_sync(0xffffffffu, ez, 1);
+      // E^{n+1}(z) of the block complete; a consumer whose wait expired votes here
+      if (named_bar_or(kStreamBar, NC, !ok)) {
+        if (tid == 0) atomicExch(err, kStreamErrTimeout);
+        return;
+      }
+
+      // ------------------------------------------------------------ H phase
+      if (own_xy && z >= z0) {
+        const int idx = z * plane + col;
+        const float ex_ym = xb[(w - 1) * 32 + lane];
+        const float ez_ym = xb[G::ER * 32 + (w - 1) * 32 + lane];
+        if (!(flags & kESplit)) {
+          Sd.E[nxt][0][idx] = ex;
+          Sd.E[nxt][1][idx] = ey;
+          Sd.E[nxt][2][idx] = ez;
+        }
+        // slots 12..29: (Da, Db1, Db2) of hx_y, hx_z, hy_z, hy_x, hz_x, hz_y
+        const float gxy = h_term(rp.z, ez, rp.y, ez_ym);
+        const float gxz = h_term(rq.y, ey, rq.x, ey_p);
+        const float gyz = h_term(ru.x, ex, rq.w, ex_p);
+        const float gyx = h_term(ru.w, ez, ru.z, ez_xm);
+        const float gzx = h_term(rv.z, ey, rv.y, ey_xm);
+        const float gzy = h_term(r7.y, ex, r7.x, ex_ym);
+        float hx, hy, hz;
+        if (!(flags & kHSplit)) {
+          hx = upd_h(rp.x, hx_c, gxy, gxz);
+          hy = upd_h(rq.z, hy_c, gyz, gyx);
+          hz = upd_h(rv.x, hz_c, gzx, gzy);
+        } else {
+          float sp[6];
+#pragma unroll
+          for (int m = 0; m < 6; ++m) sp[m] = sHs[m * G::SHC + sb];
+          sp[0] = upd_h_split(rp.x, sp[0], gxy);
+          sp[1] = upd_h_split(rp.w, sp[1], gxz);
+          sp[2] = upd_h_split(rq.z, sp[2], gyz);
+          sp[3] = upd_h_split(ru.y, sp[3], gyx);
+          sp[4] = upd_h_split(rv.x, sp[4], gzx);
+          sp[5] = upd_h_split(rv.w, sp[5], gzy);
+          if (flags >> 16) stream_inject(Sd, r7, flags, n, false, sp);
+          hx = __fadd_rn(sp[0], sp[1]);
+          hy = __fadd_rn(sp[2], sp[3]);
+          hz = __fadd_rn(sp[4], sp[5]);
+          float* const* Ho = Sd.Hs[nxt];
+#pragma unroll
+          for (int m = 0; m < 6; ++m) Ho[m][idx] = sp[m];
+        }
+        Sd.H[nxt][0][idx] = hx;
+        Sd.H[nxt][1][idx] = hy;
+        Sd.H[nxt][2][idx] = hz;
+        const int np = int(flags >> 16);
+        if (np) {  // record the probes of this cell (solver.cu:467, 521)
+          const int first = __float_as_int(r7.w);
+          for (int e = 0; e < np; ++e) {
+            const int2 pe = __ldg(Sd.cell_probes + first + e);
+            const float val = pe.y == 0 ? ex : pe.y == 1 ? ey : pe.y == 2 ? ez : pe.y == 3 ? hx : pe.y == 4 ? hy : hz;
+            Sd.rec[(size_t)pe.x * Sd.nt + n] = val;
+          }
+        }
+      }
+      ex_p = ex;
+      ey_p = ey;
+      // plane q is no longer read by this warp
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&empty[q % S]);
+    }
+    // the look-ahead plane z1 was read only by the last iteration
+    __syncwarp();
+    if (lane == 0) mbar_arrive(&empty[(q0 + npl) % S]);
+    q0 += uint32_t(npl + 1);
+  }
+}
+
+}  // namespace rfn
