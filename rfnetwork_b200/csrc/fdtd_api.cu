@@ -93,8 +93,8 @@ int threads_for_host() {
 // Kernel selection of an engine: the plain-load kernel (one cell per thread)
 // or the TMA-pipelined kernel with its tile height, stage count and z chunk.
 struct KernelConfig {
-  int variant = 0;  // 0 plain, 1 tma (float4 groups), 2 stream (one thread per cell)
-  int ty = 7;
+  int variant = 2;  // 0 plain, 1 tma (float4 groups), 2 stream (one thread per cell)
+  int ty = 8;
   int stages = 4;
   int zchunk = 0;   // 0: pick from the grid size
 };
@@ -102,7 +102,7 @@ struct KernelConfig {
 KernelConfig default_config() {
   KernelConfig c;
   if (const char* v = std::getenv("RFN_FDTD_KERNEL"))
-    c.variant = std::string(v) == "tma" ? 1 : std::string(v) == "stream" ? 2 : 0;
+    c.variant = std::string(v) == "plain" ? 0 : std::string(v) == "tma" ? 1 : 2;
   if (const char* v = std::getenv("RFN_FDTD_TY")) c.ty = std::atoi(v);
   if (const char* v = std::getenv("RFN_FDTD_STAGES")) c.stages = std::atoi(v);
   if (const char* v = std::getenv("RFN_FDTD_ZCHUNK")) c.zchunk = std::atoi(v);
@@ -813,6 +813,7 @@ void prepare(fdtd_sim* s, int nt) {
   d.src = s->src.p;
   d.rec = s->rec.p;
   d.is_src = s->is_src.p;
+  d.cells = int64_t(N);
   s->d_dev.alloc(1);
   h2d(s, s->d_dev.p, &d, sizeof(SimDev));
   s->prepared_nt = nt;

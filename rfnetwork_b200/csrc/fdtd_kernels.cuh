@@ -56,6 +56,7 @@ struct SimDev {
   const float* src;       // [P][nt] soft-source amplitudes
   float* rec;             // [P][nt] recorded field values
   const int* is_src;      // [P]
+  int64_t cells;          // floats per component array (E[b][c+1] - E[b][c], also for splits)
 };
 
 __device__ __forceinline__ float ldf(const float* p, int i, bool ok) { return ok ? __ldg(p + i) : 0.0f; }

@@ -148,7 +148,9 @@ fdtd_step_stream_kernel(const SimDev* __restrict__ sims, const StreamTile* __res
   // =================================================================== producer
   if (tid >= NC) {
     if (tid != NC) return;
-    uint32_t q = 0;
+    uint32_t q = 0;        // sequence number of the next plane
+    int sq = 0;            // its stage
+    uint32_t pq = 0;       // parity of its stage's current use
     int k = 0;
     const StreamMaps* cur_maps = nullptr;
     bool failed = false;
@@ -174,32 +176,37 @@ fdtd_step_stream_kernel(const SimDev* __restrict__ sims, const StreamTile* __res
         }
       }
       const int xs = (td.x0 - 1) & ~3, xi = (td.x0 - 1) & ~7;
-      for (int j = 0; j < nload; ++j, ++q) {
-        const int s = int(q % S);
-        if (q >= uint32_t(S) && !mbar_wait_bounded(&empty[s], ((q / S) + 1) & 1u, kStreamWaitLimit)) {
+      for (int j = 0; j < nload; ++j) {
+        // the stage's previous use (parity pq ^ 1) must have been released
+        if (q >= uint32_t(S) && !mbar_wait_bounded(&empty[sq], pq ^ 1u, kStreamWaitLimit)) {
           failed = true;
           break;
         }
         if (j == 0) s_tq[k & 3] = t;
         if (t < 0) {  // end of the stream: complete the phase without data
-          mbar_arrive(&full[s]);
+          mbar_arrive(&full[sq]);
           ++q;
           break;
         }
-        unsigned char* b = smem + s * G::STAGE;
+        unsigned char* b = smem + sq * G::STAGE;
         const int zp = td.z0 - 1 + j;
         const bool last = j == nload - 1;
         const bool split = !last && ((mask >> j) & 1u);
         fence_proxy_async();
-        mbar_arrive_expect_tx(&full[s], last ? uint32_t(G::HB) : G::MAIN_BYTES + (split ? G::SPLIT_BYTES : 0u));
-        tma_load_5d(b, &maps->H, xs, td.y0 - 1, zp, 0, cur, &full[s]);
+        mbar_arrive_expect_tx(&full[sq], last ? uint32_t(G::HB) : G::MAIN_BYTES + (split ? G::SPLIT_BYTES : 0u));
+        tma_load_5d(b, &maps->H, xs, td.y0 - 1, zp, 0, cur, &full[sq]);
         if (!last) {
-          tma_load_5d(b + G::OFF_E, &maps->E, xs, td.y0 - 1, zp, 0, cur, &full[s]);
-          tma_load_3d(b + G::OFF_I, &maps->ids, xi, td.y0 - 1, zp, &full[s]);
+          tma_load_5d(b + G::OFF_E, &maps->E, xs, td.y0 - 1, zp, 0, cur, &full[sq]);
+          tma_load_3d(b + G::OFF_I, &maps->ids, xi, td.y0 - 1, zp, &full[sq]);
           if (split) {
-            tma_load_5d(b + G::OFF_ES, &maps->Es, xs, td.y0 - 1, zp, 0, cur, &full[s]);
-            tma_load_5d(b + G::OFF_HS, &maps->Hs, xs, td.y0, zp, 0, cur, &full[s]);
+            tma_load_5d(b + G::OFF_ES, &maps->Es, xs, td.y0 - 1, zp, 0, cur, &full[sq]);
+            tma_load_5d(b + G::OFF_HS, &maps->Hs, xs, td.y0, zp, 0, cur, &full[sq]);
           }
+        }
+        ++q;
+        if (++sq == S) {
+          sq = 0;
+          pq ^= 1u;
         }
       }
       if (failed || t < 0) break;
@@ -219,9 +226,10 @@ fdtd_step_stream_kernel(const SimDev* __restrict__ sims, const StreamTile* __res
   const float4* __restrict__ rows = nullptr;
   int row_id = -1;
   float4 ra = {}, rb = {}, rd = {}, rp = {}, rq = {}, ru = {}, rv = {}, r7 = {};
-  uint32_t q0 = 0;  // sequence number of the current tile's first plane
+  int sq = 0;        // stage of the plane being computed
+  uint32_t pq = 0;   // parity of that stage's current use
   for (int k = 0;; ++k) {
-    bool ok = mbar_wait_bounded(&full[q0 % S], (q0 / S) & 1u, kStreamWaitLimit);
+    bool ok = mbar_wait_bounded(&full[sq], pq, kStreamWaitLimit);
     if (named_bar_or(kStreamBar, NC, !ok)) {
       if (tid == 0) atomicExch(err, kStreamErrTimeout);
       return;
@@ -239,73 +247,75 @@ fdtd_step_stream_kernel(const SimDev* __restrict__ sims, const StreamTile* __res
     const int oh = (x0 - 1) - ((x0 - 1) & ~3), oi = (x0 - 1) - ((x0 - 1) & ~7);
     const bool own_xy = lane >= 1 && w >= 1 && c < Sd.nx && r < Sd.ny;
     const int plane = Sd.plane;
-    const int col = r * Sd.pitch + c;  // used for owned cells only
-    const int npl = td.z1 - z0 + 1;     // planes z0-1 .. z1-1 computed
+    const int64_t N = Sd.cells;
+    float* __restrict__ const fo = Sd.E[nxt][0];   // E then H components of step n+1, N apart
+    const int npl = td.z1 - z0 + 1;                // planes z0-1 .. z1-1 computed
     const int hb = w * G::HW + oh + lane;
     const int eb = w * G::EW + oh + lane;
     const int ib = w * G::IW + oi + lane;
-    const int sb = (w - 1) * G::EW + oh + lane;  // H split box (owned rows)
+    const int sb = (w - 1) * G::EW + oh + lane;    // H split box (owned rows)
+    int idx = (z0 - 1) * plane + r * Sd.pitch + c; // cell offset of plane z (owned cells, z >= z0)
 
     float ex_p = 0.f, ey_p = 0.f;  // E^{n+1} of this cell one plane below
     for (int i = 0; i < npl; ++i) {
-      const int z = z0 - 1 + i;
-      const uint32_t q = q0 + i;
-      if (i > 0) ok = mbar_wait_bounded(&full[q % S], (q / S) & 1u, kStreamWaitLimit);
-      ok = ok && mbar_wait_bounded(&full[(q + 1) % S], ((q + 1) / S) & 1u, kStreamWaitLimit);
-      const unsigned char* st = smem + int(q % S) * G::STAGE;
+      int sn = sq + 1;
+      uint32_t pn = pq;
+      if (sn == S) {
+        sn = 0;
+        pn ^= 1u;
+      }
+      // plane z was waited for as the look-ahead of the previous iteration
+      ok = ok && mbar_wait_bounded(&full[sn], pn, kStreamWaitLimit);
+      const unsigned char* st = smem + sq * G::STAGE;
       const float* sH = reinterpret_cast<const float*>(st);
       const float* sE = reinterpret_cast<const float*>(st + G::OFF_E);
       const uint16_t* sI = reinterpret_cast<const uint16_t*>(st + G::OFF_I);
       const float* sEs = reinterpret_cast<const float*>(st + G::OFF_ES);
       const float* sHs = reinterpret_cast<const float*>(st + G::OFF_HS);
-      const float* nH = reinterpret_cast<const float*>(smem + int((q + 1) % S) * G::STAGE);
+      const float* nH = reinterpret_cast<const float*>(smem + sn * G::STAGE);
       float* xb = xch + (i & 1) * (G::XCH / 4);
       constexpr int HC = G::HC, EC = G::EC;
+      const bool store = own_xy && i > 0;
 
       // ------------------------------------------------------------ E phase
-      float ex = 0.f, ey = 0.f, ez = 0.f;
-      float hx_c = 0.f, hy_c = 0.f, hz_c = 0.f;
-      uint32_t flags = 0;
-      if (ok) {
-        hx_c = sH[hb];
-        hy_c = sH[HC + hb];
-        hz_c = sH[2 * HC + hb];
-        const float dhz_y = sH[2 * HC + hb + G::HW] - hz_c, dhy_z = nH[HC + hb] - hy_c;
-        const float dhx_z = nH[hb] - hx_c, dhz_x = sH[2 * HC + hb + 1] - hz_c;
-        const float dhy_x = sH[HC + hb + 1] - hy_c, dhx_y = sH[hb + G::HW] - hx_c;
-        const int id = sI[ib];
-        if (id != row_id) {
-          const float4* row = rows + 8 * id;
-          ra = __ldg(row); rb = __ldg(row + 1); rd = __ldg(row + 2); rp = __ldg(row + 3);
-          rq = __ldg(row + 4); ru = __ldg(row + 5); rv = __ldg(row + 6); r7 = __ldg(row + 7);
-          row_id = id;
-        }
-        flags = __float_as_uint(r7.z);
-        if (!(flags & kESplit)) {
-          // both splits share Ca: f' = Ca f + Cb1 d1 + Cb2 d2
-          ex = upd_e(ra.x, sE[eb], ra.y, dhz_y, ra.w, dhy_z);
-          ey = upd_e(rb.x, sE[EC + eb], rb.y, dhx_z, rb.w, dhz_x);
-          ez = upd_e(rd.x, sE[2 * EC + eb], rd.y, dhy_x, rd.w, dhx_y);
-        } else {
-          float sp[6];
+      // (after an expired wait the values are stale but in bounds; the vote
+      // below then ends the block before anything is stored)
+      const float hx_c = sH[hb], hy_c = sH[HC + hb], hz_c = sH[2 * HC + hb];
+      const float dhz_y = sH[2 * HC + hb + G::HW] - hz_c, dhy_z = nH[HC + hb] - hy_c;
+      const float dhx_z = nH[hb] - hx_c, dhz_x = sH[2 * HC + hb + 1] - hz_c;
+      const float dhy_x = sH[HC + hb + 1] - hy_c, dhx_y = sH[hb + G::HW] - hx_c;
+      const int id = ok ? int(sI[ib]) : 0;  // a stage that never arrived may hold any bits
+      if (id != row_id) {
+        const float4* row = rows + 8 * id;
+        ra = __ldg(row); rb = __ldg(row + 1); rd = __ldg(row + 2); rp = __ldg(row + 3);
+        rq = __ldg(row + 4); ru = __ldg(row + 5); rv = __ldg(row + 6); r7 = __ldg(row + 7);
+        row_id = id;
+      }
+      const uint32_t flags = __float_as_uint(r7.z);
+      float ex, ey, ez;
+      if (!(flags & kESplit)) {
+        // both splits share Ca: f' = Ca f + Cb1 d1 + Cb2 d2
+        ex = upd_e(ra.x, sE[eb], ra.y, dhz_y, ra.w, dhy_z);
+        ey = upd_e(rb.x, sE[EC + eb], rb.y, dhx_z, rb.w, dhz_x);
+        ez = upd_e(rd.x, sE[2 * EC + eb], rd.y, dhy_x, rd.w, dhx_y);
+      } else {
+        float sp[6];
 #pragma unroll
-          for (int m = 0; m < 6; ++m) sp[m] = sEs[m * EC + eb];
-          sp[0] = upd_e_split(ra.x, sp[0], ra.y, dhz_y);  // ex_y
-          sp[1] = upd_e_split(ra.z, sp[1], ra.w, dhy_z);  // ex_z
-          sp[2] = upd_e_split(rb.x, sp[2], rb.y, dhx_z);  // ey_z
-          sp[3] = upd_e_split(rb.z, sp[3], rb.w, dhz_x);  // ey_x
-          sp[4] = upd_e_split(rd.x, sp[4], rd.y, dhy_x);  // ez_x
-          sp[5] = upd_e_split(rd.z, sp[5], rd.w, dhx_y);  // ez_y
-          if (flags >> 16) stream_inject(Sd, r7, flags, n, true, sp);
-          ex = __fadd_rn(sp[0], sp[1]);
-          ey = __fadd_rn(sp[2], sp[3]);
-          ez = __fadd_rn(sp[4], sp[5]);
-          if (own_xy && z >= z0) {
-            const int idx = z * plane + col;
-            float* const* Eo = Sd.Es[nxt];
+        for (int m = 0; m < 6; ++m) sp[m] = sEs[m * EC + eb];
+        sp[0] = upd_e_split(ra.x, sp[0], ra.y, dhz_y);  // ex_y
+        sp[1] = upd_e_split(ra.z, sp[1], ra.w, dhy_z);  // ex_z
+        sp[2] = upd_e_split(rb.x, sp[2], rb.y, dhx_z);  // ey_z
+        sp[3] = upd_e_split(rb.z, sp[3], rb.w, dhz_x);  // ey_x
+        sp[4] = upd_e_split(rd.x, sp[4], rd.y, dhy_x);  // ez_x
+        sp[5] = upd_e_split(rd.z, sp[5], rd.w, dhx_y);  // ez_y
+        if (flags >> 16) stream_inject(Sd, r7, flags, n, true, sp);
+        ex = __fadd_rn(sp[0], sp[1]);
+        ey = __fadd_rn(sp[2], sp[3]);
+        ez = __fadd_rn(sp[4], sp[5]);
+        if (store) {
+          float* const so = Sd.Es[nxt][0];
 #pragma unroll
-            for (int m = 0; m < 6; ++m) Eo[m][idx] = sp[m];
-          }
+          for (int m = 0; m < 6; ++m) so[m * N + idx] = sp[m];
         }
       }
       xb[w * 32 + lane] = ex;
@@ -319,14 +329,13 @@ fdtd_step_stream_kernel(const SimDev* __restrict__ sims, const StreamTile* __res
       }
 
       // ------------------------------------------------------------ H phase
-      if (own_xy && z >= z0) {
-        const int idx = z * plane + col;
+      if (store) {
         const float ex_ym = xb[(w - 1) * 32 + lane];
         const float ez_ym = xb[G::ER * 32 + (w - 1) * 32 + lane];
         if (!(flags & kESplit)) {
-          Sd.E[nxt][0][idx] = ex;
-          Sd.E[nxt][1][idx] = ey;
-          Sd.E[nxt][2][idx] = ez;
+          fo[idx] = ex;
+          fo[N + idx] = ey;
+          fo[2 * N + idx] = ez;
         }
         // slots 12..29: (Da, Db1, Db2) of hx_y, hx_z, hy_z, hy_x, hz_x, hz_y
         const float gxy = h_term(rp.z, ez, rp.y, ez_ym);
@@ -354,13 +363,13 @@ fdtd_step_stream_kernel(const SimDev* __restrict__ sims, const StreamTile* __res
           hx = __fadd_rn(sp[0], sp[1]);
           hy = __fadd_rn(sp[2], sp[3]);
           hz = __fadd_rn(sp[4], sp[5]);
-          float* const* Ho = Sd.Hs[nxt];
+          float* const so = Sd.Hs[nxt][0];
 #pragma unroll
-          for (int m = 0; m < 6; ++m) Ho[m][idx] = sp[m];
+          for (int m = 0; m < 6; ++m) so[m * N + idx] = sp[m];
         }
-        Sd.H[nxt][0][idx] = hx;
-        Sd.H[nxt][1][idx] = hy;
-        Sd.H[nxt][2][idx] = hz;
+        fo[3 * N + idx] = hx;
+        fo[4 * N + idx] = hy;
+        fo[5 * N + idx] = hz;
         const int np = int(flags >> 16);
         if (np) {  // record the probes of this cell (solver.cu:467, 521)
           const int first = __float_as_int(r7.w);
@@ -373,14 +382,20 @@ fdtd_step_stream_kernel(const SimDev* __restrict__ sims, const StreamTile* __res
       }
       ex_p = ex;
       ey_p = ey;
-      // plane q is no longer read by this warp
+      // plane z is no longer read by this warp
       __syncwarp();
-      if (lane == 0) mbar_arrive(&empty[q % S]);
+      if (lane == 0) mbar_arrive(&empty[sq]);
+      sq = sn;
+      pq = pn;
+      idx += plane;
     }
     // the look-ahead plane z1 was read only by the last iteration
     __syncwarp();
-    if (lane == 0) mbar_arrive(&empty[(q0 + npl) % S]);
-    q0 += uint32_t(npl + 1);
+    if (lane == 0) mbar_arrive(&empty[sq]);
+    if (++sq == S) {
+      sq = 0;
+      pq ^= 1u;
+    }
   }
 }
 
