@@ -282,6 +282,8 @@ void encode_stream_maps(StreamMaps& m, const fdtd_sim* s, int ty) {
   if (s->splits.n) {
     encode_map(&m.Es, s->splits.p, F, 4, s, 5, 36, ty + 1, 6, N, 12 * N);
     encode_map(&m.Hs, s->splits.p + 6 * N, F, 4, s, 5, 36, ty, 6, N, 12 * N);
+    encode_map(&m.Es16, s->splits.p, F, 4, s, 5, kStreamWin, ty + 1, 6, N, 12 * N);
+    encode_map(&m.Hs16, s->splits.p + 6 * N, F, 4, s, 5, kStreamWin, ty, 6, N, 12 * N);
   }
   encode_map(&m.ids, s->mat.p, CU_TENSOR_MAP_DATA_TYPE_UINT16, 2, s, 3, 40, ty + 1, 1, 0, 0);
 }
@@ -556,13 +558,38 @@ struct Engine {
         for (int y0 = 0; y0 < s->ny; y0 += ty)
           for (int x0 = 0; x0 < s->nx; x0 += kStreamOwnX) {
             const int z1 = std::min(s->nz, z0 + zc);
-            uint64_t mask = 0;
+            // planes holding split cells in the E region, and the x extent of those cells
+            uint64_t mask = 0, narrow = 0;
+            int wx0 = -1;
+            std::vector<std::pair<int, int>> span(size_t(z1 - z0 + 1), {-1, -1});
             for (int j = 0; j < z1 - z0 + 1; ++j) {
               const int z = z0 - 1 + j;
-              if (z >= 0 && split_idx.count(x0 - 1, x0 + kStreamOwnX, y0 - 1, y0 + ty, z, z + 1) > 0)
-                mask |= uint64_t(1) << j;
+              if (z < 0 || split_idx.count(x0 - 1, x0 + kStreamOwnX, y0 - 1, y0 + ty, z, z + 1) == 0) continue;
+              mask |= uint64_t(1) << j;
+              int lo = 1 << 30, hi = -1;
+              for (int x = std::max(0, x0 - 1); x < std::min(s->nx, x0 + kStreamOwnX); ++x)
+                if (split_idx.count(x, x + 1, y0 - 1, y0 + ty, z, z + 1) > 0) {
+                  lo = std::min(lo, x);
+                  hi = std::max(hi, x);
+                }
+              span[size_t(j)] = {lo, hi};
+              if (wx0 < 0 && hi < (lo & ~3) + kStreamWin) wx0 = lo & ~3;
             }
-            c.host_tiles.push_back(StreamTile{int(i), x0, y0, z0, z1, 0, uint32_t(mask), uint32_t(mask >> 32)});
+            for (int j = 0; j < z1 - z0 + 1 && wx0 >= 0; ++j)
+              if (((mask >> j) & 1u) && span[size_t(j)].first >= wx0 && span[size_t(j)].second < wx0 + kStreamWin)
+                narrow |= uint64_t(1) << j;
+            StreamTile t{};
+            t.sim = int(i);
+            t.x0 = x0;
+            t.y0 = y0;
+            t.z0 = z0;
+            t.z1 = z1;
+            t.wx0 = std::max(wx0, 0);
+            t.split_lo = uint32_t(mask);
+            t.split_hi = uint32_t(mask >> 32);
+            t.narrow_lo = uint32_t(narrow);
+            t.narrow_hi = uint32_t(narrow >> 32);
+            c.host_tiles.push_back(t);
           }
     }
     c.n_tiles = int(c.host_tiles.size());

@@ -19,7 +19,10 @@
 //               index   16-bit material rows, 40 columns
 //               splits  the 6 E and 6 H split components, only for planes the
 //                       host flagged as holding split-field cells (PML slabs,
-//                       soft sources) -- a 64-bit mask per tile
+//                       soft sources) -- a 64-bit mask per tile; over 36
+//                       columns, or over the 16-column window [wx0, wx0+16)
+//                       on planes whose split cells all lie in it (the x-PML
+//                       slab crossing an ordinary tile), a second mask
 //             Every box starts at an x that is a multiple of 16 bytes at or
 //             below x0-1; the consumers index from that offset. Boxes reaching
 //             outside the grid fill with zeros and a zero material index
@@ -47,16 +50,20 @@ constexpr uint32_t kStreamWaitLimit = 1u << 20;  // sleeping polls (each <= 2 us
 constexpr int kStreamErrTimeout = 1;
 constexpr int kStreamBar = 1;             // named barrier of the consumer warps
 
-// Tensor maps of one simulation for the streaming kernel.
+constexpr int kStreamWin = 16;            // columns of a narrow split window
+
+// Tensor maps of one simulation for the streaming kernel (split maps over 36
+// columns and over a 16-column window).
 struct StreamMaps {
-  CUtensorMap E, H, ids, Es, Hs;
+  CUtensorMap E, H, ids, Es, Hs, Es16, Hs16;
 };
 
-// One tile: owned [x0, x0+31) x [y0, y0+TY) x [z0, z1); bit j of the mask set
-// when plane z0-1+j holds split-field cells inside the tile's E region.
+// One tile: owned [x0, x0+31) x [y0, y0+TY) x [z0, z1). Bit j of `split` is
+// set when plane z0-1+j holds split-field cells inside the tile's E region;
+// bit j of `narrow` when all of them lie in columns [wx0, wx0+16).
 struct StreamTile {
-  int sim, x0, y0, z0, z1, pad;
-  uint32_t mask_lo, mask_hi;
+  int sim, x0, y0, z0, z1, wx0, pad0, pad1;
+  uint32_t split_lo, split_hi, narrow_lo, narrow_hi;
 };
 
 template <int TY>
@@ -79,10 +86,15 @@ struct StreamGeom {
   static constexpr int STAGE = OFF_HS + A(SHB);
   static constexpr uint32_t MAIN_BYTES = HB + EB + IB;
   static constexpr uint32_t SPLIT_BYTES = SEB + SHB;
+  static constexpr int SECN = ER * kStreamWin;     // floats per E split component, narrow window
+  static constexpr int SHCN = TY * kStreamWin;     // floats per H split component, narrow window
+  static constexpr uint32_t SPLIT_BYTES_N = 6 * (SECN + SHCN) * 4;
   static constexpr int NCW = TY + 1;               // consumer warps
   static constexpr int CONSUMERS = 32 * NCW;
   static constexpr int THREADS = CONSUMERS + 32;   // + the producer warp
   static constexpr int XCH = 2 * ER * 32 * 4;      // one E neighbour-exchange buffer (ex, ez), bytes
+  // resident blocks per SM the register budget is sized for (shared memory allows as many)
+  static constexpr int MIN_BLOCKS = TY <= 4 ? 4 : TY <= 6 ? 3 : 2;
 };
 
 template <int TY, int S>
@@ -93,8 +105,12 @@ constexpr int stream_smem_bytes() {
 
 __device__ __forceinline__ StreamTile load_stream_tile(const StreamTile* tiles, int i) {
   const int4* p = reinterpret_cast<const int4*>(tiles + i);
-  const int4 a = __ldg(p), b = __ldg(p + 1);
-  return StreamTile{a.x, a.y, a.z, a.w, b.x, b.y, uint32_t(b.z), uint32_t(b.w)};
+  const int4 a = __ldg(p), b = __ldg(p + 1), c = __ldg(p + 2);
+  return StreamTile{a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w, uint32_t(c.x), uint32_t(c.y), uint32_t(c.z), uint32_t(c.w)};
+}
+
+__device__ __forceinline__ void prefetch_l1(const void* p) {
+  asm volatile("prefetch.global.L1 [%0];" ::"l"(p));
 }
 
 // Soft sources of one field group of a cell (solver.cu:459-488, 515-541):
@@ -120,7 +136,7 @@ __device__ __forceinline__ void stream_inject(const SimDev& Sd, const float4& r7
 }
 
 template <int TY, int S>
-__global__ void __launch_bounds__(StreamGeom<TY>::THREADS)
+__global__ void __launch_bounds__(StreamGeom<TY>::THREADS, StreamGeom<TY>::MIN_BLOCKS)
 fdtd_step_stream_kernel(const SimDev* __restrict__ sims, const StreamTile* __restrict__ tiles, int n_tiles, int n,
                         unsigned* __restrict__ counter, unsigned base, int* __restrict__ err) {
   using G = StreamGeom<TY>;
@@ -159,12 +175,13 @@ fdtd_step_stream_kernel(const SimDev* __restrict__ sims, const StreamTile* __res
       const int t = v < unsigned(n_tiles) ? int(v) : -1;
       StreamTile td{};
       int nload = 1;
-      uint64_t mask = 0;
+      uint64_t mask = 0, narrow = 0;
       const StreamMaps* maps = nullptr;
       if (t >= 0) {
         td = load_stream_tile(tiles, t);
         nload = td.z1 - td.z0 + 2;  // planes z0-1 .. z1
-        mask = uint64_t(td.mask_lo) | (uint64_t(td.mask_hi) << 32);
+        mask = uint64_t(td.split_lo) | (uint64_t(td.split_hi) << 32);
+        narrow = uint64_t(td.narrow_lo) | (uint64_t(td.narrow_hi) << 32);
         maps = reinterpret_cast<const StreamMaps*>(sims[td.sim].maps);
         if (maps != cur_maps) {
           tensormap_acquire(&maps->E);
@@ -172,6 +189,8 @@ fdtd_step_stream_kernel(const SimDev* __restrict__ sims, const StreamTile* __res
           tensormap_acquire(&maps->ids);
           tensormap_acquire(&maps->Es);
           tensormap_acquire(&maps->Hs);
+          tensormap_acquire(&maps->Es16);
+          tensormap_acquire(&maps->Hs16);
           cur_maps = maps;
         }
       }
@@ -192,13 +211,19 @@ fdtd_step_stream_kernel(const SimDev* __restrict__ sims, const StreamTile* __res
         const int zp = td.z0 - 1 + j;
         const bool last = j == nload - 1;
         const bool split = !last && ((mask >> j) & 1u);
+        const bool win = (narrow >> j) & 1u;
         fence_proxy_async();
-        mbar_arrive_expect_tx(&full[sq], last ? uint32_t(G::HB) : G::MAIN_BYTES + (split ? G::SPLIT_BYTES : 0u));
+        mbar_arrive_expect_tx(&full[sq], last    ? uint32_t(G::HB)
+                                         : !split ? G::MAIN_BYTES
+                                                  : G::MAIN_BYTES + (win ? G::SPLIT_BYTES_N : G::SPLIT_BYTES));
         tma_load_5d(b, &maps->H, xs, td.y0 - 1, zp, 0, cur, &full[sq]);
         if (!last) {
           tma_load_5d(b + G::OFF_E, &maps->E, xs, td.y0 - 1, zp, 0, cur, &full[sq]);
           tma_load_3d(b + G::OFF_I, &maps->ids, xi, td.y0 - 1, zp, &full[sq]);
-          if (split) {
+          if (split && win) {
+            tma_load_5d(b + G::OFF_ES, &maps->Es16, td.wx0, td.y0 - 1, zp, 0, cur, &full[sq]);
+            tma_load_5d(b + G::OFF_HS, &maps->Hs16, td.wx0, td.y0, zp, 0, cur, &full[sq]);
+          } else if (split) {
             tma_load_5d(b + G::OFF_ES, &maps->Es, xs, td.y0 - 1, zp, 0, cur, &full[sq]);
             tma_load_5d(b + G::OFF_HS, &maps->Hs, xs, td.y0, zp, 0, cur, &full[sq]);
           }
@@ -254,6 +279,10 @@ fdtd_step_stream_kernel(const SimDev* __restrict__ sims, const StreamTile* __res
     const int eb = w * G::EW + oh + lane;
     const int ib = w * G::IW + oi + lane;
     const int sb = (w - 1) * G::EW + oh + lane;    // H split box (owned rows)
+    // narrow window: this cell's column inside [wx0, wx0+16) when it is a split cell there
+    const int wc = c - td.wx0;
+    const int ebn = w * kStreamWin + wc, sbn = (w - 1) * kStreamWin + wc;
+    const uint64_t narrow = uint64_t(td.narrow_lo) | (uint64_t(td.narrow_hi) << 32);
     int idx = (z0 - 1) * plane + r * Sd.pitch + c; // cell offset of plane z (owned cells, z >= z0)
 
     float ex_p = 0.f, ey_p = 0.f;  // E^{n+1} of this cell one plane below
@@ -276,6 +305,7 @@ fdtd_step_stream_kernel(const SimDev* __restrict__ sims, const StreamTile* __res
       float* xb = xch + (i & 1) * (G::XCH / 4);
       constexpr int HC = G::HC, EC = G::EC;
       const bool store = own_xy && i > 0;
+      const bool win = (narrow >> i) & 1u;
 
       // ------------------------------------------------------------ E phase
       // (after an expired wait the values are stale but in bounds; the vote
@@ -285,6 +315,11 @@ fdtd_step_stream_kernel(const SimDev* __restrict__ sims, const StreamTile* __res
       const float dhx_z = nH[hb] - hx_c, dhz_x = sH[2 * HC + hb + 1] - hz_c;
       const float dhy_x = sH[HC + hb + 1] - hy_c, dhx_y = sH[hb + G::HW] - hx_c;
       const int id = ok ? int(sI[ib]) : 0;  // a stage that never arrived may hold any bits
+      if (i + 1 < npl) {
+        // the next plane's row into L1 while this plane computes
+        const int idn = reinterpret_cast<const uint16_t*>(smem + sn * G::STAGE + G::OFF_I)[ib];
+        if (ok && idn != id) prefetch_l1(rows + 8 * idn);
+      }
       if (id != row_id) {
         const float4* row = rows + 8 * id;
         ra = __ldg(row); rb = __ldg(row + 1); rd = __ldg(row + 2); rp = __ldg(row + 3);
@@ -301,7 +336,10 @@ fdtd_step_stream_kernel(const SimDev* __restrict__ sims, const StreamTile* __res
       } else {
         float sp[6];
 #pragma unroll
-        for (int m = 0; m < 6; ++m) sp[m] = sEs[m * EC + eb];
+        for (int m = 0; m < 6; ++m) {
+          const int o = win ? m * G::SECN + ebn : m * EC + eb;  // one load at the selected offset
+          sp[m] = sEs[o];
+        }
         sp[0] = upd_e_split(ra.x, sp[0], ra.y, dhz_y);  // ex_y
         sp[1] = upd_e_split(ra.z, sp[1], ra.w, dhy_z);  // ex_z
         sp[2] = upd_e_split(rb.x, sp[2], rb.y, dhx_z);  // ey_z
@@ -352,7 +390,10 @@ fdtd_step_stream_kernel(const SimDev* __restrict__ sims, const StreamTile* __res
         } else {
           float sp[6];
 #pragma unroll
-          for (int m = 0; m < 6; ++m) sp[m] = sHs[m * G::SHC + sb];
+          for (int m = 0; m < 6; ++m) {
+            const int o = win ? m * G::SHCN + sbn : m * G::SHC + sb;
+            sp[m] = sHs[o];
+          }
           sp[0] = upd_h_split(rp.x, sp[0], gxy);
           sp[1] = upd_h_split(rp.w, sp[1], gxz);
           sp[2] = upd_h_split(rq.z, sp[2], gyz);
