@@ -157,8 +157,66 @@ int fdtd_batch_get_stats(const fdtd_batch* b, fdtd_stats* out);
 const char* fdtd_batch_last_error(const fdtd_batch* b);
 void fdtd_batch_destroy(fdtd_batch* b);
 
-/* Last error of calls that have no handle (fdtd_create, fdtd_batch_create). */
+/* Last error of calls that have no handle (fdtd_create, fdtd_batch_create,
+ * fdtd_step_noalloc). */
 const char* fdtd_global_error(void);
+
+/* ------------------------------------------------ caller-owned buffers */
+
+/* Device buffers of one grid in the engine's own layout, all allocated and
+ * owned by the caller. N = nz * ny * pitch, pitch >= nx.
+ *   fields       2 x 6 x N floats: [time buffer][ex ey ez hx hy hz][z][y][pitch];
+ *                zero before step 0. Step n reads buffer n & 1 and writes the other.
+ *   splits       2 x 12 x N floats: [time buffer][ex_y ex_z ey_z ey_x ez_x ez_y
+ *                hx_y hx_z hy_z hy_x hz_x hz_y][z][y][pitch]; zero before step 0.
+ *                Touched only at cells whose row flags say split, but required.
+ *   mat          N uint16 row indices, [z][y][pitch]; columns x >= nx hold 0.
+ *                The rows and the per-cell indices (C order [x][y][z]) are what
+ *                fdtd_get_material_table returns for a compiled simulation.
+ *   rows         n_rows x 32 words, as fdtd_get_material_table returns them.
+ *   cell_probes  (probe, field) int32 pairs, one per probe, sorted by the probe's
+ *                cell (x * ny + y) * nz + z after the Yee shift of
+ *                fdtd_add_probe, ties in probe order; a row's word 31 is the
+ *                index of its cell's first pair, bits 16..31 of word 30 the count.
+ *   src, rec     n_probes x nt floats: source amplitudes in, recorded values out.
+ *   is_src       n_probes int32 flags. */
+typedef struct fdtd_device_grid {
+  int nx, ny, nz, pitch;
+  int nt;
+  float* fields;
+  float* splits;
+  const uint16_t* mat;
+  const uint32_t* rows;
+  const int32_t* cell_probes;
+  const float* src;
+  float* rec;
+  const int32_t* is_src;
+} fdtd_device_grid;
+
+/* Advance steps n0 .. n0+n_steps-1 of a grid held in caller-owned buffers,
+ * enqueued on `stream` (cudaStream_t as void*, NULL = default stream), with
+ * the plain step kernel: the same bits as fdtd_run.
+ *
+ * It allocates nothing. It exists for callers that must not let a library take
+ * device memory on its own. Examples are a host framework whose caching
+ * allocator owns the GPU's memory and accounts for every byte, and a
+ * memory-budgeted service. A cudaMalloc there bypasses the budget, and
+ * cudaFree waits for the whole device. The kernel's only data besides the
+ * caller's buffers are its grid descriptor and tile list. They live in a fixed
+ * static device array of 1 MiB + 1 KiB, which every GPU that loads the library
+ * keeps until the process exits.
+ * Limits and rules:
+ *  - At most 65536 tiles of 31 x 7 cells per z chunk, that is
+ *    ceil(nx/31) * ceil(ny/7) <= 65536. Larger grids get FDTD_ERR_LIMIT.
+ *  - The first call on a device looks up the array's device address. Make that
+ *    first call before any stream capture on the device.
+ *  - All calls share the array. Each call rewrites the descriptor and tile list
+ *    it uses, so nothing in it needs to start at zero. Calls whose work
+ *    overlaps on the GPU, for example on two streams, race on it.
+ * Errors are reported through fdtd_global_error(). No counterpart exists in the
+ * reference, which allocates its device buffers itself in every
+ * solver_run_cu call. */
+int fdtd_step_noalloc(const fdtd_device_grid* g, int n0, int n_steps, void* stream);
 
 #ifdef __cplusplus
 }

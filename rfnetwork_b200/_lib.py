@@ -21,7 +21,7 @@ EXPORTED = (
     "fdtd_set_kernel", "fdtd_batch_set_kernel",
     "fdtd_get_dft", "fdtd_get_monitor", "fdtd_get_stats", "fdtd_last_error", "fdtd_destroy",
     "fdtd_batch_create", "fdtd_batch_run", "fdtd_batch_set_stream", "fdtd_batch_get_stats",
-    "fdtd_batch_last_error", "fdtd_batch_destroy", "fdtd_global_error",
+    "fdtd_batch_last_error", "fdtd_batch_destroy", "fdtd_global_error", "fdtd_step_noalloc",
 )
 
 

@@ -15,6 +15,7 @@
 #include <cstring>
 #include <map>
 #include <memory>
+#include <mutex>
 #include <string>
 #include <thread>
 #include <vector>
@@ -1262,3 +1263,127 @@ void fdtd_batch_destroy(fdtd_batch* b) {
 const char* fdtd_global_error(void) { return g_error.c_str(); }
 
 }  // extern "C"
+
+// ------------------------------------------------ stepping without allocation
+//
+// fdtd_step_noalloc advances a grid whose device buffers the caller owns, with
+// the plain step kernel (fdtd_step_kernel). That kernel reads two small
+// engine-built arrays besides the caller's data: the grid descriptor (SimDev)
+// and the tile list. The other entry points cudaMalloc them per simulation;
+// here they live in one file-scope device array of fixed size, so the call
+// allocates nothing on the device.
+namespace {
+
+constexpr int kNoallocMaxTiles = 65536;          // tile-list capacity (16 B per tile)
+constexpr size_t kNoallocDescBytes = 1024;       // room for the SimDev descriptor
+constexpr size_t kNoallocScratchBytes = kNoallocDescBytes + size_t(kNoallocMaxTiles) * sizeof(int4);  // 1 MiB + 1 KiB
+static_assert(sizeof(SimDev) <= kNoallocDescBytes, "descriptor does not fit its scratch slot");
+
+// Shared by every call on a device, for the life of the process.
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoallocScratchBytes];
+
+constexpr int kNoallocMaxDevices = 64;
+std::mutex g_noalloc_mutex;
+unsigned char* g_noalloc_ptr[kNoallocMaxDevices] = {};   // device address of the array, per device
+int4 g_noalloc_tiles[kNoallocMaxTiles];                  // host staging of the tile list
+
+}  // namespace
+
+extern "C" int fdtd_step_noalloc(const fdtd_device_grid* g, int n0, int n_steps, void* stream) {
+  if (!g) {
+    g_error = "fdtd_step_noalloc: null grid";
+    return FDTD_ERR_ARG;
+  }
+  const int nx = g->nx, ny = g->ny, nz = g->nz, pitch = g->pitch;
+  if (nx < 2 || ny < 2 || nz < 2 || nx > 65535 || ny > 65535 || nz > 65535 || pitch < nx) {
+    g_error = "fdtd_step_noalloc: dimensions must be 2..65535 cells with pitch >= nx";
+    return FDTD_ERR_ARG;
+  }
+  if (g->nt < 1 || n0 < 0 || n_steps < 0 || int64_t(n0) + n_steps > g->nt) {
+    g_error = "fdtd_step_noalloc: steps n0 .. n0+n_steps-1 must lie in [0, nt)";
+    return FDTD_ERR_ARG;
+  }
+  const size_t N = size_t(nz) * ny * pitch;
+  if (N >= (size_t(1) << 31) - size_t(2) * ny * pitch) {
+    g_error = "fdtd_step_noalloc: grid too large for 32-bit cell offsets";
+    return FDTD_ERR_LIMIT;
+  }
+  // the engine's tiling of the plain kernel: 31 x 7 columns, z cut so that
+  // about 8 blocks per SM exist (at least 8 planes per chunk)
+  const int64_t xy_tiles = int64_t((nx + kTileX - 1) / kTileX) * ((ny + kTileY - 1) / kTileY);
+  if (xy_tiles > kNoallocMaxTiles) {
+    g_error = "fdtd_step_noalloc: the grid needs " + std::to_string(xy_tiles) +
+              " tiles per z chunk; the static tile list holds " + std::to_string(kNoallocMaxTiles);
+    return FDTD_ERR_LIMIT;
+  }
+  if (!g->fields || !g->splits || !g->mat || !g->rows || !g->cell_probes || !g->src || !g->rec || !g->is_src) {
+    g_error = "fdtd_step_noalloc: every buffer pointer must be a device address";
+    return FDTD_ERR_ARG;
+  }
+  if (n_steps == 0) return FDTD_OK;
+  try {
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kNoallocMaxDevices) throw ArgError{FDTD_ERR_LIMIT, "device ordinal out of range"};
+    if (!g_noalloc_ptr[dev]) {
+      // once per device: host code cannot name the array's device address directly
+      void* p = nullptr;
+      CK(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+      g_noalloc_ptr[dev] = static_cast<unsigned char*>(p);
+    }
+    unsigned char* scratch = g_noalloc_ptr[dev];
+    int n_sm = 148;
+    CK(cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev));
+    const int64_t want = int64_t(n_sm) * 8;
+    int chunks = int(std::max<int64_t>(1, (want + xy_tiles - 1) / xy_tiles));
+    chunks = std::min(chunks, std::max(1, nz / 8));
+    chunks = int(std::min<int64_t>(chunks, kNoallocMaxTiles / xy_tiles));
+    const int zlen = (nz + chunks - 1) / chunks;
+    int n_tiles = 0;
+    for (int z0 = 0; z0 < nz; z0 += zlen)
+      for (int y0 = 0; y0 < ny; y0 += kTileY)
+        for (int x0 = 0; x0 < nx; x0 += kTileX) {
+          const int z1 = std::min(nz, z0 + zlen);
+          g_noalloc_tiles[n_tiles++] = make_int4(0, x0 | (y0 << 16), z0 | (z1 << 16), 0);
+        }
+    SimDev d{};
+    d.nx = nx; d.ny = ny; d.nz = nz; d.pitch = pitch; d.plane = ny * pitch; d.nt = g->nt;
+    for (int b = 0; b < 2; ++b) {
+      for (int c = 0; c < 3; ++c) {
+        d.E[b][c] = g->fields + (size_t(b) * 6 + c) * N;
+        d.H[b][c] = g->fields + (size_t(b) * 6 + 3 + c) * N;
+      }
+      for (int c = 0; c < 6; ++c) {
+        d.Es[b][c] = g->splits + (size_t(b) * 12 + c) * N;
+        d.Hs[b][c] = g->splits + (size_t(b) * 12 + 6 + c) * N;
+      }
+    }
+    d.mat = g->mat;
+    d.rows = reinterpret_cast<const float4*>(g->rows);
+    d.cell_probes = reinterpret_cast<const int2*>(g->cell_probes);
+    d.src = g->src;
+    d.rec = g->rec;
+    d.is_src = g->is_src;
+    d.cells = int64_t(N);
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    // both copies come from pageable host memory, so they are staged before
+    // they return and the host arrays may be refilled by the next call
+    CK(cudaMemcpyAsync(scratch, &d, sizeof(SimDev), cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(scratch + kNoallocDescBytes, g_noalloc_tiles, size_t(n_tiles) * sizeof(int4),
+                       cudaMemcpyHostToDevice, st));
+    const SimDev* d_desc = reinterpret_cast<const SimDev*>(scratch);
+    const int4* d_tiles = reinterpret_cast<const int4*>(scratch + kNoallocDescBytes);
+    for (int n = n0; n < n0 + n_steps; ++n) {
+      fdtd_step_kernel<kTileY><<<n_tiles, dim3(32, kBlockY), 0, st>>>(d_desc, d_tiles, n);
+      CK(cudaGetLastError());
+    }
+    return FDTD_OK;
+  } catch (const ArgError& a) {
+    g_error = "fdtd_step_noalloc: " + a.msg;
+    return a.code;
+  } catch (const CudaError& c) {
+    g_error = "fdtd_step_noalloc: " + c.where + ": " + cudaGetErrorString(c.code);
+    return FDTD_ERR_CUDA;
+  }
+}
