@@ -62,6 +62,9 @@ def parse_args():
     ap.add_argument("--nt", type=int, default=NT, help="time steps per simulation")
     ap.add_argument("--e2e-steps", type=int, default=None, help="end-to-end calls timed (default: --steps)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", choices=("boxes", "batch"), default="boxes",
+                    help="boxes: the bandwidth model (default); batch: 64 uneven simulations in one launch "
+                         "per step against 64 sequential single-simulation runs")
     return ap.parse_args()
 
 
@@ -344,6 +347,80 @@ def run_reference(args, rank, world):
     }
 
 
+# ------------------------------------------------------------ batched workload
+
+BATCH_SIMS = 64
+BATCH_NT = 3000
+BATCH_FREQ = 21
+
+
+def run_batch(args, rank, world, local_rank):
+    """64 simulations with seeded axes U{32..160}, 8-cell PML, 8 boxes, one Gaussian point
+    source, 4 Ez probes, 21-frequency DFT each; stepped together (fdtd_batch_run: one step
+    launch per time step for all of them, the time loop as one CUDA graph) and one after
+    another (fdtd_run per simulation). Each rank runs its own copy."""
+    import torch
+    from rfnetwork_b200 import _lib, configs
+
+    torch.cuda.set_device(local_rank)
+    nt = args.nt if args.nt != NT else BATCH_NT
+    sims, cells = [], 0
+    for i in range(BATCH_SIMS):
+        m = configs.batch_member(3, i, nt=nt)
+        co, pr, mo, mem, Nx, Ny, Nz, Nt = m.pack_inputs(gpu=True)
+        sim = _lib.Simulation(Nx, Ny, Nz)
+        sim.set_coefficients(co)
+        for p in pr:
+            src = bool(p["is_source"])
+            sim.add_probe(int(p["field"]), p["idx"], src, p["values"][:Nt] if src else None)
+        f = np.linspace(1e9, 20e9, BATCH_FREQ)
+        sim.set_dft([(k, k, 1.0) for k in range(len(pr))], 2 * np.pi * f * float(m.dt))
+        sims.append(sim)
+        cells += Nx * Ny * Nz
+    batch = _lib.Batch(sims)
+    for _ in range(max(args.warmup, 1)):
+        batch.run(nt)
+    t_batch = []
+    for _ in range(args.steps):
+        batch.run(nt)
+        t_batch.append(batch.stats()["last_run_ms"])
+    recs = [s.probe_values().copy() for s in sims]
+    # the same simulations one after another, each through its own run
+    for s in sims:
+        s.run(nt)
+    t_seq = []
+    for _ in range(args.steps):
+        tot = 0.0
+        for s in sims:
+            s.run(nt)
+            tot += s.stats()["last_run_ms"]
+        t_seq.append(tot)
+    same = all(np.array_equal(s.probe_values(), r) for s, r in zip(sims, recs))
+    st = batch.stats()
+    batch.close()
+    for s in sims:
+        s.close()
+    if rank != 0:
+        return None
+    ms_b, ms_s = statistics.fmean(t_batch), statistics.fmean(t_seq)
+    return {
+        "metric": "batched sims/s", "value": round(world * BATCH_SIMS / (ms_b * 1e-3), 3), "unit": "sims/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_b, 2),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic: seeded uneven grids with dielectric boxes and a Gaussian point source",
+        "config": {"workload": f"batch of {BATCH_SIMS} sims, axes U{{32..160}}, 8-cell PML, {nt} steps, "
+                               f"{BATCH_FREQ}-freq DFT", "cells_total": cells, "time_steps": nt,
+                   "step": "one batched run of all simulations",
+                   "kernel": {k: st[k] for k in ("variant", "tile_y", "stages", "zchunk", "grid", "n_tiles")}},
+        "sequential": {"value": round(world * BATCH_SIMS / (ms_s * 1e-3), 3), "unit": "sims/s",
+                       "ms_per_step": round(ms_s, 2)},
+        "batched_over_sequential": round(ms_s / ms_b, 3),
+        "mcell_updates_per_s": round(world * cells * nt / (ms_b * 1e-3) / 1e6, 1),
+        "bit_identical_to_sequential": same,
+        "gpu_launches": int(st["step_launches"] + st["dft_launches"]) * args.steps,
+    }
+
+
 def main():
     args = parse_args()
     rank = int(os.environ.get("RANK", 0))
@@ -351,6 +428,8 @@ def main():
     local_rank = int(os.environ.get("LOCAL_RANK", 0))
     if args.impl == "reference":
         out = run_reference(args, rank, world)
+    elif args.workload == "batch":
+        out = run_batch(args, rank, world, local_rank)
     else:
         out = run_ours(args, rank, world, local_rank)
         if rank == 0 and world == 1 and not args.no_cpu_baseline:

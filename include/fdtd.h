@@ -55,7 +55,7 @@ typedef struct fdtd_stats {
   int64_t dft_launches;  /* DFT kernel launches issued by the last run */
   double last_run_ms;    /* device time of the last run (CUDA events) */
   double compile_ms;     /* host time spent building the material table */
-  int variant;           /* step kernel: 0 plain loads, 1 TMA float4 groups, 2 TMA streaming */
+  int variant;           /* step kernel: 0 plain loads, 1 TMA streaming */
   int tile_y;            /* tile height (rows) of the step kernel */
   int stages;            /* shared-memory pipeline stages (TMA kernel) */
   int zchunk;            /* z planes per tile */
@@ -118,11 +118,14 @@ int fdtd_run_async(fdtd_sim* s, int nt);
 int fdtd_synchronize(fdtd_sim* s);
 
 /* Step-kernel selection: variant 0 = plain loads (1 cell per thread, 31 x 7
- * tiles), 1 = TMA-pipelined float4 groups (64 x tile_y tiles), 2 = TMA
- * streaming, one thread per cell (31 x tile_y tiles, tile_y in {4, 6, 8, 12}).
- * stages = shared-memory plane buffers. zchunk = z planes per tile (0: derived
- * from the grid). The default comes from RFN_FDTD_KERNEL (plain / tma /
- * stream) / RFN_FDTD_TY / RFN_FDTD_STAGES / RFN_FDTD_ZCHUNK or is (2, 8, 4, 0).
+ * tiles), 1 = TMA streaming, one thread per cell (31 x tile_y tiles, tile_y in
+ * {4, 6, 8, 12}). stages = shared-memory plane buffers. zchunk = z planes per
+ * tile (0: derived from the grid). tile_y = 0 with variant 1 autotunes: the
+ * first run times a few candidate (tile_y, stages, zchunk) shapes on the
+ * simulation itself for a few steps and keeps the fastest, remembered per set
+ * of grid sizes for the life of the process. The default comes from
+ * RFN_FDTD_KERNEL (plain / stream) / RFN_FDTD_TY / RFN_FDTD_STAGES /
+ * RFN_FDTD_ZCHUNK or is (1, 0, 4, 0): autotuned streaming.
  * All variants give bit-identical results. The reference has one fixed 8x8x8
  * launch shape (solver.cu:549-557). */
 int fdtd_set_kernel(fdtd_sim* s, int variant, int tile_y, int stages, int zchunk);

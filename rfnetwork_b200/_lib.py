@@ -195,8 +195,8 @@ class Simulation:
                                                      info["n_rows"]))
         return ids, rows
 
-    def set_kernel(self, variant: int = 2, tile_y: int = 8, stages: int = 4, zchunk: int = 0):
-        """Pick the step kernel (0 plain, 1 TMA float4 groups, 2 TMA streaming) and its tile shape."""
+    def set_kernel(self, variant: int = 1, tile_y: int = 0, stages: int = 4, zchunk: int = 0):
+        """Pick the step kernel (0 plain loads, 1 TMA streaming) and its tile shape (tile_y 0: autotuned)."""
         self._check(self.lib.fdtd_set_kernel(self.h, int(variant), int(tile_y), int(stages), int(zchunk)))
 
     def set_stream(self, stream_ptr: int):
@@ -269,7 +269,7 @@ class Batch:
         for s in self.sims:
             s.nt = int(nt)
 
-    def set_kernel(self, variant: int = 2, tile_y: int = 8, stages: int = 4, zchunk: int = 0):
+    def set_kernel(self, variant: int = 1, tile_y: int = 0, stages: int = 4, zchunk: int = 0):
         rc = self.lib.fdtd_batch_set_kernel(self.h, int(variant), int(tile_y), int(stages), int(zchunk))
         if rc:
             raise ValueError(self.lib.fdtd_batch_last_error(self.h).decode())

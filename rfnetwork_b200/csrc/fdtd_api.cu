@@ -9,6 +9,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -24,7 +25,6 @@
 #include "fdtd_compile.h"
 #include "fdtd_kernels.cuh"
 #include "fdtd_step_stream.cuh"
-#include "fdtd_step_tma.cuh"
 #include <cudaTypedefs.h>
 
 using namespace rfn;
@@ -94,16 +94,22 @@ int threads_for_host() {
 // Kernel selection of an engine: the plain-load kernel (one cell per thread)
 // or the TMA-pipelined kernel with its tile height, stage count and z chunk.
 struct KernelConfig {
-  int variant = 2;  // 0 plain, 1 tma (float4 groups), 2 stream (one thread per cell)
-  int ty = 8;
+  int variant = 1;  // 0 plain loads, 1 TMA streaming
+  int ty = 0;       // streaming tile height; 0: autotuned (ty, stages, zchunk) per set of grid sizes
   int stages = 4;
   int zchunk = 0;   // 0: pick from the grid size
 };
 
+// Streaming-kernel shapes the autotuner times, and its choices per set of grid
+// sizes (process-wide).
+constexpr int kTuneCandidates[][3] = {{8, 4, 0}, {8, 4, 32}, {8, 3, 0}, {12, 3, 0}, {6, 3, 0}, {4, 4, 0}, {4, 4, 16}};
+std::mutex g_tune_mutex;
+std::map<std::vector<int>, std::array<int, 3>> g_tune_cache;
+
 KernelConfig default_config() {
   KernelConfig c;
   if (const char* v = std::getenv("RFN_FDTD_KERNEL"))
-    c.variant = std::string(v) == "plain" ? 0 : std::string(v) == "tma" ? 1 : 2;
+    c.variant = std::string(v) == "plain" ? 0 : 1;
   if (const char* v = std::getenv("RFN_FDTD_TY")) c.ty = std::atoi(v);
   if (const char* v = std::getenv("RFN_FDTD_STAGES")) c.stages = std::atoi(v);
   if (const char* v = std::getenv("RFN_FDTD_ZCHUNK")) c.zchunk = std::atoi(v);
@@ -166,35 +172,6 @@ void d2h(fdtd_sim* s, void* dst, const void* src, size_t bytes) {
   s->d2h_bytes += int64_t(bytes);
 }
 
-using TmaKernelFn = void (*)(const SimDev*, const TileDesc*, int, int, unsigned*, unsigned, int*);
-
-// One instantiation of the TMA step kernel.
-struct TmaVariant {
-  int tx, ty, stages, mode;
-  int smem, threads;
-  TmaKernelFn fn;
-};
-
-template <int TX, int TY, int S, int MODE>
-TmaVariant tma_variant() {
-  return TmaVariant{TX, TY, S, MODE, tma_smem_bytes<TX, TY, S, MODE>(), TmaGeom<TX, TY, MODE>::THREADS,
-                    &fdtd_step_tma_kernel<TX, TY, S, MODE>};
-}
-
-const std::vector<TmaVariant>& tma_variants() {
-  static const std::vector<TmaVariant> v = {
-      tma_variant<64, 7, 4, MODE_WINDOW>(),  tma_variant<64, 8, 4, MODE_WINDOW>(),
-      tma_variant<64, 16, 3, MODE_WINDOW>(), tma_variant<64, 4, 6, MODE_WINDOW>(),
-      tma_variant<64, 8, 3, MODE_WINDOW>(),  tma_variant<64, 4, 4, MODE_FULL>()};
-  return v;
-}
-
-const TmaVariant* find_variant(int tx, int ty, int stages, int mode) {
-  for (auto& v : tma_variants())
-    if (v.tx == tx && v.ty == ty && v.stages == stages && v.mode == mode) return &v;
-  return nullptr;
-}
-
 using StreamKernelFn = void (*)(const SimDev*, const StreamTile*, int, int, unsigned*, unsigned, int*);
 
 // One instantiation of the streaming step kernel.
@@ -225,8 +202,7 @@ const StreamVariant* find_stream_variant(int ty, int stages) {
 // Whether a (variant, tile height, stages) triple names an instantiated kernel.
 bool kernel_exists(int variant, int ty, int stages) {
   if (variant == 0) return true;
-  if (variant == 1) return find_variant(64, ty, stages, MODE_WINDOW) != nullptr;
-  if (variant == 2) return find_stream_variant(ty, stages) != nullptr;
+  if (variant == 1) return ty == 0 || find_stream_variant(ty, stages) != nullptr;
   return false;
 }
 
@@ -255,22 +231,6 @@ void encode_map(CUtensorMap* m, const void* base, CUtensorMapDataType type, int 
                                CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
                                CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (r != CUDA_SUCCESS) throw ArgError{FDTD_ERR_CUDA, "cuTensorMapEncodeTiled failed: " + std::to_string(int(r))};
-}
-
-void encode_maps(TmaMaps& m, const fdtd_sim* s, const TmaVariant& v) {
-  std::memset(&m, 0, sizeof(m));
-  const auto F = CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
-  const int tx = v.tx, ty = v.ty;
-  const int sew = v.mode == MODE_FULL ? tx + 4 : kSplitWin, shw = v.mode == MODE_FULL ? tx : kSplitWin;
-  const size_t N = s->cells_padded;
-  // fields: [buffer][ex ey ez hx hy hz][cells]; splits: [buffer][6 E splits, 6 H splits][cells]
-  encode_map(&m.E, s->fields.p, F, 4, s, 5, tx + 4, ty + 1, 3, N, 6 * N);
-  encode_map(&m.H, s->fields.p + 3 * N, F, 4, s, 5, tx + 8, ty + 2, 3, N, 6 * N);
-  if (s->splits.n) {
-    encode_map(&m.Es, s->splits.p, F, 4, s, 5, sew, ty + 1, 6, N, 12 * N);
-    encode_map(&m.Hs, s->splits.p + 6 * N, F, 4, s, 5, shw, ty, 6, N, 12 * N);
-  }
-  encode_map(&m.ids, s->mat.p, CU_TENSOR_MAP_DATA_TYPE_UINT16, 2, s, 3, tx + 8, ty + 1, 1, 0, 0);
 }
 
 // Tensor maps of the streaming kernel (box widths of StreamGeom).
@@ -311,32 +271,9 @@ struct StreamClass {
   }
 };
 
-// Tiles of one kernel class with everything one launch of that class needs.
-struct TileClass {
-  const TmaVariant* v = nullptr;
-  std::vector<TileDesc> host_tiles;
-  std::vector<TmaMaps> host_maps;
-  DevBuf<TmaMaps> d_maps;
-  DevBuf<SimDev> d_sims;
-  DevBuf<TileDesc> d_tiles;
-  DevBuf<unsigned> d_counter;
-  int n_tiles = 0, grid = 0;
-  void reset() {
-    v = nullptr;
-    host_tiles.clear();
-    host_maps.clear();
-    d_maps.free();
-    d_sims.free();
-    d_tiles.free();
-    d_counter.free();
-    n_tiles = grid = 0;
-  }
-};
-
 struct Engine {
   std::vector<fdtd_sim*> sims;
   KernelConfig cfg;
-  TileClass cls[2];        // 0: ordinary tiles (x-PML in split windows), 1: y/z-PML slabs (all split)
   StreamClass scls;        // streaming kernel
   DevBuf<SimDev> d_sims;   // plain kernel
   DevBuf<int4> d_tiles;    // plain kernel
@@ -373,15 +310,6 @@ struct Engine {
     graph_nt = -1;
   }
 
-  // Cut [x0,x1) x [y0,y1) x [z0,z1) of simulation `si` into tiles of (tx, ty, zc).
-  static void tile_region(std::vector<TileDesc>& out, int si, int x0, int x1, int y0, int y1, int z0, int z1, int tx,
-                          int ty, int zc) {
-    for (int z = z0; z < z1; z += zc)
-      for (int y = y0; y < y1; y += ty)
-        for (int x = x0; x < x1; x += tx)
-          out.push_back(TileDesc{si, x, y, z, std::min(z1, z + zc), std::min(x1, x + tx), std::min(y1, y + ty), -1});
-  }
-
   void build_tiles() {
     reset_graph();
     int dev = 0, n_sm = 148;
@@ -391,110 +319,11 @@ struct Engine {
       d_err.alloc(1);
       CK(cudaMemset(d_err.p, 0, sizeof(int)));
     }
-    if (cfg.variant == 2) {
-      build_stream_tiles(n_sm);
-      return;
-    }
     if (cfg.variant == 1) {
-      const TmaVariant* vv[2] = {find_variant(64, cfg.ty, cfg.stages, MODE_WINDOW), find_variant(64, 4, 4, MODE_FULL)};
-      if (!vv[0]) throw ArgError{FDTD_ERR_ARG, "No TMA kernel instantiated for this tile height / stage count."};
-      int per_sm[2];
-      for (int k = 0; k < 2; ++k) {
-        cls[k].reset();
-        cls[k].v = vv[k];
-        CK(cudaFuncSetAttribute(reinterpret_cast<const void*>(vv[k]->fn),
-                                cudaFuncAttributeMaxDynamicSharedMemorySize, vv[k]->smem));
-        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[k], reinterpret_cast<const void*>(vv[k]->fn),
-                                                         vv[k]->threads, vv[k]->smem));
-        if (per_sm[k] < 1) throw ArgError{FDTD_ERR_LIMIT, "TMA kernel does not fit on an SM."};
-      }
-      const int ty = cfg.ty;
-      std::vector<Box3> cores(sims.size());
-      std::vector<std::unique_ptr<GradedIndex>> gidx(sims.size());
-      int64_t cols = 0;
-      for (size_t i = 0; i < sims.size(); ++i) {
-        gidx[i] = std::make_unique<GradedIndex>(sims[i]->grid);
-        cores[i] = core_box(*gidx[i], 4, 8);
-        const int nyc = cores[i].empty() ? 0 : cores[i].y1 - cores[i].y0;
-        cols += int64_t((sims[i]->nx + 63) / 64) * ((nyc + ty - 1) / ty);
-      }
-      const int64_t slots = int64_t(per_sm[0]) * n_sm;
-      zchunk_used = 1 << 30;
-      for (size_t i = 0; i < sims.size(); ++i) {
-        fdtd_sim* s = sims[i];
-        const Box3& c = cores[i];
-        const GradedIndex& gi = *gidx[i];
-        int zc = cfg.zchunk;
-        if (zc <= 0) {
-          // about 8 tiles per resident block, chunks of at least 8 planes
-          const int64_t chunks = std::max<int64_t>(1, (slots * 8 + std::max<int64_t>(cols, 1) - 1) /
-                                                           std::max<int64_t>(cols, 1));
-          zc = int(std::max<int64_t>(8, ((c.empty() ? s->nz : c.z1 - c.z0) + chunks - 1) / chunks));
-        }
-        zchunk_used = std::min(zchunk_used, zc);
-        const int si = int(i);
-        for (int k = 0; k < 2; ++k) {
-          cls[k].host_maps.emplace_back();
-          encode_maps(cls[k].host_maps.back(), s, *vv[k]);
-        }
-        if (c.empty()) {
-          tile_region(cls[1].host_tiles, si, 0, s->nx, 0, s->ny, 0, s->nz, 64, 4, zc);
-          continue;
-        }
-        // ordinary tiles over all x; graded cells of their E region (the x-PML)
-        // must fit one 16-column window, otherwise the tile goes to the full class
-        std::vector<TileDesc> ord;
-        tile_region(ord, si, 0, s->nx, c.y0, c.y1, c.z0, c.z1, 64, ty, zc);
-        for (TileDesc t : ord) {
-          int gmin = 1 << 30, gmax = -1;
-          if (gi.count(t.x0 - 4, t.x0 + 64, t.y0 - 1, t.y1, t.z0 - 1, t.z1) > 0)
-            for (int x = std::max(0, t.x0 - 4); x < std::min(s->nx, t.x0 + 64); ++x)
-              if (gi.count(x, x + 1, t.y0 - 1, t.y1, t.z0 - 1, t.z1) > 0) {
-                gmin = std::min(gmin, x);
-                gmax = std::max(gmax, x);
-              }
-          if (gmax < 0) {
-            t.wx0 = -1;
-            cls[0].host_tiles.push_back(t);
-          } else {
-            const int w0 = gmin / 4 * 4;
-            if (gmax < w0 + kSplitWin) {
-              t.wx0 = w0;
-              cls[0].host_tiles.push_back(t);
-            } else {
-              tile_region(cls[1].host_tiles, si, t.x0, t.x1, t.y0, t.y1, t.z0, t.z1, 64, 4, zc);
-            }
-          }
-        }
-        // y- and z-PML slabs
-        tile_region(cls[1].host_tiles, si, 0, s->nx, 0, s->ny, 0, c.z0, 64, 4, zc);
-        tile_region(cls[1].host_tiles, si, 0, s->nx, 0, s->ny, c.z1, s->nz, 64, 4, zc);
-        tile_region(cls[1].host_tiles, si, 0, s->nx, 0, c.y0, c.z0, c.z1, 64, 4, zc);
-        tile_region(cls[1].host_tiles, si, 0, s->nx, c.y1, s->ny, c.z0, c.z1, 64, 4, zc);
-      }
-      n_tiles = 0;
-      grid = 0;
-      for (int k = 0; k < 2; ++k) {
-        TileClass& t = cls[k];
-        t.n_tiles = int(t.host_tiles.size());
-        if (!t.n_tiles) continue;
-        t.d_maps.alloc(t.host_maps.size());
-        CK(cudaMemcpy(t.d_maps.p, t.host_maps.data(), t.host_maps.size() * sizeof(TmaMaps), cudaMemcpyHostToDevice));
-        std::vector<SimDev> devs;
-        for (size_t i = 0; i < sims.size(); ++i) {
-          devs.push_back(sims[i]->dev);
-          devs.back().maps = t.d_maps.p + i;
-        }
-        t.d_sims.alloc(devs.size());
-        CK(cudaMemcpy(t.d_sims.p, devs.data(), devs.size() * sizeof(SimDev), cudaMemcpyHostToDevice));
-        t.d_tiles.alloc(t.host_tiles.size());
-        CK(cudaMemcpy(t.d_tiles.p, t.host_tiles.data(), t.host_tiles.size() * sizeof(TileDesc),
-                      cudaMemcpyHostToDevice));
-        t.d_counter.alloc(1);
-        t.grid = int(std::min<int64_t>(t.n_tiles, int64_t(per_sm[k]) * n_sm));
-        n_tiles += t.n_tiles;
-        grid += t.grid;
-      }
+      if (cfg.ty == 0)
+        autotune(n_sm);
+      else
+        build_stream_tiles(n_sm);
       return;
     }
     // plain kernel: 31 x 7 tiles, z cut into chunks
@@ -523,6 +352,64 @@ struct Engine {
     d_tiles.alloc(tiles.size());
     CK(cudaMemcpy(d_tiles.p, tiles.data(), tiles.size() * sizeof(int4), cudaMemcpyHostToDevice));
     n_tiles = int(tiles.size());
+  }
+
+  // Picks the streaming kernel's (tile height, stages, z chunk) for this set
+  // of grids: each candidate runs a few time steps on the simulations
+  // themselves (their fields are cleared again by the next run), the fastest
+  // is kept and remembered for the same grid sizes.
+  void autotune(int n_sm) {
+    std::vector<int> key;
+    int nt_min = 1 << 30;
+    for (auto* s : sims) {
+      key.insert(key.end(), {s->nx, s->ny, s->nz});
+      nt_min = std::min(nt_min, s->prepared_nt);
+    }
+    {
+      std::lock_guard<std::mutex> lock(g_tune_mutex);
+      auto it = g_tune_cache.find(key);
+      if (it != g_tune_cache.end()) {
+        cfg.ty = it->second[0];
+        cfg.stages = it->second[1];
+        cfg.zchunk = it->second[2];
+        build_stream_tiles(n_sm);
+        return;
+      }
+    }
+    const int warm = 2, timed = std::min(8, nt_min - warm);
+    std::array<int, 3> best = {kTuneCandidates[0][0], kTuneCandidates[0][1], kTuneCandidates[0][2]};
+    if (timed >= 2) {
+      init();
+      cudaStream_t st = stream();
+      float best_ms = 1e30f;
+      for (const auto& cand : kTuneCandidates) {
+        cfg.ty = cand[0];
+        cfg.stages = cand[1];
+        cfg.zchunk = cand[2];
+        build_stream_tiles(n_sm);
+        CK(cudaMemsetAsync(scls.d_counter.p, 0, sizeof(unsigned), st));
+        for (int n = 0; n < warm; ++n) launch_step(st, n);
+        CK(cudaEventRecord(ev0, st));
+        for (int n = warm; n < warm + timed; ++n) launch_step(st, n);
+        CK(cudaEventRecord(ev1, st));
+        CK(cudaStreamSynchronize(st));
+        float ms = 0;
+        CK(cudaEventElapsedTime(&ms, ev0, ev1));
+        if (ms < best_ms) {
+          best_ms = ms;
+          best = {cand[0], cand[1], cand[2]};
+        }
+      }
+      check_error();
+    }
+    {
+      std::lock_guard<std::mutex> lock(g_tune_mutex);
+      g_tune_cache[key] = best;
+    }
+    cfg.ty = best[0];
+    cfg.stages = best[1];
+    cfg.zchunk = best[2];
+    build_stream_tiles(n_sm);
   }
 
   // Streaming kernel: 31 x TY column tiles cut in z chunks of at most 62
@@ -599,7 +486,7 @@ struct Engine {
     std::vector<SimDev> devs;
     for (size_t i = 0; i < sims.size(); ++i) {
       devs.push_back(sims[i]->dev);
-      devs.back().maps = reinterpret_cast<const TmaMaps*>(c.d_maps.p + i);
+      devs.back().maps = c.d_maps.p + i;
     }
     c.d_sims.alloc(devs.size());
     CK(cudaMemcpy(c.d_sims.p, devs.data(), devs.size() * sizeof(SimDev), cudaMemcpyHostToDevice));
@@ -612,23 +499,12 @@ struct Engine {
   }
 
   void launch_step(cudaStream_t st, int n) {
-    if (cfg.variant == 2) {
+    if (cfg.variant == 1) {
       StreamClass& c = scls;
       const unsigned base = unsigned(n) * unsigned(c.n_tiles + c.grid);
       c.v->fn<<<c.grid, c.v->threads, c.v->smem, st>>>(c.d_sims.p, c.d_tiles.p, c.n_tiles, n, c.d_counter.p, base,
                                                         d_err.p);
       CK(cudaGetLastError());
-      return;
-    }
-    if (cfg.variant == 1) {
-      for (int k = 0; k < 2; ++k) {
-        TileClass& t = cls[k];
-        if (!t.n_tiles) continue;
-        const unsigned base = unsigned(n) * unsigned(t.n_tiles + t.grid);
-        t.v->fn<<<t.grid, t.v->threads, t.v->smem, st>>>(t.d_sims.p, t.d_tiles.p, t.n_tiles, n, t.d_counter.p, base,
-                                                          d_err.p);
-        CK(cudaGetLastError());
-      }
     } else {
       fdtd_step_kernel<kTileY><<<n_tiles, dim3(32, kBlockY), 0, st>>>(d_sims.p, d_tiles.p, n);
       CK(cudaGetLastError());
@@ -646,8 +522,6 @@ struct Engine {
       for (size_t m = 0; m < s->monitors.size(); ++m)
         CK(cudaMemsetAsync(s->mon_out[m]->p, 0, s->mon_out[m]->n, st));
     }
-    for (auto& t : cls)
-      if (t.d_counter.n) CK(cudaMemsetAsync(t.d_counter.p, 0, sizeof(unsigned), st));
     if (scls.d_counter.n) CK(cudaMemsetAsync(scls.d_counter.p, 0, sizeof(unsigned), st));
     int dft_from = 0;
     for (int n = 0; n < nt; ++n) {
@@ -711,14 +585,18 @@ struct Engine {
       last_ms = ms;
       timing_pending = false;
     }
-    if (d_err.n) {
-      int e = 0;
-      CK(cudaMemcpy(&e, d_err.p, sizeof(int), cudaMemcpyDeviceToHost));
-      if (e) {
-        CK(cudaMemset(d_err.p, 0, sizeof(int)));
-        throw ArgError{FDTD_ERR_DEVICE, "step kernel gave up waiting for a TMA plane load (code " +
-                                            std::to_string(e) + ")"};
-      }
+    check_error();
+  }
+
+  // Reads (and clears) the error code the step kernel records when a bounded wait expires.
+  void check_error() {
+    if (!d_err.n) return;
+    int e = 0;
+    CK(cudaMemcpy(&e, d_err.p, sizeof(int), cudaMemcpyDeviceToHost));
+    if (e) {
+      CK(cudaMemset(d_err.p, 0, sizeof(int)));
+      throw ArgError{FDTD_ERR_DEVICE, "step kernel gave up waiting for a TMA plane load (code " +
+                                          std::to_string(e) + ")"};
     }
   }
 };
@@ -1056,7 +934,7 @@ int fdtd_get_material_table(fdtd_sim* s, uint16_t* ids, int64_t n_ids, uint32_t*
 int fdtd_set_kernel(fdtd_sim* s, int variant, int tile_y, int stages, int zchunk) {
   if (!s) return FDTD_ERR_ARG;
   return guarded(&s->err, [&] {
-    if (variant < 0 || variant > 2) throw ArgError{FDTD_ERR_ARG, "variant must be 0 (plain), 1 (tma) or 2 (stream)"};
+    if (variant < 0 || variant > 1) throw ArgError{FDTD_ERR_ARG, "variant must be 0 (plain) or 1 (stream)"};
     if (!kernel_exists(variant, tile_y, stages))
       throw ArgError{FDTD_ERR_ARG, "No kernel instantiated for this variant / tile height / stage count."};
     KernelConfig c;
@@ -1185,7 +1063,7 @@ int fdtd_batch_create(fdtd_sim* const* sims, int n_sims, fdtd_batch** out) {
 int fdtd_batch_set_kernel(fdtd_batch* b, int variant, int tile_y, int stages, int zchunk) {
   if (!b) return FDTD_ERR_ARG;
   return guarded(&b->err, [&] {
-    if (variant < 0 || variant > 2) throw ArgError{FDTD_ERR_ARG, "variant must be 0 (plain), 1 (tma) or 2 (stream)"};
+    if (variant < 0 || variant > 1) throw ArgError{FDTD_ERR_ARG, "variant must be 0 (plain) or 1 (stream)"};
     if (!kernel_exists(variant, tile_y, stages))
       throw ArgError{FDTD_ERR_ARG, "No kernel instantiated for this variant / tile height / stage count."};
     b->engine.cfg.variant = variant;

@@ -39,10 +39,9 @@ constexpr int kBlockY = kTileY + 1;
 
 constexpr uint32_t kESplit = 1u, kHSplit = 2u;
 
-struct TmaMaps;
 
 struct SimDev {
-  const TmaMaps* maps;    // tensor maps of the TMA kernel (set per engine)
+  const void* maps;       // tensor maps of the streaming kernel (set per engine)
   int nx, ny, nz, pitch;  // cells; pitch = floats per x row
   int plane;              // ny * pitch
   int nt;

@@ -139,16 +139,6 @@ def _engine_probe_matrix(s, variant, **kw):
     return out, st
 
 
-@pytest.mark.parametrize("ty,stages,zchunk", [(7, 4, 0), (8, 3, 5), (4, 6, 0), (16, 3, 7)])
-def test_tma_kernel_bitwise_equals_plain(engine_lib, ty, stages, zchunk):
-    """The TMA-pipelined kernel evaluates the same expressions as the plain one."""
-    s = configs.microstrip(n=(72, 40, 30), n_pml=5, nt=150)
-    a, sa = _engine_probe_matrix(s, 0)
-    b, sb = _engine_probe_matrix(s, 1, tile_y=ty, stages=stages, zchunk=zchunk)
-    assert sa["variant"] == 0 and sb["variant"] == 1
-    assert np.array_equal(a, b)
-
-
 @pytest.mark.parametrize("ty,stages,zchunk", [(8, 3, 0), (8, 4, 5), (4, 4, 0), (4, 5, 62), (6, 3, 7), (6, 4, 0),
                                               (12, 3, 0)])
 def test_stream_kernel_bitwise_equals_plain(engine_lib, ty, stages, zchunk):
@@ -159,7 +149,7 @@ def test_stream_kernel_bitwise_equals_plain(engine_lib, ty, stages, zchunk):
               configs.boxes(n=(70, 45, 38), n_pml=6, n_boxes=6, nt=120, n_ports=2, n_probes=4))
     for s in models:
         a, sa = _engine_probe_matrix(s, 0)
-        b, sb = _engine_probe_matrix(s, 2, tile_y=ty, stages=stages, zchunk=zchunk)
-        assert sa["variant"] == 0 and sb["variant"] == 2
+        b, sb = _engine_probe_matrix(s, 1, tile_y=ty, stages=stages, zchunk=zchunk)
+        assert sa["variant"] == 0 and sb["variant"] == 1
         assert np.abs(a).max() > 0
         assert np.array_equal(a, b)
