@@ -62,9 +62,10 @@ def parse_args():
     ap.add_argument("--nt", type=int, default=NT, help="time steps per simulation")
     ap.add_argument("--e2e-steps", type=int, default=None, help="end-to-end calls timed (default: --steps)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", choices=("boxes", "batch"), default="boxes",
+    ap.add_argument("--workload", choices=("boxes", "batch", "adjoint"), default="boxes",
                     help="boxes: the bandwidth model (default); batch: 64 uneven simulations in one launch "
-                         "per step against 64 sequential single-simulation runs")
+                         "per step against 64 sequential single-simulation runs; adjoint: forward + discrete "
+                         "adjoint gradient of a 48x48x4 permittivity design against one forward solve")
     return ap.parse_args()
 
 
@@ -421,6 +422,67 @@ def run_batch(args, rank, world, local_rank):
     }
 
 
+# ---------------------------------------------------------- adjoint workload
+
+def run_adjoint(args, rank, world, local_rank):
+    """128x128x96 microstrip, 10-cell PML, 4000 steps; a 48x48x4-cell design block above
+    the strip with eps_r = 1 + 9 sigmoid(theta), theta ~ N(0, 1) (seed 4); J = sum over
+    11 frequencies (8-12 GHz) of |DFT of the output Ez probe|^2; checkpoints every 64 steps.
+    One step = one gradient evaluation (forward with checkpoints + adjoint sweep)."""
+    import torch
+    from rfnetwork_b200 import configs
+    from rfnetwork_b200.adjoint import FDTDDesign
+
+    torch.cuda.set_device(local_rank)
+    nt = args.nt if args.nt != NT else 4000
+    s = configs.microstrip(n=(128, 128, 96), n_pml=10, nt=nt)
+    co, pr, *_ = s.pack_inputs(gpu=True)
+    omega = 2 * np.pi * np.linspace(8e9, 12e9, 11) * float(s.dt)
+    box = (40, 88, 40, 88, 25, 29)
+    design = FDTDDesign(s, box, [(0, len(pr) - 1, 1.0)], omega, checkpoint_every=64)
+    gen = torch.Generator().manual_seed(4)
+    theta = torch.randn(48, 48, 4, dtype=torch.float64, generator=gen)
+
+    def grad_eval():
+        t = theta.clone().requires_grad_(True)
+        J = (design(1 + 9 * torch.sigmoid(t)).abs() ** 2).sum()
+        J.backward()
+        return float(J), t.grad
+
+    for _ in range(max(args.warmup, 1)):
+        grad_eval()
+    t_grad, t_fwd = [], []
+    for _ in range(args.steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        J, g = grad_eval()
+        torch.cuda.synchronize()
+        t_grad.append(time.perf_counter() - t0)
+    design.forward_only(1 + 9 * torch.sigmoid(theta))
+    for _ in range(args.steps):   # the plain forward solve of the same design, for the ratio
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        design.forward_only(1 + 9 * torch.sigmoid(theta))
+        torch.cuda.synchronize()
+        t_fwd.append(time.perf_counter() - t0)
+    fwd_dev = design.sim.stats()["last_run_ms"] / 1e3
+    design.close()
+    if rank != 0:
+        return None
+    tg, tf = statistics.fmean(t_grad), statistics.fmean(t_fwd)
+    return {
+        "metric": "grad evals/s", "value": round(world / tg, 4), "unit": "gradient evaluations/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(tg * 1e3, 1),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32 fields, f64 accumulators",
+        "data": "synthetic: microstrip background, seeded theta",
+        "config": {"workload": f"adjoint: 128x128x96, 10-cell PML, {nt} steps, 48x48x4 design, 11 freqs, "
+                               "checkpoints every 64", "time_steps": nt, "design_cells": 48 * 48 * 4,
+                   "step": "one gradient evaluation (forward with checkpoints + adjoint), wall time"},
+        "forward_s": round(tf, 3), "forward_device_s": round(fwd_dev, 3),
+        "gradient_over_forward": round(tg / tf, 3), "J": J,
+    }
+
+
 def main():
     args = parse_args()
     rank = int(os.environ.get("RANK", 0))
@@ -430,6 +492,8 @@ def main():
         out = run_reference(args, rank, world)
     elif args.workload == "batch":
         out = run_batch(args, rank, world, local_rank)
+    elif args.workload == "adjoint":
+        out = run_adjoint(args, rank, world, local_rank)
     else:
         out = run_ours(args, rank, world, local_rank)
         if rank == 0 and world == 1 and not args.no_cpu_baseline:

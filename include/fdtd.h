@@ -144,6 +144,30 @@ int fdtd_get_stats(const fdtd_sim* s, fdtd_stats* out);
 const char* fdtd_last_error(const fdtd_sim* s);
 void fdtd_destroy(fdtd_sim* s);
 
+/* -------------------------------------------------------------- gradients */
+
+/* Like fdtd_run, and keeps a snapshot of the whole field state every `every`
+ * steps (ceil(nt/every) snapshots of 6 N floats, plus 12 N when split fields
+ * exist) for fdtd_adjoint. The reference has no gradient path; this and
+ * fdtd_adjoint have no counterpart there. Any later fdtd_run drops the
+ * snapshots. */
+int fdtd_run_checkpointed(fdtd_sim* s, int nt, int every);
+
+/* Gradient of a real objective J of the last checkpointed run's device DFT
+ * (fdtd_set_dft) with respect to the E-update coefficients of the cells of a
+ * box: box = {x0, x1, y0, y1, z0, z1} in cell indices (the coefficient arrays'
+ * indices), cells that are not split (no PML, no source).
+ *   dJ_dX  n_series x n_freq x 2 doubles: dJ/dRe X + i dJ/dIm X (the gradient
+ *          torch hands a complex output)
+ *   grad   3 x 3 x box cells doubles, [component ex ey ez][Ca, Cb1, Cb2][x][y][z]:
+ *          dJ/d(Ca_e*), dJ/d(first Cb_e*), dJ/d(second Cb_e*) in the coefficient
+ *          dict's order (Ca_ex_y with Ca_ex_z held equal, Cb_ex_y, Cb_ex_z, ...)
+ * The discrete adjoint runs backwards through the checkpoints: each segment is
+ * recomputed from its snapshot to record the box's forward fields, then
+ * reversed with the transposed update in FP32, the products accumulated in
+ * FP64. */
+int fdtd_adjoint(fdtd_sim* s, const double* dJ_dX, int n_series, int n_freq, const int* box, double* grad);
+
 /* ---------------------------------------------------------------- batches */
 
 /* Many independent simulations of uneven sizes stepped together: one kernel

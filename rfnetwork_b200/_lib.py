@@ -22,6 +22,7 @@ EXPORTED = (
     "fdtd_get_dft", "fdtd_get_monitor", "fdtd_get_stats", "fdtd_last_error", "fdtd_destroy",
     "fdtd_batch_create", "fdtd_batch_run", "fdtd_batch_set_stream", "fdtd_batch_get_stats",
     "fdtd_batch_last_error", "fdtd_batch_destroy", "fdtd_global_error", "fdtd_step_noalloc",
+    "fdtd_run_checkpointed", "fdtd_adjoint",
 )
 
 
@@ -81,6 +82,8 @@ def load():
         "fdtd_batch_last_error": ([vp], ctypes.c_char_p),
         "fdtd_batch_destroy": ([vp], None),
         "fdtd_global_error": ([], ctypes.c_char_p),
+        "fdtd_run_checkpointed": ([vp, ip, ip], ip),
+        "fdtd_adjoint": ([vp, vp, ip, ip, vp, vp], ip),
     }
     for name, (args, res) in sig.items():
         fn = getattr(lib, name)
@@ -205,6 +208,22 @@ class Simulation:
     def run(self, nt: int):
         self._check(self.lib.fdtd_run(self.h, int(nt)))
         self.nt = int(nt)
+
+    def run_checkpointed(self, nt: int, every: int):
+        """Run like ``run`` and keep a field snapshot every ``every`` steps for ``adjoint``."""
+        self._check(self.lib.fdtd_run_checkpointed(self.h, int(nt), int(every)))
+        self.nt = int(nt)
+
+    def adjoint(self, dJ_dX: np.ndarray, box) -> np.ndarray:
+        """Gradient [3 components, (Ca, Cb1, Cb2), *box shape] of J given dJ/dX of the device DFT.
+
+        dJ_dX: complex [n_series, n_freq] (dJ/dRe X + i dJ/dIm X); box: (x0, x1, y0, y1, z0, z1)."""
+        g = np.ascontiguousarray(np.stack([np.real(dJ_dX), np.imag(dJ_dX)], axis=-1), dtype=np.float64)
+        b = np.ascontiguousarray(box, dtype=np.int32)
+        shape = (3, 3, b[1] - b[0], b[3] - b[2], b[5] - b[4])
+        out = np.empty(shape, dtype=np.float64)
+        self._check(self.lib.fdtd_adjoint(self.h, _ptr(g), g.shape[0], g.shape[1], _ptr(b), _ptr(out)))
+        return out
 
     def run_async(self, nt: int):
         self._check(self.lib.fdtd_run_async(self.h, int(nt)))

@@ -24,6 +24,7 @@
 #include "../../include/fdtd.h"
 #include "fdtd_compile.h"
 #include "fdtd_kernels.cuh"
+#include "fdtd_adjoint.cuh"
 #include "fdtd_step_stream.cuh"
 #include <cudaTypedefs.h>
 
@@ -159,6 +160,12 @@ struct fdtd_sim {
   std::string err;
   fdtd_stats stats{};
   int64_t h2d_bytes = 0, d2h_bytes = 0;  // bytes copied over PCIe/C2C by this simulation
+  // state snapshots of the last checkpointed run (fdtd_run_checkpointed), one
+  // per segment of ckpt_every steps: the 6 field arrays of the time buffer
+  // the segment starts from, then (when allocated) its 12 split arrays
+  int ckpt_every = 0;
+  int ckpt_nt = -1;
+  DevBuf<float> ckpt;
 };
 
 // Host-to-device copy that counts its bytes on the simulation.
@@ -511,6 +518,114 @@ struct Engine {
     }
   }
 
+  // Discrete adjoint of the last checkpointed run of simulation s (the only
+  // member of this engine): gradient of J with respect to (Ca, Cb1, Cb2) of
+  // each E component on the box, given dJ/dX of the device DFT. The run is
+  // replayed segment by segment from its checkpoints, last segment first; each
+  // segment's forward history of the box is captured, then its steps are
+  // reversed with the adjoint kernels (fdtd_adjoint.cuh).
+  void adjoint(fdtd_sim* s, const double* dJdX, const int* box, double* grad_out) {
+    init();
+    cudaStream_t st = stream();
+    const int nt = s->ckpt_nt, K = s->ckpt_every;
+    const size_t N = s->cells_padded;
+    const int bnx = box[1] - box[0], bny = box[3] - box[2], bnz = box[5] - box[4];
+    const int64_t nb = int64_t(bnx) * bny * bnz;
+    const int P = int(s->probes.size());
+    // dJ/d(record of probe p at step n) = sum over the DFT terms (series, p, w)
+    // of w * sum_f (Re G_sf cos(w_f n) - Im G_sf sin(w_f n)), G = dJ/dX
+    std::vector<float> radj(size_t(std::max(P, 1)) * nt, 0.f);
+    {
+      std::vector<double> acc(static_cast<size_t>(nt));
+      for (int se = 0; se < s->n_series; ++se) {
+        std::fill(acc.begin(), acc.end(), 0.0);
+        for (int f = 0; f < s->n_freq; ++f) {
+          const double gr = dJdX[(size_t(se) * s->n_freq + f) * 2], gi = dJdX[(size_t(se) * s->n_freq + f) * 2 + 1];
+          if (gr == 0.0 && gi == 0.0) continue;
+          const double om = s->omega[size_t(f)];
+          for (int n = 0; n < nt; ++n) acc[size_t(n)] += gr * std::cos(om * n) - gi * std::sin(om * n);
+        }
+        for (int t = s->series_start[size_t(se)]; t < s->series_start[size_t(se) + 1]; ++t) {
+          const int p = s->term_probe[size_t(t)];
+          const double w = s->term_weight[size_t(t)];
+          for (int n = 0; n < nt; ++n) radj[size_t(p) * nt + n] += float(w * acc[size_t(n)]);
+        }
+      }
+    }
+    std::vector<int> pidx(size_t(std::max(P, 1)), 0), pfld(size_t(std::max(P, 1)), 0);
+    for (int p = 0; p < P; ++p) {
+      const int64_t cell = s->grid.probe_cell[size_t(p)];
+      const int z = int(cell % s->nz), y = int((cell / s->nz) % s->ny), x = int(cell / (int64_t(s->nz) * s->ny));
+      pidx[size_t(p)] = z * s->ny * s->pitch + y * s->pitch + x;
+      pfld[size_t(p)] = s->probes[size_t(p)].field;
+    }
+    DevBuf<float> lamE, lamH, qb, adb, hist, d_radj;
+    DevBuf<double> grad;
+    DevBuf<int> d_pidx, d_pfld;
+    lamE.alloc(6 * N);
+    lamH.alloc(6 * N);
+    qb.alloc(6 * N);
+    adb.alloc(6 * N);
+    hist.alloc(size_t(K) * 9 * size_t(nb));
+    grad.alloc(9 * size_t(nb));
+    d_radj.alloc(radj.size());
+    d_pidx.alloc(pidx.size());
+    d_pfld.alloc(pfld.size());
+    CK(cudaMemcpy(d_radj.p, radj.data(), radj.size() * sizeof(float), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(d_pidx.p, pidx.data(), pidx.size() * sizeof(int), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(d_pfld.p, pfld.data(), pfld.size() * sizeof(int), cudaMemcpyHostToDevice));
+    CK(cudaMemsetAsync(lamE.p, 0, 6 * N * sizeof(float), st));
+    CK(cudaMemsetAsync(lamH.p, 0, 6 * N * sizeof(float), st));
+    CK(cudaMemsetAsync(qb.p, 0, 6 * N * sizeof(float), st));
+    CK(cudaMemsetAsync(grad.p, 0, 9 * size_t(nb) * sizeof(double), st));
+    AdjDev a{};
+    a.s = s->dev;
+    a.lamE = lamE.p;
+    a.lamH = lamH.p;
+    a.q = qb.p;
+    a.ad = adb.p;
+    a.N = int64_t(N);
+    a.bx0 = box[0]; a.bx1 = box[1]; a.by0 = box[2]; a.by1 = box[3]; a.bz0 = box[4]; a.bz1 = box[5];
+    a.grad = grad.p;
+    const dim3 blk(32, 8), grd((s->nx + 31) / 32, (s->ny + 7) / 8, s->nz);
+    const int cap_blocks = int(std::min<int64_t>(1024, (nb + 255) / 256));
+    const size_t stride = 6 * N + (s->splits.n ? 12 * N : 0);
+    const int nseg = (nt + K - 1) / K;
+    for (int k = nseg - 1; k >= 0; --k) {
+      const int n0 = k * K, n1 = std::min(nt, n0 + K);
+      const size_t b = size_t(n0 & 1);
+      const float* src = s->ckpt.p + size_t(k) * stride;
+      CK(cudaMemcpyAsync(s->fields.p + b * 6 * N, src, 6 * N * sizeof(float), cudaMemcpyDeviceToDevice, st));
+      if (s->splits.n)
+        CK(cudaMemcpyAsync(s->splits.p + b * 12 * N, src + 6 * N, 12 * N * sizeof(float), cudaMemcpyDeviceToDevice,
+                           st));
+      if (cfg.variant == 1) {
+        // the streaming kernel's tile counter as it stood before step n0
+        const unsigned c0 = unsigned(n0) * unsigned(scls.n_tiles + scls.grid);
+        CK(cudaMemcpyAsync(scls.d_counter.p, &c0, sizeof(unsigned), cudaMemcpyHostToDevice, st));
+        CK(cudaStreamSynchronize(st));  // c0 lives on this stack frame
+      }
+      for (int n = n0; n < n1; ++n) {
+        adj_capture_kernel<<<cap_blocks, 256, 0, st>>>(a, n & 1, hist.p + size_t(n - n0) * 9 * size_t(nb));
+        CK(cudaGetLastError());
+        launch_step(st, n);
+      }
+      for (int n = n1 - 1; n >= n0; --n) {
+        a.hist = hist.p + size_t(n - n0) * 9 * size_t(nb);
+        if (P > 0) {
+          adj_probe_kernel<<<(P + 127) / 128, 128, 0, st>>>(a, d_pidx.p, d_pfld.p, d_radj.p, P, nt, n);
+          CK(cudaGetLastError());
+        }
+        adj_e_kernel<<<grd, blk, 0, st>>>(a);
+        adj_h_kernel<<<grd, blk, 0, st>>>(a);
+        CK(cudaGetLastError());
+      }
+    }
+    CK(cudaStreamSynchronize(st));
+    check_error();
+    CK(cudaMemcpy(grad_out, grad.p, 9 * size_t(nb) * sizeof(double), cudaMemcpyDeviceToHost));
+  }
+
   // Enqueue one full run of nt steps on stream st (used for capture and for
   // direct launches alike).
   void enqueue(cudaStream_t st, int nt) {
@@ -525,6 +640,16 @@ struct Engine {
     if (scls.d_counter.n) CK(cudaMemsetAsync(scls.d_counter.p, 0, sizeof(unsigned), st));
     int dft_from = 0;
     for (int n = 0; n < nt; ++n) {
+      for (auto* s : sims)
+        if (s->ckpt_every > 0 && n % s->ckpt_every == 0 && s->ckpt.n) {
+          const size_t N = s->cells_padded, b = size_t(n & 1);
+          const size_t stride = 6 * N + (s->splits.n ? 12 * N : 0);
+          float* dst = s->ckpt.p + size_t(n / s->ckpt_every) * stride;
+          CK(cudaMemcpyAsync(dst, s->fields.p + b * 6 * N, 6 * N * sizeof(float), cudaMemcpyDeviceToDevice, st));
+          if (s->splits.n)
+            CK(cudaMemcpyAsync(dst + 6 * N, s->splits.p + b * 12 * N, 12 * N * sizeof(float),
+                               cudaMemcpyDeviceToDevice, st));
+        }
       launch_step(st, n);
       ++step_launches;
       for (auto* s : sims)
@@ -958,6 +1083,12 @@ int fdtd_run_async(fdtd_sim* s, int nt) {
   if (!s) return FDTD_ERR_ARG;
   return guarded(&s->err, [&] {
     if (nt < 1) throw ArgError{FDTD_ERR_ARG, "nt must be positive."};
+    if (s->ckpt_every) {  // leave checkpoint mode: the time loop is captured without snapshots again
+      s->ckpt_every = 0;
+      s->ckpt.free();
+      s->ckpt_nt = -1;
+      s->engine.reset();
+    }
     const bool rebuild = !s->prepared || s->prepared_nt != nt || !s->engine;
     prepare(s, nt);
     if (rebuild) {
@@ -969,6 +1100,58 @@ int fdtd_run_async(fdtd_sim* s, int nt) {
     }
     s->engine->run_async(nt);
     fill_stats(s, s->engine.get());
+  });
+}
+
+int fdtd_run_checkpointed(fdtd_sim* s, int nt, int every) {
+  if (!s) return FDTD_ERR_ARG;
+  const int rc = guarded(&s->err, [&] {
+    if (nt < 1 || every < 1) throw ArgError{FDTD_ERR_ARG, "nt and the checkpoint interval must be positive."};
+    // a re-prepared simulation has new device buffers: the engine (descriptors,
+    // tensor maps, graph) must be rebuilt with it
+    const bool rebuild = !s->prepared || s->prepared_nt != nt || !s->engine || s->ckpt_every != every ||
+                         s->ckpt_nt != nt;
+    prepare(s, nt);
+    const size_t N = s->cells_padded;
+    const size_t stride = 6 * N + (s->splits.n ? 12 * N : 0);
+    const size_t nseg = size_t((nt + every - 1) / every);
+    if (rebuild) {
+      s->engine = std::make_unique<Engine>();
+      s->engine->sims = {s};
+      s->engine->cfg = s->cfg;
+      s->engine->ext_stream = s->ext_stream;
+      s->engine->build_tiles();
+    }
+    s->ckpt_every = every;
+    s->ckpt_nt = nt;
+    if (s->ckpt.n != nseg * stride) s->ckpt.alloc(nseg * stride);
+    s->engine->run_async(nt);
+    fill_stats(s, s->engine.get());
+  });
+  if (rc) return rc;
+  return fdtd_synchronize(s);
+}
+
+int fdtd_adjoint(fdtd_sim* s, const double* dJ_dX, int n_series, int n_freq, const int* box, double* grad) {
+  if (!s) return FDTD_ERR_ARG;
+  return guarded(&s->err, [&] {
+    if (!dJ_dX || !box || !grad) throw ArgError{FDTD_ERR_ARG, "null argument"};
+    if (!s->engine || s->ckpt_every < 1 || s->ckpt_nt < 1 || !s->ckpt.n)
+      throw ArgError{FDTD_ERR_STATE, "fdtd_adjoint needs a preceding fdtd_run_checkpointed."};
+    if (n_series != s->n_series || n_freq != s->n_freq || n_series < 1 || n_freq < 1)
+      throw ArgError{FDTD_ERR_ARG, "dJ/dX size does not match the DFT of the run."};
+    if (s->engine->sims.size() != 1) throw ArgError{FDTD_ERR_STATE, "adjoint runs need a single simulation."};
+    if (box[0] < 0 || box[2] < 0 || box[4] < 0 || box[1] > s->nx || box[3] > s->ny || box[5] > s->nz ||
+        box[0] >= box[1] || box[2] >= box[3] || box[4] >= box[5])
+      throw ArgError{FDTD_ERR_ARG, "gradient box must be a non-empty box inside the grid."};
+    for (int x = box[0]; x < box[1]; ++x)
+      for (int y = box[2]; y < box[3]; ++y)
+        for (int z = box[4]; z < box[5]; ++z) {
+          const uint32_t f = s->grid.rows[s->grid.ids[(size_t(x) * s->ny + y) * s->nz + z]].w[R_FLAGS];
+          if (f & kFlagESplit)
+            throw ArgError{FDTD_ERR_ARG, "gradient box holds split-field (PML or source) cells."};
+        }
+    s->engine->adjoint(s, dJ_dX, box, grad);
   });
 }
 
