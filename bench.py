@@ -62,10 +62,11 @@ def parse_args():
     ap.add_argument("--nt", type=int, default=NT, help="time steps per simulation")
     ap.add_argument("--e2e-steps", type=int, default=None, help="end-to-end calls timed (default: --steps)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", choices=("boxes", "batch", "adjoint"), default="boxes",
+    ap.add_argument("--workload", choices=("boxes", "batch", "adjoint", "design"), default="boxes",
                     help="boxes: the bandwidth model (default); batch: 64 uneven simulations in one launch "
                          "per step against 64 sequential single-simulation runs; adjoint: forward + discrete "
-                         "adjoint gradient of a 48x48x4 permittivity design against one forward solve")
+                         "adjoint gradient of a 48x48x4 permittivity design against one forward solve; "
+                         "design: Adam steps on 32 design variants, batched forward and batched adjoint")
     return ap.parse_args()
 
 
@@ -397,13 +398,27 @@ def run_batch(args, rank, world, local_rank):
             tot += s.stats()["last_run_ms"]
         t_seq.append(tot)
     same = all(np.array_equal(s.probe_values(), r) for s, r in zip(sims, recs))
+    # and one after another with the plain kernel, every step launched from the
+    # host (no graph), as the reference's engine runs a simulation
+    t_plain = []
+    for s in sims:
+        s.set_kernel(0)
+        s.set_graph(False)
+        s.run(nt)
+    for _ in range(args.steps):
+        tot = 0.0
+        for s in sims:
+            s.run(nt)
+            tot += s.stats()["last_run_ms"]
+        t_plain.append(tot)
+    same = same and all(np.array_equal(s.probe_values(), r) for s, r in zip(sims, recs))
     st = batch.stats()
     batch.close()
     for s in sims:
         s.close()
     if rank != 0:
         return None
-    ms_b, ms_s = statistics.fmean(t_batch), statistics.fmean(t_seq)
+    ms_b, ms_s, ms_p = statistics.fmean(t_batch), statistics.fmean(t_seq), statistics.fmean(t_plain)
     return {
         "metric": "batched sims/s", "value": round(world * BATCH_SIMS / (ms_b * 1e-3), 3), "unit": "sims/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_b, 2),
@@ -416,6 +431,11 @@ def run_batch(args, rank, world, local_rank):
         "sequential": {"value": round(world * BATCH_SIMS / (ms_s * 1e-3), 3), "unit": "sims/s",
                        "ms_per_step": round(ms_s, 2)},
         "batched_over_sequential": round(ms_s / ms_b, 3),
+        "sequential_plain_launches": {"value": round(world * BATCH_SIMS / (ms_p * 1e-3), 3), "unit": "sims/s",
+                                      "ms_per_step": round(ms_p, 2),
+                                      "how": "fdtd_run per simulation, plain kernel, every step launched "
+                                             "from the host (no CUDA graph); device time incl. launch gaps"},
+        "batched_over_sequential_plain_launches": round(ms_p / ms_b, 3),
         "mcell_updates_per_s": round(world * cells * nt / (ms_b * 1e-3) / 1e6, 1),
         "bit_identical_to_sequential": same,
         "gpu_launches": int(st["step_launches"] + st["dft_launches"]) * args.steps,
@@ -428,7 +448,8 @@ def run_adjoint(args, rank, world, local_rank):
     """128x128x96 microstrip, 10-cell PML, 4000 steps; a 48x48x4-cell design block above
     the strip with eps_r = 1 + 9 sigmoid(theta), theta ~ N(0, 1) (seed 4); J = sum over
     11 frequencies (8-12 GHz) of |DFT of the output Ez probe|^2; checkpoints every 64 steps.
-    One step = one gradient evaluation (forward with checkpoints + adjoint sweep)."""
+    One step = one gradient evaluation (forward with checkpoints + adjoint sweep). The same
+    gradient with the box history recorded instead of checkpoints is reported beside it."""
     import torch
     from rfnetwork_b200 import configs
     from rfnetwork_b200.adjoint import FDTDDesign
@@ -439,47 +460,140 @@ def run_adjoint(args, rank, world, local_rank):
     co, pr, *_ = s.pack_inputs(gpu=True)
     omega = 2 * np.pi * np.linspace(8e9, 12e9, 11) * float(s.dt)
     box = (40, 88, 40, 88, 25, 29)
-    design = FDTDDesign(s, box, [(0, len(pr) - 1, 1.0)], omega, checkpoint_every=64)
     gen = torch.Generator().manual_seed(4)
     theta = torch.randn(48, 48, 4, dtype=torch.float64, generator=gen)
 
-    def grad_eval():
-        t = theta.clone().requires_grad_(True)
-        J = (design(1 + 9 * torch.sigmoid(t)).abs() ** 2).sum()
-        J.backward()
-        return float(J), t.grad
+    def measure(design):
+        def grad_eval():
+            t = theta.clone().requires_grad_(True)
+            J = (design(1 + 9 * torch.sigmoid(t)).abs() ** 2).sum()
+            J.backward()
+            return float(J.detach()), t.grad
 
-    for _ in range(max(args.warmup, 1)):
-        grad_eval()
-    t_grad, t_fwd = [], []
-    for _ in range(args.steps):
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        J, g = grad_eval()
-        torch.cuda.synchronize()
-        t_grad.append(time.perf_counter() - t0)
-    design.forward_only(1 + 9 * torch.sigmoid(theta))
-    for _ in range(args.steps):   # the plain forward solve of the same design, for the ratio
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
+        for _ in range(max(args.warmup, 1)):
+            grad_eval()
+        t_grad, fwd_dev, adj_dev = [], [], []
+        for _ in range(args.steps):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            J, g = grad_eval()
+            torch.cuda.synchronize()
+            t_grad.append(time.perf_counter() - t0)
+            st = design.sim.stats()
+            fwd_dev.append(st["last_run_ms"] / 1e3)
+            adj_dev.append(st["adjoint_ms"] / 1e3)
         design.forward_only(1 + 9 * torch.sigmoid(theta))
-        torch.cuda.synchronize()
-        t_fwd.append(time.perf_counter() - t0)
-    fwd_dev = design.sim.stats()["last_run_ms"] / 1e3
-    design.close()
+        t_fwd, plain_dev = [], []
+        for _ in range(args.steps):   # the plain forward solve of the same design, for the ratio
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            design.forward_only(1 + 9 * torch.sigmoid(theta))
+            torch.cuda.synchronize()
+            t_fwd.append(time.perf_counter() - t0)
+            plain_dev.append(design.sim.stats()["last_run_ms"] / 1e3)
+        st = design.sim.stats()
+        design.close()
+        tg, tf = statistics.fmean(t_grad), statistics.fmean(t_fwd)
+        dev_grad = statistics.fmean(fwd_dev) + statistics.fmean(adj_dev)
+        dev_plain = statistics.fmean(plain_dev)
+        return {
+            "value": round(world / tg, 4), "ms_per_step": round(tg * 1e3, 1), "J": J,
+            "forward_s": round(tf, 3), "gradient_over_forward": round(tg / tf, 3),
+            "device": {"forward_for_gradient_s": round(statistics.fmean(fwd_dev), 4),
+                       "adjoint_s": round(statistics.fmean(adj_dev), 4), "plain_forward_s": round(dev_plain, 4),
+                       "gradient_over_forward": round(dev_grad / dev_plain, 3),
+                       "adjoint_launches": st["adjoint_launches"]},
+            "gpu_launches": int(st["step_launches"] + st["adjoint_launches"]),
+        }
+
+    ck = measure(FDTDDesign(s, box, [(0, len(pr) - 1, 1.0)], omega, checkpoint_every=64))
+    rec = measure(FDTDDesign(s, box, [(0, len(pr) - 1, 1.0)], omega))
     if rank != 0:
         return None
-    tg, tf = statistics.fmean(t_grad), statistics.fmean(t_fwd)
     return {
-        "metric": "grad evals/s", "value": round(world / tg, 4), "unit": "gradient evaluations/s",
-        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(tg * 1e3, 1),
+        "metric": "grad evals/s", "value": ck["value"], "unit": "gradient evaluations/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ck["ms_per_step"],
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32 fields, f64 accumulators",
         "data": "synthetic: microstrip background, seeded theta",
         "config": {"workload": f"adjoint: 128x128x96, 10-cell PML, {nt} steps, 48x48x4 design, 11 freqs, "
                                "checkpoints every 64", "time_steps": nt, "design_cells": 48 * 48 * 4,
                    "step": "one gradient evaluation (forward with checkpoints + adjoint), wall time"},
-        "forward_s": round(tf, 3), "forward_device_s": round(fwd_dev, 3),
-        "gradient_over_forward": round(tg / tf, 3), "J": J,
+        "forward_s": ck["forward_s"], "gradient_over_forward": ck["gradient_over_forward"], "device": ck["device"],
+        "J": ck["J"], "gpu_launches": ck["gpu_launches"],
+        "recorded_history": {k: rec[k] for k in ("value", "ms_per_step", "forward_s", "gradient_over_forward",
+                                                   "device", "J")},
+    }
+
+
+# ---------------------------------------------------- batched design workload
+
+def run_design(args, rank, world, local_rank):
+    """32 variants of a 96x96x64 microstrip (10-cell PML, 3000 steps), each with its own
+    32x32x4-cell design block above the strip, eps_r = 1 + 9 sigmoid(theta), theta ~ N(0, 1)
+    (seed 5); J_i = sum over 5 frequencies (8-12 GHz) of |DFT of the output Ez probe|^2.
+    One step = one Adam step (lr 0.05) on all 32 designs: a batched forward solve with the
+    box histories recorded, a batched adjoint sweep, the optimizer update."""
+    import torch
+    from rfnetwork_b200 import configs
+    from rfnetwork_b200.adjoint import FDTDDesignBatch
+
+    torch.cuda.set_device(local_rank)
+    nt = args.nt if args.nt != NT else 3000
+    n_var = 32
+    s = configs.microstrip(n=(96, 96, 64), n_pml=10, nt=nt)
+    co, pr, *_ = s.pack_inputs(gpu=True)
+    omega = 2 * np.pi * np.linspace(8e9, 12e9, 5) * float(s.dt)
+    box = (32, 64, 32, 64, 22, 26)
+    designs = FDTDDesignBatch([s] * n_var, box, [(0, len(pr) - 1, 1.0)], omega)
+    gen = torch.Generator().manual_seed(5)
+    theta = torch.randn(n_var, 32, 32, 4, dtype=torch.float64, generator=gen).requires_grad_(True)
+    opt = torch.optim.Adam([theta], lr=0.05)
+    scale = None
+    J_hist = []
+
+    def adam_step():
+        nonlocal scale
+        opt.zero_grad()
+        X = designs(list(1 + 9 * torch.sigmoid(theta)))
+        J = (X.abs() ** 2).sum(dim=(1, 2))          # per variant
+        if scale is None:
+            scale = float(J.detach().mean())
+        (-(J / scale).sum()).backward()               # maximise the output power of every variant
+        opt.step()
+        J_hist.append(J.detach().numpy() / scale)
+
+    for _ in range(max(args.warmup, 1)):
+        adam_step()
+    t = []
+    fwd_ms, adj_ms = [], []
+    for _ in range(args.steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        adam_step()
+        torch.cuda.synchronize()
+        t.append(time.perf_counter() - t0)
+        st = designs.batch.stats()
+        fwd_ms.append(st["last_run_ms"])
+        adj_ms.append(st["adjoint_ms"])
+    st = designs.batch.stats()
+    designs.close()
+    if rank != 0:
+        return None
+    ts = statistics.fmean(t)
+    cells = 96 * 96 * 64
+    return {
+        "metric": "grad evals/s", "value": round(world * n_var / ts, 3), "unit": "gradient evaluations/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ts * 1e3, 1),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32 fields, f64 accumulators",
+        "data": "synthetic: microstrip background, seeded theta per variant",
+        "config": {"workload": f"design: {n_var} variants of 96x96x64, 10-cell PML, {nt} steps, 32x32x4 design "
+                               "each, 5 freqs, Adam lr 0.05", "time_steps": nt, "variants": n_var,
+                   "step": "one Adam step of all variants (batched forward + batched adjoint), wall time"},
+        "device": {"forward_ms": round(statistics.fmean(fwd_ms), 1), "adjoint_ms": round(statistics.fmean(adj_ms), 1),
+                   "forward_mcell_updates_per_s": round(n_var * cells * nt / statistics.fmean(fwd_ms) / 1e3, 1),
+                   "adjoint_mcell_updates_per_s": round(n_var * cells * nt / statistics.fmean(adj_ms) / 1e3, 1)},
+        "objective_mean": [round(float(np.mean(j)), 4) for j in J_hist],
+        "gpu_launches": int(st["step_launches"] + st["adjoint_launches"]),
     }
 
 
@@ -494,6 +608,8 @@ def main():
         out = run_batch(args, rank, world, local_rank)
     elif args.workload == "adjoint":
         out = run_adjoint(args, rank, world, local_rank)
+    elif args.workload == "design":
+        out = run_design(args, rank, world, local_rank)
     else:
         out = run_ours(args, rank, world, local_rank)
         if rank == 0 and world == 1 and not args.no_cpu_baseline:

@@ -62,6 +62,8 @@ typedef struct fdtd_stats {
   int grid;              /* blocks launched per step */
   int64_t h2d_bytes;     /* host-to-device bytes copied for this simulation so far */
   int64_t d2h_bytes;     /* device-to-host bytes read back from it so far */
+  int64_t adjoint_launches; /* reverse-step kernel launches of the last fdtd_adjoint */
+  double adjoint_ms;     /* device time of the last fdtd_adjoint (CUDA events) */
 } fdtd_stats;
 
 /* --------------------------------------------------------------- one grid */
@@ -133,6 +135,11 @@ int fdtd_set_kernel(fdtd_sim* s, int variant, int tile_y, int stages, int zchunk
 /* Launch on a caller stream (cudaStream_t passed as void*); NULL = own stream. */
 int fdtd_set_stream(fdtd_sim* s, void* stream);
 
+/* Whether runs replay the time loop as one captured CUDA graph (enabled = 1,
+ * the default) or issue every launch from the host step by step (0), as the
+ * reference's solver_run_cu does (rfnetwork/core/src/solver.cu:1005-1120). */
+int fdtd_set_graph(fdtd_sim* s, int enabled);
+
 /* Results of the last run. out: n_probes x nt floats, probe-major. */
 int fdtd_get_probe_values(fdtd_sim* s, float* out, int n_probes, int nt);
 /* out: n_series x n_freq x 2 doubles (re, im). */
@@ -148,23 +155,42 @@ void fdtd_destroy(fdtd_sim* s);
 
 /* Like fdtd_run, and keeps a snapshot of the whole field state every `every`
  * steps (ceil(nt/every) snapshots of 6 N floats, plus 12 N when split fields
- * exist) for fdtd_adjoint. The reference has no gradient path; this and
- * fdtd_adjoint have no counterpart there. Any later fdtd_run drops the
- * snapshots. */
+ * exist) for fdtd_adjoint, which then recomputes each segment from its
+ * snapshot. The reference has no gradient path; the functions of this section
+ * have no counterpart there. Any later fdtd_run drops the snapshots. */
 int fdtd_run_checkpointed(fdtd_sim* s, int nt, int every);
 
-/* Gradient of a real objective J of the last checkpointed run's device DFT
- * (fdtd_set_dft) with respect to the E-update coefficients of the cells of a
- * box: box = {x0, x1, y0, y1, z0, z1} in cell indices (the coefficient arrays'
- * indices), cells that are not split (no PML, no source).
+/* Like fdtd_run, and records for fdtd_adjoint the forward history of one
+ * gradient box at every step: E and the six H differences of its cells,
+ * 9 x box cells x nt floats (a 49 x 49 x 5 box over 4000 steps: 1.7 GB). The
+ * adjoint then needs no recomputation. box as for fdtd_adjoint. Any later
+ * fdtd_run drops the history. */
+int fdtd_run_recorded(fdtd_sim* s, int nt, const int* box);
+
+/* Sets the E-update coefficients of the cells of a box: coefs = 3 x 3 x box
+ * cells floats, [ex ey ez][Ca, Cb1, Cb2][x][y][z] (the layout of fdtd_adjoint's
+ * gradient); both Ca arrays of a component (Ca_ex_y and Ca_ex_z, ...) take the
+ * same value, Cb1 / Cb2 are the first / second Cb array of the component in
+ * the coefficient dict's order. The same as fdtd_set_coefficient on those 12
+ * arrays, but once the simulation has been compiled it patches the material
+ * table in place (one row per box cell) instead of compiling the grid again,
+ * so design loops pay no per-iteration compile and keep their captured
+ * graphs. The box cells must not be split (no PML, no source). Not while a
+ * run of this simulation is in flight. No reference counterpart. */
+int fdtd_set_box_coefficients(fdtd_sim* s, const int* box, const float* coefs);
+
+/* Gradient of a real objective J of the last checkpointed or recorded run's
+ * device DFT (fdtd_set_dft) with respect to the E-update coefficients of the
+ * cells of a box: box = {x0, x1, y0, y1, z0, z1} in cell indices (the
+ * coefficient arrays' indices), cells that are not split (no PML, no source);
+ * after fdtd_run_recorded, the recorded box.
  *   dJ_dX  n_series x n_freq x 2 doubles: dJ/dRe X + i dJ/dIm X (the gradient
  *          torch hands a complex output)
  *   grad   3 x 3 x box cells doubles, [component ex ey ez][Ca, Cb1, Cb2][x][y][z]:
  *          dJ/d(Ca_e*), dJ/d(first Cb_e*), dJ/d(second Cb_e*) in the coefficient
  *          dict's order (Ca_ex_y with Ca_ex_z held equal, Cb_ex_y, Cb_ex_z, ...)
- * The discrete adjoint runs backwards through the checkpoints: each segment is
- * recomputed from its snapshot to record the box's forward fields, then
- * reversed with the transposed update in FP32, the products accumulated in
+ * The discrete adjoint runs backwards from the last step, one kernel launch
+ * per step, with the transposed update in FP32 and the products accumulated in
  * FP64. */
 int fdtd_adjoint(fdtd_sim* s, const double* dJ_dX, int n_series, int n_freq, const int* box, double* grad);
 
@@ -181,6 +207,14 @@ int fdtd_batch_run(fdtd_batch* b, int nt);
 int fdtd_batch_set_kernel(fdtd_batch* b, int variant, int tile_y, int stages, int zchunk);
 int fdtd_batch_set_stream(fdtd_batch* b, void* stream);
 int fdtd_batch_get_stats(const fdtd_batch* b, fdtd_stats* out);
+
+/* Gradients of a batch (no reference counterpart): fdtd_batch_run_recorded is
+ * fdtd_run_recorded for every member, boxes = n_sims x 6 ints; then
+ * fdtd_batch_adjoint runs the adjoints of all members together, one launch per
+ * reverse step over all their tiles. dJ_dX[i] and grad[i] are member i's
+ * arrays, sized as for fdtd_adjoint by its own DFT and box. */
+int fdtd_batch_run_recorded(fdtd_batch* b, int nt, const int* boxes);
+int fdtd_batch_adjoint(fdtd_batch* b, const double* const* dJ_dX, double* const* grad);
 const char* fdtd_batch_last_error(const fdtd_batch* b);
 void fdtd_batch_destroy(fdtd_batch* b);
 

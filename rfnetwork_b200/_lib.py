@@ -22,7 +22,8 @@ EXPORTED = (
     "fdtd_get_dft", "fdtd_get_monitor", "fdtd_get_stats", "fdtd_last_error", "fdtd_destroy",
     "fdtd_batch_create", "fdtd_batch_run", "fdtd_batch_set_stream", "fdtd_batch_get_stats",
     "fdtd_batch_last_error", "fdtd_batch_destroy", "fdtd_global_error", "fdtd_step_noalloc",
-    "fdtd_run_checkpointed", "fdtd_adjoint",
+    "fdtd_run_checkpointed", "fdtd_run_recorded", "fdtd_adjoint", "fdtd_batch_run_recorded",
+    "fdtd_batch_adjoint", "fdtd_set_graph", "fdtd_set_box_coefficients",
 )
 
 
@@ -35,6 +36,7 @@ class FdtdStats(ctypes.Structure):
         ("last_run_ms", ctypes.c_double), ("compile_ms", ctypes.c_double),
         ("variant", ctypes.c_int), ("tile_y", ctypes.c_int), ("stages", ctypes.c_int), ("zchunk", ctypes.c_int),
         ("grid", ctypes.c_int), ("h2d_bytes", ctypes.c_int64), ("d2h_bytes", ctypes.c_int64),
+        ("adjoint_launches", ctypes.c_int64), ("adjoint_ms", ctypes.c_double),
     ]
 
     def as_dict(self):
@@ -69,6 +71,8 @@ def load():
         "fdtd_run_async": ([vp, ip], ip),
         "fdtd_synchronize": ([vp], ip),
         "fdtd_set_stream": ([vp, vp], ip),
+        "fdtd_set_graph": ([vp, ip], ip),
+        "fdtd_set_box_coefficients": ([vp, vp, vp], ip),
         "fdtd_get_probe_values": ([vp, vp, ip, ip], ip),
         "fdtd_get_dft": ([vp, vp, ip, ip], ip),
         "fdtd_get_monitor": ([vp, ip, vp, i64], ip),
@@ -83,7 +87,10 @@ def load():
         "fdtd_batch_destroy": ([vp], None),
         "fdtd_global_error": ([], ctypes.c_char_p),
         "fdtd_run_checkpointed": ([vp, ip, ip], ip),
+        "fdtd_run_recorded": ([vp, ip, vp], ip),
         "fdtd_adjoint": ([vp, vp, ip, ip, vp, vp], ip),
+        "fdtd_batch_run_recorded": ([vp, ip, vp], ip),
+        "fdtd_batch_adjoint": ([vp, pp, pp], ip),
     }
     for name, (args, res) in sig.items():
         fn = getattr(lib, name)
@@ -99,6 +106,15 @@ def _ptr(a: np.ndarray):
 
 class FdtdError(RuntimeError):
     pass
+
+
+def _dj_pairs(dJ_dX) -> np.ndarray:
+    """complex [series, freq] -> float64 [series, freq, (re, im)]."""
+    return np.ascontiguousarray(np.stack([np.real(dJ_dX), np.imag(dJ_dX)], axis=-1), dtype=np.float64)
+
+
+def _grad_shape(b) -> tuple:
+    return (3, 3, int(b[1] - b[0]), int(b[3] - b[2]), int(b[5] - b[4]))
 
 
 class Simulation:
@@ -205,6 +221,10 @@ class Simulation:
     def set_stream(self, stream_ptr: int):
         self._check(self.lib.fdtd_set_stream(self.h, ctypes.c_void_p(int(stream_ptr))))
 
+    def set_graph(self, enabled: bool):
+        """Replay the time loop as a CUDA graph (default) or launch every step from the host."""
+        self._check(self.lib.fdtd_set_graph(self.h, int(bool(enabled))))
+
     def run(self, nt: int):
         self._check(self.lib.fdtd_run(self.h, int(nt)))
         self.nt = int(nt)
@@ -214,14 +234,27 @@ class Simulation:
         self._check(self.lib.fdtd_run_checkpointed(self.h, int(nt), int(every)))
         self.nt = int(nt)
 
+    def set_box_coefficients(self, box, coefs: np.ndarray):
+        """E-update coefficients [3 components, (Ca, Cb1, Cb2), *box shape] of the cells of ``box``."""
+        b = np.ascontiguousarray(box, dtype=np.int32)
+        c = np.ascontiguousarray(coefs, dtype=np.float32)
+        if c.shape != _grad_shape(b):
+            raise ValueError(f"coefficients of shape {_grad_shape(b)} expected, got {c.shape}")
+        self._check(self.lib.fdtd_set_box_coefficients(self.h, _ptr(b), _ptr(c)))
+
+    def run_recorded(self, nt: int, box):
+        """Run like ``run`` and record the forward history of ``box`` at every step for ``adjoint``."""
+        b = np.ascontiguousarray(box, dtype=np.int32)
+        self._check(self.lib.fdtd_run_recorded(self.h, int(nt), _ptr(b)))
+        self.nt = int(nt)
+
     def adjoint(self, dJ_dX: np.ndarray, box) -> np.ndarray:
         """Gradient [3 components, (Ca, Cb1, Cb2), *box shape] of J given dJ/dX of the device DFT.
 
         dJ_dX: complex [n_series, n_freq] (dJ/dRe X + i dJ/dIm X); box: (x0, x1, y0, y1, z0, z1)."""
-        g = np.ascontiguousarray(np.stack([np.real(dJ_dX), np.imag(dJ_dX)], axis=-1), dtype=np.float64)
+        g = _dj_pairs(dJ_dX)
         b = np.ascontiguousarray(box, dtype=np.int32)
-        shape = (3, 3, b[1] - b[0], b[3] - b[2], b[5] - b[4])
-        out = np.empty(shape, dtype=np.float64)
+        out = np.empty(_grad_shape(b), dtype=np.float64)
         self._check(self.lib.fdtd_adjoint(self.h, _ptr(g), g.shape[0], g.shape[1], _ptr(b), _ptr(out)))
         return out
 
@@ -287,6 +320,31 @@ class Batch:
             raise FdtdError(f"{FDTD_ERRORS.get(rc, rc)}: {self.lib.fdtd_batch_last_error(self.h).decode()}")
         for s in self.sims:
             s.nt = int(nt)
+
+    def _check(self, rc):
+        if rc:
+            msg = self.lib.fdtd_batch_last_error(self.h).decode()
+            if rc == 1:
+                raise ValueError(msg)
+            raise FdtdError(f"{FDTD_ERRORS.get(rc, rc)}: {msg}")
+
+    def run_recorded(self, nt: int, boxes):
+        """Batched ``Simulation.run_recorded``: boxes[i] is member i's gradient box."""
+        b = np.ascontiguousarray(boxes, dtype=np.int32).reshape(len(self.sims), 6)
+        self._check(self.lib.fdtd_batch_run_recorded(self.h, int(nt), _ptr(b)))
+        self.boxes = b.copy()
+        for s in self.sims:
+            s.nt = int(nt)
+
+    def adjoint(self, dJ_dX) -> list:
+        """Gradients of all members after ``run_recorded``: dJ_dX[i] complex [series, freq] of member i."""
+        gs = [_dj_pairs(d) for d in dJ_dX]
+        outs = [np.empty(_grad_shape(b), dtype=np.float64) for b in self.boxes]
+        n = len(self.sims)
+        din = (ctypes.c_void_p * n)(*[g.ctypes.data for g in gs])
+        dout = (ctypes.c_void_p * n)(*[o.ctypes.data for o in outs])
+        self._check(self.lib.fdtd_batch_adjoint(self.h, din, dout))
+        return outs
 
     def set_kernel(self, variant: int = 1, tile_y: int = 0, stages: int = 4, zchunk: int = 0):
         rc = self.lib.fdtd_batch_set_kernel(self.h, int(variant), int(tile_y), int(stages), int(zchunk))

@@ -16,8 +16,12 @@ the solver does (edge averages weighted by half cell widths, the reference's
 average_cells, rfnetwork/solver.py:892-912), turned into the update
 coefficients Ca = (2 eps - sigma dt) / (2 eps + sigma dt) and
 Cb = 2 dt / (2 eps + sigma dt) (rfnetwork/solver.py:954-961), scaled by the
-packing's inverse cell widths, and the engine runs the time loop keeping a
-field snapshot every ``checkpoint_every`` steps (fdtd_run_checkpointed).
+packing's inverse cell widths, and the engine runs the time loop keeping what
+the adjoint needs: by default the forward history of the gradient box at every
+step (fdtd_run_recorded; 36 bytes per box cell per step), or, when that would
+exceed ``history_budget`` bytes or ``checkpoint_every`` is given, a field
+snapshot every ``checkpoint_every`` (default ~sqrt(nt)) steps
+(fdtd_run_checkpointed), from which the adjoint recomputes each segment.
 Backward: the engine's discrete adjoint (fdtd_adjoint) returns dJ/d(Ca, Cb) of
 the affected E sites; torch chains them to the design tensors.
 """
@@ -28,7 +32,7 @@ import math
 import numpy as np
 import torch
 
-from ._lib import Simulation
+from ._lib import Batch, Simulation
 from .solver_constants import COEFF_NAMES
 from .units import conv
 
@@ -57,17 +61,20 @@ class _Run(torch.autograd.Function):
 class FDTDDesign:
     """A model whose design cells' material enters the time loop differentiably."""
 
-    def __init__(self, solver, design_box, terms, omega, checkpoint_every: int | None = None):
+    def __init__(self, solver, design_box, terms, omega, checkpoint_every: int | None = None,
+                 history_budget: float = 8 * 2**30):
         co, pr, mo, mem, Nx, Ny, Nz, Nt = solver.pack_inputs(gpu=True)
         self.shape = (Nx, Ny, Nz)
         self.nt = Nt
-        self.checkpoint_every = int(checkpoint_every or max(1, round(math.sqrt(Nt))))
         self.base = {k: np.ascontiguousarray(v, dtype=np.float32) for k, v in co.items()}
         x0, x1, y0, y1, z0, z1 = [int(v) for v in design_box]
         self.design_box = (x0, x1, y0, y1, z0, z1)
         # E sites whose average touches a design cell sit at most one cell below it
         self.box = (max(x0 - 1, 0), min(x1, Nx), max(y0 - 1, 0), min(y1, Ny), max(z0 - 1, 0), min(z1, Nz))
         bx0, bx1, by0, by1, bz0, bz1 = self.box
+        history_bytes = 36 * (bx1 - bx0) * (by1 - by0) * (bz1 - bz0) * Nt
+        self.recorded = checkpoint_every is None and history_bytes <= history_budget
+        self.checkpoint_every = None if self.recorded else int(checkpoint_every or max(1, round(math.sqrt(Nt))))
         self.probes = pr  # the probe dicts of the packing (source amplitudes, fields, indices)
         self.sim = Simulation(Nx, Ny, Nz)
         self.sim.set_coefficients(self.base)
@@ -143,21 +150,16 @@ class FDTDDesign:
 
     # -------------------------------------------------------------- running
     def _set(self, coefs: np.ndarray):
-        bx0, bx1, by0, by1, bz0, bz1 = self.box
-        box_sl = (slice(bx0, bx1), slice(by0, by1), slice(bz0, bz1))
-        for c in range(3):
-            for name in _CA[c]:  # both twins take the same value on the box: its sites stay unsplit
-                ca = self.base[name].copy()
-                ca[box_sl] = coefs[c, 0].astype(np.float32)
-                self.sim.set_coefficient(name, ca)
-            for k in range(2):
-                cb = self.base[_CB[c][k]].copy()
-                cb[box_sl] = coefs[c, 1 + k].astype(np.float32)
-                self.sim.set_coefficient(_CB[c][k], cb)
+        # both Ca twins take the same value on the box, so its sites stay unsplit;
+        # once compiled, the engine patches its material table in place
+        self.sim.set_box_coefficients(self.box, coefs)
 
     def _run(self, coefs: np.ndarray) -> np.ndarray:
         self._set(coefs)
-        self.sim.run_checkpointed(self.nt, self.checkpoint_every)
+        if self.recorded:
+            self.sim.run_recorded(self.nt, self.box)
+        else:
+            self.sim.run_checkpointed(self.nt, self.checkpoint_every)
         return self.sim.dft()
 
     def forward_only(self, eps_r, sigma=None) -> np.ndarray:
@@ -174,4 +176,52 @@ class FDTDDesign:
         self.sim.close()
 
 
-__all__ = ["FDTDDesign", "COEFF_NAMES"]
+class _RunBatch(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, coefs, design):
+        ctx.design = design
+        return torch.from_numpy(design._run(coefs.detach().cpu().numpy()))
+
+    @staticmethod
+    def backward(ctx, gX):
+        g = ctx.design.batch.adjoint(list(gX.detach().cpu().numpy()))
+        return torch.from_numpy(np.stack(g)), None
+
+
+class FDTDDesignBatch:
+    """Several designs (variants of models, one design box each) whose forward
+    solves run as one batch and whose adjoints run as one batched sweep.
+
+        designs = FDTDDesignBatch([solver] * 32, box, terms, omega)
+        X = designs([1 + 9 * torch.sigmoid(t) for t in thetas])   # complex [member, series, freq]
+
+    Every member keeps the box history of its forward run (fdtd_batch_run_recorded);
+    the gradient boxes must have one shape so the coefficients stack."""
+
+    def __init__(self, solvers, design_box, terms, omega):
+        self.members = [FDTDDesign(s, design_box, terms, omega, checkpoint_every=None, history_budget=float("inf"))
+                        for s in solvers]
+        shapes = {tuple(b - a for a, b in zip(m.box[0::2], m.box[1::2])) for m in self.members}
+        if len(shapes) != 1 or len({m.nt for m in self.members}) != 1:
+            raise ValueError("batch members need one gradient-box shape and one number of time steps")
+        self.nt = self.members[0].nt
+        self.batch = Batch([m.sim for m in self.members])
+
+    def _run(self, coefs: np.ndarray) -> np.ndarray:
+        for m, c in zip(self.members, coefs):
+            m._set(c)
+        self.batch.run_recorded(self.nt, [m.box for m in self.members])
+        return np.stack([m.sim.dft() for m in self.members])
+
+    def __call__(self, eps_r, sigma=None):
+        sig = sigma if sigma is not None else [None] * len(self.members)
+        coefs = torch.stack([m.coefficients(e, g) for m, e, g in zip(self.members, eps_r, sig)])
+        return _RunBatch.apply(coefs, self)
+
+    def close(self):
+        self.batch.close()
+        for m in self.members:
+            m.close()
+
+
+__all__ = ["FDTDDesign", "FDTDDesignBatch", "COEFF_NAMES"]

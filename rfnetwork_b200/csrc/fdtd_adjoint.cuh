@@ -2,26 +2,33 @@
 // probe series with respect to the E-update coefficients of a box of cells.
 //
 // The forward step n (fdtd_step_kernel / fdtd_step_stream_kernel) is linear
-// in the state (E, H and the split fields):
-//   E split pair  s_{2c}' = C[4c] s_{2c} + C[4c+1] dA_c(H),
-//                 s_{2c+1}' = C[4c+2] s_{2c+1} + C[4c+3] dB_c(H)   (+ sources)
-//   H split pair  h_s' = Da_s h_s + g_s(E')                        (+ sources)
-// with an unsplit cell the special case of equal decays (both halves of the
-// pair share Ca / Da and the total is what is stored). The adjoint keeps one
-// value per half of every pair for every cell -- for an unsplit cell the two
-// halves stay equal, so one formula serves all cells -- and runs the
-// transposed recursion backwards in time, one reverse step as three launches:
-//   adj_probe_kernel  dJ/d(recorded value) into the pair halves of the probed
-//                     component (the records read E^{n+1} and H^{n+1})
-//   adj_e_kernel      lamE: add the transposed g terms (own Db2 lamH, the
-//                     neighbours' Q), decay by Ca, emit dA / dB adjoints, and
-//                     accumulate the gradient of the box cells in FP64
-//   adj_h_kernel      lamH: decay by Da and add the transposed differences of
-//                     the neighbouring dA / dB adjoints; and Q_s = Db1_s lamH_s,
-//                     the part of the next reverse step's H-update transpose
-//                     that lands on the neighbouring E cell (the probe kernel
-//                     keeps Q in step with what it adds to lamH)
-// Index conventions follow the forward kernels: arrays [z][y][pitch].
+// in the state. Writing every E and H component as a pair of split halves,
+//   E  s_{2c}' = Ca_{2c} s_{2c} + Cb_{2c} dA_c(H),
+//      s_{2c+1}' = Ca_{2c+1} s_{2c+1} + Cb_{2c+1} dB_c(H),    E_c' = s_{2c}' + s_{2c+1}'
+//   H  h_s' = Da_s h_s + Db2_s e(own) - Db1_s e(-1 neighbour),  H_c' = h_{2c}' + h_{2c+1}'
+// (sources add constants; probes record the totals after the step). An
+// unsplit cell is the case of equal decays, whose stored total is the sum.
+//
+// The adjoint state mirrors the forward storage: for an unsplit cell both
+// halves of a pair carry the same adjoint (d/ds_k of E = s_0 + s_1 is the
+// same for both halves, and equal decays keep them equal), so one total per
+// component is kept, in a [2 buffers][3] array like the fields; split cells
+// (PML slabs, source cells) keep both halves in [2][6] arrays like the split
+// fields. One reverse step is one launch, adj_step_kernel, which walks z
+// upwards through a 30 x TY tile much as the forward kernel does:
+//   E part   mu = lamE + (own Db2 lamH) - (Db1 lamH of the +1 neighbours),
+//            lamE' = Ca mu, and the adjoints of the H differences ad = Cb mu,
+//            computed on the tile and its -1 halo row / column;
+//   H part   lamH' = Da lamH + (ad of the -1 neighbours - own ad), the
+//            transposed differences, with the -1 neighbours' ad taken by warp
+//            shuffle (x), shared memory (y) and registers (z);
+//   records  the adjoints dJ/d(record of step n-1) of this cell's probes are
+//            added to lamE' / lamH' as they are stored;
+//   gradient mu times the forward history of the box cells, accumulated in
+//            FP64: dJ/dCa = sum mu E^n, dJ/dCb1 = sum mu dA(H^n), dJ/dCb2 =
+//            sum mu dB(H^n).
+// Reverse step n reads buffer n & 1 and writes the other; the history of step
+// n sits at slot n - hist_n0 of each simulation's hist.
 #pragma once
 
 #include <cstdint>
@@ -30,131 +37,311 @@
 
 namespace rfn {
 
-struct AdjDev {
-  SimDev s;             // geometry, material table, probe list
-  float* lamE;          // [6][N] E pair halves (ex_y ex_z ey_z ey_x ez_x ez_y)
-  float* lamH;          // [6][N] H pair halves (hx_y hx_z hy_z hy_x hz_x hz_y)
-  float* q;             // [6][N] Db1_s lamH_s
-  float* ad;            // [6][N] adjoints of dA_x dB_x dA_y dB_y dA_z dB_z
-  int64_t N;            // floats per component array
+struct AdjSim {
+  int nx, ny, nz, pitch, plane, nt;
+  const uint16_t* mat;       // material index [z][y][pitch]
+  const float4* rows;        // 8 float4 per table row
+  const int2* cell_probes;   // (probe, field) grouped per probe cell
+  int64_t N;                 // floats per component array
+  // adjoint state, [2 buffers][6][N]: E totals ex ey ez, then H totals hx hy hz
+  // (unsplit cells); halves [2][12][N]: ex_y ex_z ey_z ey_x ez_x ez_y, then
+  // hx_y hx_z hy_z hy_x hz_x hz_y (split cells; null without split cells)
+  float* lam;
+  float* lams;
+  const float* radj;         // [P][nt] dJ/d(record of probe p at step n)
+  const int* probe_idx;      // [P] cell offset of each probe
+  const int* probe_field;    // [P] 0..5 = ex ey ez hx hy hz
+  int n_probes;
   int bx0, bx1, by0, by1, bz0, bz1;  // gradient box (cells)
-  double* grad;         // [3 components][Ca, Cb1, Cb2][box cells]
-  const float* hist;    // forward history of this step: [9][box cells] = E_x E_y E_z, dA_x dB_x .. dB_z
+  int64_t nb;                // cells in the box
+  double* grad;              // [3 components][Ca, Cb1, Cb2][box cells]
+  const float* hist;         // forward history: [9][nb] per step = E_x E_y E_z, dA_x dB_x .. dB_z
 };
 
-__device__ __forceinline__ const float4* adj_row(const SimDev& s, int idx) { return s.rows + 8 * s.mat[idx]; }
+// Box history of one simulation at one step: E^n and the six H differences
+// the E update of step n uses.
+struct CapSim {
+  SimDev s;
+  int bx0, bx1, by0, by1, bz0, bz1;
+  int64_t nb;
+  float* hist;               // [steps][9][nb]
+};
 
-// The Db1 coefficient of each H split s (slots 13, 16, 19, 22, 25, 28).
-__device__ __forceinline__ void adj_db1(const float4* row, float (&b1)[6]) {
-  const float4 p = __ldg(row + 3), q = __ldg(row + 4), u = __ldg(row + 5), v = __ldg(row + 6), r7 = __ldg(row + 7);
-  b1[0] = p.y; b1[1] = q.x; b1[2] = q.w; b1[3] = u.z; b1[4] = v.y; b1[5] = r7.x;
-}
+__device__ __forceinline__ float adj_ld(const float* p, int i) { return __ldg(p + i); }
 
-// Field values recorded by probes at step n are E^{n+1} / H^{n+1}: their
-// adjoints enter both halves of the probed component's pair.
-__global__ void adj_probe_kernel(AdjDev a, const int* __restrict__ probe_idx, const int* __restrict__ probe_field,
-                                 const float* __restrict__ radj, int n_probes, int nt, int n) {
-  const int p = blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= n_probes) return;
-  const float r = radj[size_t(p) * nt + n];
-  if (r == 0.f) return;
-  const int f = probe_field[p];
-  const int64_t idx = probe_idx[p];
-  float* base = f < 3 ? a.lamE : a.lamH;
-  const int c = f < 3 ? f : f - 3;
-  atomicAdd(base + (2 * c) * a.N + idx, r);
-  atomicAdd(base + (2 * c + 1) * a.N + idx, r);
-  if (f >= 3) {
-    float b1[6];
-    adj_db1(adj_row(a.s, int(idx)), b1);
-    atomicAdd(a.q + (2 * c) * a.N + idx, b1[2 * c] * r);
-    atomicAdd(a.q + (2 * c + 1) * a.N + idx, b1[2 * c + 1] * r);
+// The adjoint halves of the H pairs of one cell (totals duplicated for an
+// unsplit cell); tot / half point at component 0 of the H totals / halves.
+__device__ __forceinline__ void adj_load_h(const float* tot, const float* half, int64_t N, int idx, uint32_t fl,
+                                           float (&h)[6]) {
+  if (fl & kHSplit) {
+#pragma unroll
+    for (int k = 0; k < 6; ++k) h[k] = adj_ld(half + k * N, idx);
+  } else {
+    const float hx = adj_ld(tot, idx), hy = adj_ld(tot + N, idx), hz = adj_ld(tot + 2 * N, idx);
+    h[0] = hx; h[1] = hx; h[2] = hy; h[3] = hy; h[4] = hz; h[5] = hz;
   }
 }
 
-__global__ void adj_e_kernel(AdjDev a) {
-  const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y, z = blockIdx.z;
-  const SimDev& s = a.s;
-  if (x >= s.nx || y >= s.ny) return;
-  const int idx = z * s.plane + y * s.pitch + x;
-  const int64_t N = a.N;
-  const float4* row = adj_row(s, idx);
-  const float4 ra = __ldg(row), rb = __ldg(row + 1), rd = __ldg(row + 2);
-  const float4 p = __ldg(row + 3), q = __ldg(row + 4), u = __ldg(row + 5), v = __ldg(row + 6), r7 = __ldg(row + 7);
-  // Db2 of the six H splits at this cell (slots 14, 17, 20, 23, 26, 29)
-  const float b2[6] = {p.z, q.y, u.x, u.w, v.z, r7.y};
-  float ag[6];
+__device__ __forceinline__ uint32_t adj_flags(const float4* row) { return __float_as_uint(__ldg(row + 7).z); }
+
+// Tile of the adjoint step kernel: lane 0 is the -1 halo column, lanes 1..30
+// the owned columns and lane 31 only provides Db1 lamH of the column above
+// the tile (x0 + 30) to lane 30; warp 0 is the -1 halo row, warps 1..TY the
+// owned rows and warp TY+1 only provides Db1 lamH of the row above the tile.
+constexpr int kAdjTileX = 30;
+constexpr int kAdjTileY = 7;
+
+template <int TY, int MINB>
+__global__ void __launch_bounds__(32 * (TY + 2), MINB)
+adj_step_kernel(const AdjSim* __restrict__ sims, const int4* __restrict__ tiles, int n, int hist_n0) {
+  const int4 t = tiles[blockIdx.x];
+  const AdjSim& A = sims[t.x];
+  const int x0 = t.y & 0xffff, y0 = int(unsigned(t.y) >> 16), z0 = t.z & 0xffff, z1 = int(unsigned(t.z) >> 16);
+  const int lane = threadIdx.x, w = threadIdx.y;
+  const int c = x0 - 1 + lane;  // this lane's column
+  const int r = y0 - 1 + w;     // this warp's row
+  const int nx = A.nx, ny = A.ny, nz = A.nz, pitch = A.pitch, plane = A.plane;
+  const bool in_xy = c >= 0 && c < nx && r >= 0 && r < ny;
+  const bool worker = lane < 31 && w <= TY;  // computes E (tile and -1 halo)
+  const bool own = in_xy && lane >= 1 && lane <= 30 && w >= 1 && w <= TY;
+  const int cur = n & 1, nxt = cur ^ 1;
+  const int col = r * pitch + c;
+  const int64_t N = A.N;
+  const float* __restrict__ rE = A.lam + cur * 6 * N;    // read: E totals, then H totals
+  const float* __restrict__ rH = rE + 3 * N;
+  float* __restrict__ wE = A.lam + nxt * 6 * N;          // write
+  float* __restrict__ wH = wE + 3 * N;
+  const float* __restrict__ rEs = A.lams + cur * 12 * N;  // halves (split cells only)
+  const float* __restrict__ rHs = rEs + 6 * N;
+  float* __restrict__ wEs = A.lams + nxt * 12 * N;
+  float* __restrict__ wHs = wEs + 6 * N;
+  const uint16_t* __restrict__ mat = A.mat;
+  const float4* __restrict__ rows = A.rows;
+
+  __shared__ float s_qhx[2][TY + 2][32];  // Db1 lamH of hx_y, read by the row below
+  __shared__ float s_qhz[2][TY + 2][32];  // Db1 lamH of hz_y
+  __shared__ float s_a0[2][TY + 2][32];   // ad of dA_x (= dhz_y), read by the row above
+  __shared__ float s_a5[2][TY + 2][32];   // ad of dB_z (= dhx_y)
+
+  auto mat_at = [&](int z) -> int { return (in_xy && z >= 0 && z < nz) ? int(__ldg(mat + z * plane + col)) : 0; };
+  auto flags_of = [&](int id) -> uint32_t { return adj_flags(rows + 8 * id); };
+
+  // register pipeline along z: material ids four planes ahead, flags three,
+  // H adjoints two and E adjoints one, so every load of a plane depends on
+  // registers only and is consumed one plane after it was issued
+  auto load_e = [&](int z, uint32_t fl, float (&e)[6]) {
+    if (!(worker && in_xy && z >= 0 && z < nz)) return;
+    const int i = z * plane + col;
+    if (fl & kESplit) {
 #pragma unroll
-  for (int k = 0; k < 6; ++k) ag[k] = a.lamH[k * N + idx];
-  const bool xn = x + 1 < s.nx, yn = y + 1 < s.ny, zn = z + 1 < s.nz;
-  auto qn = [&](int k, bool ok, int off) { return ok ? a.q[k * N + idx + off] : 0.f; };
-  // transposed g terms: own Db2 lamH, minus the neighbour's Db1 lamH
-  const float aEx = (b2[2] * ag[2] - qn(2, zn, s.plane)) + (b2[5] * ag[5] - qn(5, yn, s.pitch));
-  const float aEy = (b2[1] * ag[1] - qn(1, zn, s.plane)) + (b2[4] * ag[4] - qn(4, xn, 1));
-  const float aEz = (b2[0] * ag[0] - qn(0, yn, s.pitch)) + (b2[3] * ag[3] - qn(3, xn, 1));
-  const float aET[3] = {aEx, aEy, aEz};
-  const float ca[6] = {ra.x, ra.z, rb.x, rb.z, rd.x, rd.z};  // decay of each E split
-  const float cb[6] = {ra.y, ra.w, rb.y, rb.w, rd.y, rd.w};  // difference coefficient of each E split
-  float mu[6];
-#pragma unroll
-  for (int k = 0; k < 6; ++k) {
-    mu[k] = a.lamE[k * N + idx] + aET[k / 2];
-    a.lamE[k * N + idx] = ca[k] * mu[k];
-    a.ad[k * N + idx] = cb[k] * mu[k];
+      for (int k = 0; k < 6; ++k) e[k] = adj_ld(rEs + k * N, i);
+    } else {
+      e[0] = adj_ld(rE, i); e[1] = adj_ld(rE + N, i); e[2] = adj_ld(rE + 2 * N, i);
+    }
+  };
+  auto load_h = [&](int z, uint32_t fl, float (&h)[6]) {
+    if (in_xy && z >= 0 && z < nz) adj_load_h(rH, rHs, N, z * plane + col, fl, h);
+  };
+  int id_c = mat_at(z0 - 1);
+  int id_n1 = mat_at(z0);
+  int id_n2 = mat_at(z0 + 1);
+  int id_n3 = mat_at(z0 + 2);
+  uint32_t fl_c = flags_of(id_c);
+  uint32_t fl_n1 = flags_of(id_n1);
+  uint32_t fl_n2 = flags_of(id_n2);
+  float h_c[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f}, h_n[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+  float e_c[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+  load_h(z0 - 1, fl_c, h_c);
+  load_h(z0, fl_n1, h_n);
+  load_e(z0 - 1, fl_c, e_c);
+  {
+    const float4* rc = rows + 8 * id_c;
+    s_qhx[(z0 - 1) & 1][w][lane] = __ldg(rc + 3).y * h_c[0];
+    s_qhz[(z0 - 1) & 1][w][lane] = __ldg(rc + 7).x * h_c[5];
   }
-  if (x >= a.bx0 && x < a.bx1 && y >= a.by0 && y < a.by1 && z >= a.bz0 && z < a.bz1) {
-    const int bnx = a.bx1 - a.bx0, bny = a.by1 - a.by0, bnz = a.bz1 - a.bz0;
-    const int64_t nb = int64_t(bnx) * bny * bnz;
-    const int64_t bi = (int64_t(x - a.bx0) * bny + (y - a.by0)) * bnz + (z - a.bz0);
+  float a1_p = 0.f, a2_p = 0.f;
+  __syncthreads();
+
+  for (int z = z0 - 1; z < z1; ++z) {
+    const bool zin = z >= 0 && z < nz;
+    const bool live = in_xy && zin;
+    const int idx = z * plane + col;
+    const int buf = z & 1;
+
+    // ---- loads for the planes ahead (addresses from registers only)
+    const int id_n4 = mat_at(z + 4);
+    const uint32_t fl_n3 = flags_of(id_n3);
+    float h_n2[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f}, e_n[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    load_h(z + 2, fl_n2, h_n2);
+    load_e(z + 1, fl_n1, e_n);
+    // ---- table rows of this plane and of the look-ahead
+    const float4* rn = rows + 8 * id_n1;
+    const float4 p_n = __ldg(rn + 3), q_n = __ldg(rn + 4), r7_n = __ldg(rn + 7);
+    const float4* row = rows + 8 * id_c;
+    const float4 ra = __ldg(row + 0), rb = __ldg(row + 1), rd = __ldg(row + 2);
+    const float4 p = __ldg(row + 3), q = __ldg(row + 4), u = __ldg(row + 5), v = __ldg(row + 6), r7 = __ldg(row + 7);
+    float lE[6];
 #pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      // unsplit design cells: both halves of the pair hold the same adjoint
-      const double m = double(mu[2 * c]);
-      a.grad[(3 * c + 0) * nb + bi] += m * double(a.hist[c * nb + bi]);
-      a.grad[(3 * c + 1) * nb + bi] += m * double(a.hist[(3 + 2 * c) * nb + bi]);
-      a.grad[(3 * c + 2) * nb + bi] += double(mu[2 * c + 1]) * double(a.hist[(4 + 2 * c) * nb + bi]);
+    for (int k = 0; k < 6; ++k) lE[k] = e_c[k];
+
+    // ---- Db1 lamH of the +1 neighbours: z+1 from the look-ahead, x+1 from
+    // the lane on the right, y+1 from the row above (written last plane)
+    const float qz_hx = q_n.x * h_n[1], qz_hy = q_n.w * h_n[2];
+    const float qx_hy = __shfl_down_sync(0xffffffffu, u.z * h_c[3], 1);
+    const float qx_hz = __shfl_down_sync(0xffffffffu, v.y * h_c[4], 1);
+    const float qy_hx = s_qhx[buf][w + (w <= TY ? 1 : 0)][lane];
+    const float qy_hz = s_qhz[buf][w + (w <= TY ? 1 : 0)][lane];
+    // and this column's own values at z+1 for the row below, next plane
+    s_qhx[buf ^ 1][w][lane] = p_n.y * h_n[0];
+    s_qhz[buf ^ 1][w][lane] = r7_n.x * h_n[5];
+
+    // ---- E part: mu, lamE', ad
+    float mu[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f}, ad[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    if (live && worker) {
+      // Db2 slots: hx_y p.z, hx_z q.y, hy_z u.x, hy_x u.w, hz_x v.z, hz_y r7.y
+      const float aEx = (u.x * h_c[2] - qz_hy) + (r7.y * h_c[5] - qy_hz);
+      const float aEy = (q.y * h_c[1] - qz_hx) + (v.z * h_c[4] - qx_hz);
+      const float aEz = (p.z * h_c[0] - qy_hx) + (u.w * h_c[3] - qx_hy);
+      if (!(fl_c & kESplit)) {
+        const float mx = lE[0] + aEx, my = lE[1] + aEy, mz = lE[2] + aEz;
+        mu[0] = mx; mu[1] = mx; mu[2] = my; mu[3] = my; mu[4] = mz; mu[5] = mz;
+        lE[0] = ra.x * mx; lE[1] = rb.x * my; lE[2] = rd.x * mz;
+      } else {
+        const float aE[3] = {aEx, aEy, aEz};
+        const float ca[6] = {ra.x, ra.z, rb.x, rb.z, rd.x, rd.z};
+#pragma unroll
+        for (int k = 0; k < 6; ++k) {
+          mu[k] = lE[k] + aE[k / 2];
+          lE[k] = ca[k] * mu[k];
+        }
+      }
+      const float cb[6] = {ra.y, ra.w, rb.y, rb.w, rd.y, rd.w};
+#pragma unroll
+      for (int k = 0; k < 6; ++k) ad[k] = cb[k] * mu[k];
+    }
+
+    // ---- -1 neighbours' ad
+    s_a0[buf][w][lane] = ad[0];
+    s_a5[buf][w][lane] = ad[5];
+    const float a3_m = __shfl_up_sync(0xffffffffu, ad[3], 1);
+    const float a4_m = __shfl_up_sync(0xffffffffu, ad[4], 1);
+    __syncthreads();
+
+    if (own && z >= z0 && zin) {
+      const float a0_m = s_a0[buf][w - 1][lane];
+      const float a5_m = s_a5[buf][w - 1][lane];
+      const float aH[3] = {(a2_p - ad[2]) + (a5_m - ad[5]), (a1_p - ad[1]) + (a4_m - ad[4]),
+                           (a0_m - ad[0]) + (a3_m - ad[3])};
+      float lh[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+      if (!(fl_c & kHSplit)) {
+        lh[0] = p.x * h_c[0] + aH[0];
+        lh[1] = q.z * h_c[2] + aH[1];
+        lh[2] = v.x * h_c[4] + aH[2];
+      } else {
+        const float da[6] = {p.x, p.w, q.z, u.y, v.x, v.w};
+#pragma unroll
+        for (int k = 0; k < 6; ++k) lh[k] = da[k] * h_c[k] + aH[k / 2];
+      }
+      // adjoints of this cell's records of step n-1 (E^n, H^n)
+      const int np = int(fl_c >> 16);
+      if (np && n >= 1) {
+        const int first = __float_as_int(r7.w);
+        for (int e = 0; e < np; ++e) {
+          const int2 pe = __ldg(A.cell_probes + first + e);
+          const float rv = __ldg(A.radj + size_t(pe.x) * A.nt + (n - 1));
+          // both halves of a split pair, or the total (slots 0..2) of an unsplit cell
+          const bool is_e = pe.y < 3;
+          const int cc = is_e ? pe.y : pe.y - 3;
+          const bool sp = (fl_c & (is_e ? kESplit : kHSplit)) != 0;
+#pragma unroll
+          for (int k = 0; k < 6; ++k)
+            if (sp ? (k / 2 == cc) : (k == cc)) {
+              if (is_e) lE[k] += rv;
+              else lh[k] += rv;
+            }
+        }
+      }
+      if (fl_c & kESplit) {
+#pragma unroll
+        for (int k = 0; k < 6; ++k) wEs[k * N + idx] = lE[k];
+      } else {
+        wE[idx] = lE[0]; wE[N + idx] = lE[1]; wE[2 * N + idx] = lE[2];
+      }
+      if (fl_c & kHSplit) {
+#pragma unroll
+        for (int k = 0; k < 6; ++k) wHs[k * N + idx] = lh[k];
+      } else {
+        wH[idx] = lh[0]; wH[N + idx] = lh[1]; wH[2 * N + idx] = lh[2];
+      }
+      if (A.hist && c >= A.bx0 && c < A.bx1 && r >= A.by0 && r < A.by1 && z >= A.bz0 && z < A.bz1) {
+        const int bny = A.by1 - A.by0, bnz = A.bz1 - A.bz0;
+        const int64_t nb = A.nb;
+        const int64_t bi = (int64_t(c - A.bx0) * bny + (r - A.by0)) * bnz + (z - A.bz0);
+        const float* hs = A.hist + int64_t(n - hist_n0) * 9 * nb;
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+          A.grad[(3 * k + 0) * nb + bi] += double(mu[2 * k]) * double(__ldg(hs + k * nb + bi));
+          A.grad[(3 * k + 1) * nb + bi] += double(mu[2 * k]) * double(__ldg(hs + (3 + 2 * k) * nb + bi));
+          A.grad[(3 * k + 2) * nb + bi] += double(mu[2 * k + 1]) * double(__ldg(hs + (4 + 2 * k) * nb + bi));
+        }
+      }
+    }
+    a1_p = ad[1];
+    a2_p = ad[2];
+    id_c = id_n1;
+    fl_c = fl_n1;
+    id_n1 = id_n2;
+    fl_n1 = fl_n2;
+    id_n2 = id_n3;
+    fl_n2 = fl_n3;
+    id_n3 = id_n4;
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+      h_c[k] = h_n[k];
+      h_n[k] = h_n2[k];
+      e_c[k] = e_n[k];
     }
   }
 }
 
-__global__ void adj_h_kernel(AdjDev a) {
-  const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y, z = blockIdx.z;
-  const SimDev& s = a.s;
-  if (x >= s.nx || y >= s.ny) return;
-  const int idx = z * s.plane + y * s.pitch + x;
-  const int64_t N = a.N;
-  auto ad = [&](int k) { return a.ad[k * N + idx]; };
-  auto adm = [&](int k, bool ok, int off) { return ok ? a.ad[k * N + idx - off] : 0.f; };
-  const bool xm = x > 0, ym = y > 0, zm = z > 0;
-  // transposed differences (dA_x = dhz_y, dB_x = dhy_z, dA_y = dhx_z, dB_y = dhz_x, dA_z = dhy_x, dB_z = dhx_y)
-  const float aHx = (adm(2, zm, s.plane) - ad(2)) + (adm(5, ym, s.pitch) - ad(5));
-  const float aHy = (adm(1, zm, s.plane) - ad(1)) + (adm(4, xm, 1) - ad(4));
-  const float aHz = (adm(0, ym, s.pitch) - ad(0)) + (adm(3, xm, 1) - ad(3));
-  const float aH[3] = {aHx, aHy, aHz};
-  const float4* row = adj_row(s, idx);
-  const float4 p = __ldg(row + 3), q = __ldg(row + 4), u = __ldg(row + 5), v = __ldg(row + 6), r7 = __ldg(row + 7);
-  const float da[6] = {p.x, p.w, q.z, u.y, v.x, v.w};
-  const float b1[6] = {p.y, q.x, q.w, u.z, v.y, r7.x};
-#pragma unroll
-  for (int k = 0; k < 6; ++k) {
-    const float l = da[k] * a.lamH[k * N + idx] + aH[k / 2];
-    a.lamH[k * N + idx] = l;
-    a.q[k * N + idx] = b1[k] * l;
+// Adjoints of the records of step `step` into buffer `buf` (the start of the
+// reverse sweep; later steps add theirs inside adj_step_kernel). One block
+// row per simulation.
+__global__ void adj_inject_kernel(const AdjSim* __restrict__ sims, int step, int buf) {
+  const AdjSim& A = sims[blockIdx.y];
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= A.n_probes) return;
+  const float rv = A.radj[size_t(p) * A.nt + step];
+  if (rv == 0.f) return;
+  const int idx = A.probe_idx[p], f = A.probe_field[p];
+  const uint32_t fl = adj_flags(A.rows + 8 * A.mat[idx]);
+  const int64_t N = A.N;
+  // field f: total f of [E totals, H totals], or halves 2f, 2f+1 of the 12 halves
+  if (fl & (f < 3 ? kESplit : kHSplit)) {
+    float* h = A.lams + buf * 12 * N;
+    atomicAdd(h + (2 * f) * N + idx, rv);
+    atomicAdd(h + (2 * f + 1) * N + idx, rv);
+  } else {
+    atomicAdd(A.lam + (buf * 6 + f) * N + idx, rv);
   }
 }
 
-// Forward history of the box at the start of step n: E^n and the H
-// differences the E update of step n uses.
-__global__ void adj_capture_kernel(AdjDev a, int buf, float* __restrict__ hist) {
-  const int bnx = a.bx1 - a.bx0, bny = a.by1 - a.by0, bnz = a.bz1 - a.bz0;
-  const int64_t nb = int64_t(bnx) * bny * bnz;
-  const SimDev& s = a.s;
+// Forward history of the boxes at the start of step n (fields of buffer
+// n & 1), written at step slot n - n0. One block row per simulation.
+__global__ void adj_capture_kernel(const CapSim* __restrict__ caps, int n, int n0) {
+  const CapSim& C = caps[blockIdx.y];
+  const SimDev& s = C.s;
+  const int bnx = C.bx1 - C.bx0, bny = C.by1 - C.by0, bnz = C.bz1 - C.bz0;
+  (void)bnx;
+  const int64_t nb = C.nb;
+  float* hist = C.hist + int64_t(n - n0) * 9 * nb;
+  const int b = n & 1;
+  const float* const* E = s.E[b];
+  const float* const* H = s.H[b];
   for (int64_t bi = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; bi < nb; bi += int64_t(gridDim.x) * blockDim.x) {
     const int zz = int(bi % bnz), yy = int((bi / bnz) % bny), xx = int(bi / (int64_t(bnz) * bny));
-    const int x = a.bx0 + xx, y = a.by0 + yy, z = a.bz0 + zz;
+    const int x = C.bx0 + xx, y = C.by0 + yy, z = C.bz0 + zz;
     const int idx = z * s.plane + y * s.pitch + x;
-    const float* const* E = s.E[buf];
-    const float* const* H = s.H[buf];
     auto h = [&](int c, bool ok, int off) { return ok ? H[c][idx + off] : 0.f; };
     const bool xn = x + 1 < s.nx, yn = y + 1 < s.ny, zn = z + 1 < s.nz;
     const float hx = H[0][idx], hy = H[1][idx], hz = H[2][idx];

@@ -160,13 +160,53 @@ struct fdtd_sim {
   std::string err;
   fdtd_stats stats{};
   int64_t h2d_bytes = 0, d2h_bytes = 0;  // bytes copied over PCIe/C2C by this simulation
-  // state snapshots of the last checkpointed run (fdtd_run_checkpointed), one
-  // per segment of ckpt_every steps: the 6 field arrays of the time buffer
-  // the segment starts from, then (when allocated) its 12 split arrays
+  // What the last run kept for a gradient (fdtd_adjoint): adj_mode 1 = state
+  // snapshots (fdtd_run_checkpointed), one per segment of ckpt_every steps:
+  // the 6 field arrays of the time buffer the segment starts from, then (when
+  // allocated) its 12 split arrays; adj_mode 2 = the forward history of the
+  // gradient box at every step (fdtd_run_recorded), [nt][9][box cells].
+  int adj_mode = 0;
   int ckpt_every = 0;
   int ckpt_nt = -1;
   DevBuf<float> ckpt;
+  int adj_box[6] = {0, 0, 0, 0, 0, 0};
+  DevBuf<float> hist;
+  bool adj_in_batch = false;  // the recorded run was a batch run
+  bool use_graph = true;      // fdtd_set_graph
+  // table rows given to the cells of one box by fdtd_set_box_coefficients
+  // (one per cell, after the compiled rows)
+  int base_rows = 0;
+  int box_rows_from = -1;
+  int box_rows_box[6] = {0, 0, 0, 0, 0, 0};
+  int generation = 0;  // bumped whenever device buffers are reallocated
 };
+
+int64_t box_cells(const int* b) { return int64_t(b[1] - b[0]) * (b[3] - b[2]) * (b[5] - b[4]); }
+
+// dJ/d(record of probe p at step n), [P][nt], from dJ/dX of the device DFT
+// (X_sf = sum over the series' terms (p, w) of w sum_n rec_p[n] e^{-i w_f n};
+// with the gradient convention G = dJ/dRe X + i dJ/dIm X this is
+// sum over the terms (series, p, w) of w sum_f (Re G_sf cos(w_f n) - Im G_sf sin(w_f n))).
+std::vector<float> record_adjoints(const fdtd_sim* s, const double* dJdX, int nt) {
+  const int P = int(s->probes.size());
+  std::vector<float> radj(size_t(std::max(P, 1)) * nt, 0.f);
+  std::vector<double> acc(static_cast<size_t>(nt));
+  for (int se = 0; se < s->n_series; ++se) {
+    std::fill(acc.begin(), acc.end(), 0.0);
+    for (int f = 0; f < s->n_freq; ++f) {
+      const double gr = dJdX[(size_t(se) * s->n_freq + f) * 2], gi = dJdX[(size_t(se) * s->n_freq + f) * 2 + 1];
+      if (gr == 0.0 && gi == 0.0) continue;
+      const double om = s->omega[size_t(f)];
+      for (int n = 0; n < nt; ++n) acc[size_t(n)] += gr * std::cos(om * n) - gi * std::sin(om * n);
+    }
+    for (int t = s->series_start[size_t(se)]; t < s->series_start[size_t(se) + 1]; ++t) {
+      const int p = s->term_probe[size_t(t)];
+      const double w = s->term_weight[size_t(t)];
+      for (int n = 0; n < nt; ++n) radj[size_t(p) * nt + n] += float(w * acc[size_t(n)]);
+    }
+  }
+  return radj;
+}
 
 // Host-to-device copy that counts its bytes on the simulation.
 void h2d(fdtd_sim* s, void* dst, const void* src, size_t bytes) {
@@ -293,7 +333,9 @@ struct Engine {
   cudaGraphExec_t graph = nullptr;
   int graph_nt = -1;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-  int64_t step_launches = 0, dft_launches = 0;
+  int64_t step_launches = 0, dft_launches = 0, adj_launches = 0;
+  double adj_ms = 0;
+  bool use_graph = true;  // replay the time loop as a captured CUDA graph
   double last_ms = 0;
   bool timing_pending = false;
 
@@ -336,29 +378,38 @@ struct Engine {
     // plain kernel: 31 x 7 tiles, z cut into chunks
     std::vector<SimDev> devs;
     for (auto* s : sims) devs.push_back(s->dev);
-    std::vector<int4> tiles;
-    int64_t xy_tiles = 0;
-    for (auto* s : sims) xy_tiles += int64_t((s->nx + kTileX - 1) / kTileX) * ((s->ny + kTileY - 1) / kTileY);
-    const int64_t want = int64_t(n_sm) * 8;
-    for (size_t i = 0; i < sims.size(); ++i) {
-      fdtd_sim* s = sims[i];
-      int chunks = int(std::max<int64_t>(1, (want + xy_tiles - 1) / std::max<int64_t>(xy_tiles, 1)));
-      chunks = std::min(chunks, std::max(1, s->nz / 8));
-      const int zlen = cfg.zchunk > 0 ? cfg.zchunk : (s->nz + chunks - 1) / chunks;
-      zchunk_used = zlen;
-      for (int z0 = 0; z0 < s->nz; z0 += zlen)
-        for (int y0 = 0; y0 < s->ny; y0 += kTileY)
-          for (int x0 = 0; x0 < s->nx; x0 += kTileX) {
-            const int z1 = std::min(s->nz, z0 + zlen);
-            tiles.push_back(make_int4(int(i), x0 | (y0 << 16), z0 | (z1 << 16), 0));
-          }
-    }
+    const std::vector<int4> tiles = plain_tiles(n_sm, cfg.zchunk, &zchunk_used);
     grid = int(tiles.size());
     d_sims.alloc(devs.size());
     CK(cudaMemcpy(d_sims.p, devs.data(), devs.size() * sizeof(SimDev), cudaMemcpyHostToDevice));
     d_tiles.alloc(tiles.size());
     CK(cudaMemcpy(d_tiles.p, tiles.data(), tiles.size() * sizeof(int4), cudaMemcpyHostToDevice));
     n_tiles = int(tiles.size());
+  }
+
+  // Tiles of the plain kernel and of the adjoint step kernel: 31 x kTileY
+  // columns cut in z chunks, (simulation, x0 | y0 << 16, z0 | z1 << 16, 0),
+  // about eight per SM over the whole set of simulations.
+  std::vector<int4> plain_tiles(int n_sm, int zchunk, int* zlen_out = nullptr, int tx = kTileX, int ty = kTileY,
+                                int per_sm = 8) {
+    std::vector<int4> tiles;
+    int64_t xy_tiles = 0;
+    for (auto* s : sims) xy_tiles += int64_t((s->nx + tx - 1) / tx) * ((s->ny + ty - 1) / ty);
+    const int64_t want = int64_t(n_sm) * per_sm;
+    for (size_t i = 0; i < sims.size(); ++i) {
+      fdtd_sim* s = sims[i];
+      int chunks = int(std::max<int64_t>(1, (want + xy_tiles - 1) / std::max<int64_t>(xy_tiles, 1)));
+      chunks = std::min(chunks, std::max(1, s->nz / 8));
+      const int zlen = zchunk > 0 ? zchunk : (s->nz + chunks - 1) / chunks;
+      if (zlen_out) *zlen_out = zlen;
+      for (int z0 = 0; z0 < s->nz; z0 += zlen)
+        for (int y0 = 0; y0 < s->ny; y0 += ty)
+          for (int x0 = 0; x0 < s->nx; x0 += tx) {
+            const int z1 = std::min(s->nz, z0 + zlen);
+            tiles.push_back(make_int4(int(i), x0 | (y0 << 16), z0 | (z1 << 16), 0));
+          }
+    }
+    return tiles;
   }
 
   // Picks the streaming kernel's (tile height, stages, z chunk) for this set
@@ -518,112 +569,204 @@ struct Engine {
     }
   }
 
-  // Discrete adjoint of the last checkpointed run of simulation s (the only
-  // member of this engine): gradient of J with respect to (Ca, Cb1, Cb2) of
-  // each E component on the box, given dJ/dX of the device DFT. The run is
-  // replayed segment by segment from its checkpoints, last segment first; each
-  // segment's forward history of the box is captured, then its steps are
-  // reversed with the adjoint kernels (fdtd_adjoint.cuh).
-  void adjoint(fdtd_sim* s, const double* dJdX, const int* box, double* grad_out) {
+  // Box-history capture of the simulations in recorded mode (adj_mode 2):
+  // one adj_capture_kernel launch per time step, before the step, inside the
+  // captured time loop.
+  DevBuf<CapSim> d_caps;
+  int n_caps = 0, cap_blocks = 1;
+
+  void build_caps() {
+    std::vector<CapSim> v;
+    int64_t nb_max = 0;
+    for (auto* s : sims)
+      if (s->adj_mode == 2) {
+        CapSim c{};
+        c.s = s->dev;
+        c.bx0 = s->adj_box[0]; c.bx1 = s->adj_box[1]; c.by0 = s->adj_box[2];
+        c.by1 = s->adj_box[3]; c.bz0 = s->adj_box[4]; c.bz1 = s->adj_box[5];
+        c.nb = box_cells(s->adj_box);
+        c.hist = s->hist.p;
+        nb_max = std::max(nb_max, c.nb);
+        v.push_back(c);
+      }
+    n_caps = int(v.size());
+    d_caps.alloc(v.size());
+    if (!v.empty()) CK(cudaMemcpy(d_caps.p, v.data(), v.size() * sizeof(CapSim), cudaMemcpyHostToDevice));
+    cap_blocks = int(std::min<int64_t>(1024, std::max<int64_t>(1, (nb_max + 255) / 256)));
+  }
+
+  static int adj_tiles_per_sm() {
+    const char* v = std::getenv("RFN_ADJ_TILES_PER_SM");
+    return v ? std::max(1, std::atoi(v)) : 4;
+  }
+
+  // One simulation's part of an adjoint sweep: dJ/dX of its device DFT, the
+  // gradient box, and where the [9][box cells] gradient goes.
+  struct AdjRequest {
+    fdtd_sim* s;
+    const double* dJdX;
+    const int* box;
+    double* grad_out;
+  };
+
+  // Discrete adjoint of the last run of the simulations of this engine, all
+  // made for a gradient in the same mode (adj_mode of the first): gradient of
+  // J with respect to (Ca, Cb1, Cb2) of each E component on each box. The
+  // adjoint state runs backwards from step nt-1 with one adj_step_kernel
+  // launch per step over the tiles of all simulations. In recorded mode the
+  // box history of every step is already on the device; with checkpoints the
+  // run is replayed segment by segment, last segment first, capturing the
+  // segment's box history before its steps are reversed.
+  void adjoint(const std::vector<AdjRequest>& req) {
     init();
     cudaStream_t st = stream();
-    const int nt = s->ckpt_nt, K = s->ckpt_every;
-    const size_t N = s->cells_padded;
-    const int bnx = box[1] - box[0], bny = box[3] - box[2], bnz = box[5] - box[4];
-    const int64_t nb = int64_t(bnx) * bny * bnz;
-    const int P = int(s->probes.size());
-    // dJ/d(record of probe p at step n) = sum over the DFT terms (series, p, w)
-    // of w * sum_f (Re G_sf cos(w_f n) - Im G_sf sin(w_f n)), G = dJ/dX
-    std::vector<float> radj(size_t(std::max(P, 1)) * nt, 0.f);
-    {
-      std::vector<double> acc(static_cast<size_t>(nt));
-      for (int se = 0; se < s->n_series; ++se) {
-        std::fill(acc.begin(), acc.end(), 0.0);
-        for (int f = 0; f < s->n_freq; ++f) {
-          const double gr = dJdX[(size_t(se) * s->n_freq + f) * 2], gi = dJdX[(size_t(se) * s->n_freq + f) * 2 + 1];
-          if (gr == 0.0 && gi == 0.0) continue;
-          const double om = s->omega[size_t(f)];
-          for (int n = 0; n < nt; ++n) acc[size_t(n)] += gr * std::cos(om * n) - gi * std::sin(om * n);
-        }
-        for (int t = s->series_start[size_t(se)]; t < s->series_start[size_t(se) + 1]; ++t) {
-          const int p = s->term_probe[size_t(t)];
-          const double w = s->term_weight[size_t(t)];
-          for (int n = 0; n < nt; ++n) radj[size_t(p) * nt + n] += float(w * acc[size_t(n)]);
-        }
+    const int mode = req[0].s->adj_mode;
+    const int nt = req[0].s->ckpt_nt, K = mode == 1 ? req[0].s->ckpt_every : nt;
+    int dev = 0, n_sm = 148;
+    CK(cudaGetDevice(&dev));
+    CK(cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev));
+    struct Bufs {
+      DevBuf<float> lam, lams, radj, seg;
+      DevBuf<int> pidx, pfld;
+      DevBuf<double> grad;
+    };
+    std::vector<std::unique_ptr<Bufs>> bufs;
+    std::vector<AdjSim> as(req.size());
+    std::vector<CapSim> caps;
+    int64_t nb_max = 0;
+    int p_max = 0;
+    for (size_t i = 0; i < req.size(); ++i) {
+      fdtd_sim* s = req[i].s;
+      const int* box = req[i].box;
+      auto B = std::make_unique<Bufs>();
+      const size_t N = s->cells_padded;
+      const int64_t nb = box_cells(box);
+      nb_max = std::max(nb_max, nb);
+      const int P = int(s->probes.size());
+      p_max = std::max(p_max, P);
+      const std::vector<float> radj = record_adjoints(s, req[i].dJdX, nt);
+      std::vector<int> pidx(size_t(std::max(P, 1)), 0), pfld(size_t(std::max(P, 1)), 0);
+      for (int pr = 0; pr < P; ++pr) {
+        const int64_t cell = s->grid.probe_cell[size_t(pr)];
+        const int z = int(cell % s->nz), y = int((cell / s->nz) % s->ny), x = int(cell / (int64_t(s->nz) * s->ny));
+        pidx[size_t(pr)] = z * s->ny * s->pitch + y * s->pitch + x;
+        pfld[size_t(pr)] = s->probes[size_t(pr)].field;
       }
-    }
-    std::vector<int> pidx(size_t(std::max(P, 1)), 0), pfld(size_t(std::max(P, 1)), 0);
-    for (int p = 0; p < P; ++p) {
-      const int64_t cell = s->grid.probe_cell[size_t(p)];
-      const int z = int(cell % s->nz), y = int((cell / s->nz) % s->ny), x = int(cell / (int64_t(s->nz) * s->ny));
-      pidx[size_t(p)] = z * s->ny * s->pitch + y * s->pitch + x;
-      pfld[size_t(p)] = s->probes[size_t(p)].field;
-    }
-    DevBuf<float> lamE, lamH, qb, adb, hist, d_radj;
-    DevBuf<double> grad;
-    DevBuf<int> d_pidx, d_pfld;
-    lamE.alloc(6 * N);
-    lamH.alloc(6 * N);
-    qb.alloc(6 * N);
-    adb.alloc(6 * N);
-    hist.alloc(size_t(K) * 9 * size_t(nb));
-    grad.alloc(9 * size_t(nb));
-    d_radj.alloc(radj.size());
-    d_pidx.alloc(pidx.size());
-    d_pfld.alloc(pfld.size());
-    CK(cudaMemcpy(d_radj.p, radj.data(), radj.size() * sizeof(float), cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(d_pidx.p, pidx.data(), pidx.size() * sizeof(int), cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(d_pfld.p, pfld.data(), pfld.size() * sizeof(int), cudaMemcpyHostToDevice));
-    CK(cudaMemsetAsync(lamE.p, 0, 6 * N * sizeof(float), st));
-    CK(cudaMemsetAsync(lamH.p, 0, 6 * N * sizeof(float), st));
-    CK(cudaMemsetAsync(qb.p, 0, 6 * N * sizeof(float), st));
-    CK(cudaMemsetAsync(grad.p, 0, 9 * size_t(nb) * sizeof(double), st));
-    AdjDev a{};
-    a.s = s->dev;
-    a.lamE = lamE.p;
-    a.lamH = lamH.p;
-    a.q = qb.p;
-    a.ad = adb.p;
-    a.N = int64_t(N);
-    a.bx0 = box[0]; a.bx1 = box[1]; a.by0 = box[2]; a.by1 = box[3]; a.bz0 = box[4]; a.bz1 = box[5];
-    a.grad = grad.p;
-    const dim3 blk(32, 8), grd((s->nx + 31) / 32, (s->ny + 7) / 8, s->nz);
-    const int cap_blocks = int(std::min<int64_t>(1024, (nb + 255) / 256));
-    const size_t stride = 6 * N + (s->splits.n ? 12 * N : 0);
-    const int nseg = (nt + K - 1) / K;
-    for (int k = nseg - 1; k >= 0; --k) {
-      const int n0 = k * K, n1 = std::min(nt, n0 + K);
-      const size_t b = size_t(n0 & 1);
-      const float* src = s->ckpt.p + size_t(k) * stride;
-      CK(cudaMemcpyAsync(s->fields.p + b * 6 * N, src, 6 * N * sizeof(float), cudaMemcpyDeviceToDevice, st));
-      if (s->splits.n)
-        CK(cudaMemcpyAsync(s->splits.p + b * 12 * N, src + 6 * N, 12 * N * sizeof(float), cudaMemcpyDeviceToDevice,
-                           st));
-      if (cfg.variant == 1) {
-        // the streaming kernel's tile counter as it stood before step n0
-        const unsigned c0 = unsigned(n0) * unsigned(scls.n_tiles + scls.grid);
-        CK(cudaMemcpyAsync(scls.d_counter.p, &c0, sizeof(unsigned), cudaMemcpyHostToDevice, st));
-        CK(cudaStreamSynchronize(st));  // c0 lives on this stack frame
+      B->lam.alloc(12 * N);
+      CK(cudaMemsetAsync(B->lam.p, 0, 12 * N * sizeof(float), st));
+      if (s->splits.n) {
+        B->lams.alloc(24 * N);
+        CK(cudaMemsetAsync(B->lams.p, 0, 24 * N * sizeof(float), st));
       }
-      for (int n = n0; n < n1; ++n) {
-        adj_capture_kernel<<<cap_blocks, 256, 0, st>>>(a, n & 1, hist.p + size_t(n - n0) * 9 * size_t(nb));
+      B->radj.alloc(radj.size());
+      CK(cudaMemcpy(B->radj.p, radj.data(), radj.size() * sizeof(float), cudaMemcpyHostToDevice));
+      B->pidx.alloc(pidx.size());
+      CK(cudaMemcpy(B->pidx.p, pidx.data(), pidx.size() * sizeof(int), cudaMemcpyHostToDevice));
+      B->pfld.alloc(pfld.size());
+      CK(cudaMemcpy(B->pfld.p, pfld.data(), pfld.size() * sizeof(int), cudaMemcpyHostToDevice));
+      B->grad.alloc(9 * size_t(nb));
+      CK(cudaMemsetAsync(B->grad.p, 0, 9 * size_t(nb) * sizeof(double), st));
+      AdjSim& a = as[i];
+      a = AdjSim{};
+      a.nx = s->nx; a.ny = s->ny; a.nz = s->nz; a.pitch = s->pitch; a.plane = s->ny * s->pitch; a.nt = nt;
+      a.mat = s->mat.p;
+      a.rows = s->rows.p;
+      a.cell_probes = s->cell_probes.p;
+      a.N = int64_t(N);
+      a.lam = B->lam.p;
+      a.lams = B->lams.p;
+      a.radj = B->radj.p;
+      a.probe_idx = B->pidx.p;
+      a.probe_field = B->pfld.p;
+      a.n_probes = P;
+      a.bx0 = box[0]; a.bx1 = box[1]; a.by0 = box[2]; a.by1 = box[3]; a.bz0 = box[4]; a.bz1 = box[5];
+      a.nb = nb;
+      a.grad = B->grad.p;
+      if (mode == 2) {
+        a.hist = s->hist.p;
+      } else {
+        B->seg.alloc(size_t(K) * 9 * size_t(nb));
+        a.hist = B->seg.p;
+        CapSim c{};
+        c.s = s->dev;
+        c.bx0 = box[0]; c.bx1 = box[1]; c.by0 = box[2]; c.by1 = box[3]; c.bz0 = box[4]; c.bz1 = box[5];
+        c.nb = nb;
+        c.hist = B->seg.p;
+        caps.push_back(c);
+      }
+      bufs.push_back(std::move(B));
+    }
+    const std::vector<int4> tiles = plain_tiles(n_sm, 0, nullptr, kAdjTileX, kAdjTileY, adj_tiles_per_sm());
+    DevBuf<AdjSim> d_as;
+    DevBuf<int4> d_t;
+    DevBuf<CapSim> d_c;
+    d_as.alloc(as.size());
+    CK(cudaMemcpy(d_as.p, as.data(), as.size() * sizeof(AdjSim), cudaMemcpyHostToDevice));
+    d_t.alloc(tiles.size());
+    CK(cudaMemcpy(d_t.p, tiles.data(), tiles.size() * sizeof(int4), cudaMemcpyHostToDevice));
+    if (!caps.empty()) {
+      d_c.alloc(caps.size());
+      CK(cudaMemcpy(d_c.p, caps.data(), caps.size() * sizeof(CapSim), cudaMemcpyHostToDevice));
+    }
+    const int cap_grid = int(std::min<int64_t>(1024, std::max<int64_t>(1, (nb_max + 255) / 256)));
+    const dim3 blk(32, kAdjTileY + 2);
+    // register cap: two resident blocks per SM (default) or three
+    const char* mb = std::getenv("RFN_ADJ_MINB");
+    auto adj_fn = (mb && std::atoi(mb) == 3) ? &adj_step_kernel<kAdjTileY, 3> : &adj_step_kernel<kAdjTileY, 2>;
+    if (p_max > 0) {
+      adj_inject_kernel<<<dim3((p_max + 127) / 128, unsigned(as.size())), 128, 0, st>>>(d_as.p, nt - 1,
+                                                                                        (nt - 1) & 1);
+      CK(cudaGetLastError());
+    }
+    adj_launches = 0;
+    CK(cudaEventRecord(ev0, st));
+    if (mode == 2) {
+      for (int n = nt - 1; n >= 0; --n) {
+        adj_fn<<<int(tiles.size()), blk, 0, st>>>(d_as.p, d_t.p, n, 0);
         CK(cudaGetLastError());
-        launch_step(st, n);
+        ++adj_launches;
       }
-      for (int n = n1 - 1; n >= n0; --n) {
-        a.hist = hist.p + size_t(n - n0) * 9 * size_t(nb);
-        if (P > 0) {
-          adj_probe_kernel<<<(P + 127) / 128, 128, 0, st>>>(a, d_pidx.p, d_pfld.p, d_radj.p, P, nt, n);
+    } else {
+      const int nseg = (nt + K - 1) / K;
+      for (int k = nseg - 1; k >= 0; --k) {
+        const int n0 = k * K, n1 = std::min(nt, n0 + K);
+        const size_t b = size_t(n0 & 1);
+        for (const auto& r : req) {
+          fdtd_sim* s = r.s;
+          const size_t N = s->cells_padded;
+          const size_t stride = 6 * N + (s->splits.n ? 12 * N : 0);
+          const float* src = s->ckpt.p + size_t(k) * stride;
+          CK(cudaMemcpyAsync(s->fields.p + b * 6 * N, src, 6 * N * sizeof(float), cudaMemcpyDeviceToDevice, st));
+          if (s->splits.n)
+            CK(cudaMemcpyAsync(s->splits.p + b * 12 * N, src + 6 * N, 12 * N * sizeof(float),
+                               cudaMemcpyDeviceToDevice, st));
+        }
+        if (cfg.variant == 1) {
+          // the streaming kernel's tile counter as it stood before step n0
+          const unsigned c0 = unsigned(n0) * unsigned(scls.n_tiles + scls.grid);
+          CK(cudaMemcpyAsync(scls.d_counter.p, &c0, sizeof(unsigned), cudaMemcpyHostToDevice, st));
+          CK(cudaStreamSynchronize(st));  // c0 lives on this stack frame
+        }
+        for (int n = n0; n < n1; ++n) {
+          adj_capture_kernel<<<dim3(cap_grid, unsigned(caps.size())), 256, 0, st>>>(d_c.p, n, n0);
           CK(cudaGetLastError());
+          launch_step(st, n);
         }
-        adj_e_kernel<<<grd, blk, 0, st>>>(a);
-        adj_h_kernel<<<grd, blk, 0, st>>>(a);
-        CK(cudaGetLastError());
+        for (int n = n1 - 1; n >= n0; --n) {
+          adj_fn<<<int(tiles.size()), blk, 0, st>>>(d_as.p, d_t.p, n, n0);
+          CK(cudaGetLastError());
+          ++adj_launches;
+        }
       }
     }
+    CK(cudaEventRecord(ev1, st));
     CK(cudaStreamSynchronize(st));
+    float ms = 0;
+    CK(cudaEventElapsedTime(&ms, ev0, ev1));
+    adj_ms = ms;
     check_error();
-    CK(cudaMemcpy(grad_out, grad.p, 9 * size_t(nb) * sizeof(double), cudaMemcpyDeviceToHost));
+    for (size_t i = 0; i < req.size(); ++i)
+      CK(cudaMemcpy(req[i].grad_out, bufs[i]->grad.p, bufs[i]->grad.n * sizeof(double), cudaMemcpyDeviceToHost));
   }
 
   // Enqueue one full run of nt steps on stream st (used for capture and for
@@ -650,6 +793,10 @@ struct Engine {
             CK(cudaMemcpyAsync(dst + 6 * N, s->splits.p + b * 12 * N, 12 * N * sizeof(float),
                                cudaMemcpyDeviceToDevice, st));
         }
+      if (n_caps) {
+        adj_capture_kernel<<<dim3(cap_blocks, unsigned(n_caps)), 256, 0, st>>>(d_caps.p, n, 0);
+        CK(cudaGetLastError());
+      }
       launch_step(st, n);
       ++step_launches;
       for (auto* s : sims)
@@ -674,8 +821,18 @@ struct Engine {
   void run_async(int nt) {
     init();
     cudaStream_t st = stream();
+    if (!use_graph) {  // every launch issued from the host, step by step
+      reset_graph();
+      build_caps();
+      CK(cudaEventRecord(ev0, st));
+      enqueue(st, nt);
+      CK(cudaEventRecord(ev1, st));
+      timing_pending = true;
+      return;
+    }
     if (graph_nt != nt) {
       reset_graph();
+      build_caps();
       cudaStream_t cap;
       CK(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
       cudaGraph_t g = nullptr;
@@ -738,6 +895,8 @@ void compile_host(fdtd_sim* s) {
   if (!compile_grid(s->nx, s->ny, s->nz, cp, s->probes, threads_for_host(), s->grid, err))
     throw ArgError{FDTD_ERR_LIMIT, err};
   s->compiled = true;
+  s->base_rows = int(s->grid.rows.size());
+  s->box_rows_from = -1;
 }
 
 void prepare(fdtd_sim* s, int nt) {
@@ -749,6 +908,7 @@ void prepare(fdtd_sim* s, int nt) {
   const int nx = s->nx, ny = s->ny, nz = s->nz;
   if (!s->prepared) {
     compile_host(s);
+    ++s->generation;
     s->pitch = ((nx + 31) / 32) * 32;
     s->cells_padded = size_t(nz) * ny * s->pitch;
     if (s->cells_padded >= (size_t(1) << 31) - size_t(2) * ny * s->pitch)
@@ -901,15 +1061,178 @@ int coef_index(const char* name) {
 
 }  // namespace
 
+// Drops what the last run kept for a gradient (snapshots or box history).
+void leave_adjoint_mode(fdtd_sim* s) {
+  s->adj_mode = 0;
+  s->adj_in_batch = false;
+  s->ckpt_every = 0;
+  s->ckpt_nt = -1;
+  s->ckpt.free();
+  s->hist.free();
+  std::fill(s->adj_box, s->adj_box + 6, 0);
+}
+
+// A fresh single-simulation engine for s (descriptors, tiles, graph).
+void new_engine(fdtd_sim* s) {
+  s->engine.reset();
+  s->engine = std::make_unique<Engine>();
+  s->engine->sims = {s};
+  s->engine->cfg = s->cfg;
+  s->engine->ext_stream = s->ext_stream;
+  s->engine->use_graph = s->use_graph;
+  s->engine->build_tiles();
+}
+
+// A gradient box must be non-empty, inside the grid and free of cells with
+// split E storage (PML slabs, source cells): the gradient treats the box
+// cells' E pairs as one total with one Ca.
+void check_gradient_box(const fdtd_sim* s, const int* box) {
+  if (box[0] < 0 || box[2] < 0 || box[4] < 0 || box[1] > s->nx || box[3] > s->ny || box[5] > s->nz ||
+      box[0] >= box[1] || box[2] >= box[3] || box[4] >= box[5])
+    throw ArgError{FDTD_ERR_ARG, "gradient box must be a non-empty box inside the grid."};
+  for (int x = box[0]; x < box[1]; ++x)
+    for (int y = box[2]; y < box[3]; ++y)
+      for (int z = box[4]; z < box[5]; ++z) {
+        const uint32_t f = s->grid.rows[s->grid.ids[(size_t(x) * s->ny + y) * s->nz + z]].w[R_FLAGS];
+        if (f & kFlagESplit) throw ArgError{FDTD_ERR_ARG, "gradient box holds split-field (PML or source) cells."};
+      }
+}
+
 struct fdtd_batch {
   std::vector<fdtd_sim*> sims;
   Engine engine;
   bool dirty = true;
+  std::vector<int> gens;  // members' device-buffer generations the engine was built on
   std::string err;
   fdtd_stats stats{};
 };
 
+// Whether a member's device buffers moved since the batch engine was built.
+bool batch_moved(const fdtd_batch* b) {
+  if (b->gens.size() != b->sims.size()) return true;
+  for (size_t i = 0; i < b->sims.size(); ++i)
+    if (b->gens[i] != b->sims[i]->generation) return true;
+  return false;
+}
+
+void note_generations(fdtd_batch* b) {
+  b->gens.clear();
+  for (auto* s : b->sims) b->gens.push_back(s->generation);
+}
+
+// Material index of the box cells on the device: ids [x][y][z] of the box.
+__global__ void set_box_ids_kernel(uint16_t* mat, int ny, int pitch, int x0, int y0, int z0, int bnx, int bny,
+                                   int bnz, const uint16_t* ids) {
+  const int64_t nb = int64_t(bnx) * bny * bnz;
+  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < nb; i += int64_t(gridDim.x) * blockDim.x) {
+    const int zz = int(i % bnz), yy = int((i / bnz) % bny), xx = int(i / (int64_t(bnz) * bny));
+    mat[size_t(z0 + zz) * ny * pitch + size_t(y0 + yy) * pitch + (x0 + xx)] = ids[i];
+  }
+}
+
+// E-update coefficients of a box: host arrays, and the compiled table when
+// there is one (one dedicated row per box cell after the compiled rows).
+void set_box_coefficients(fdtd_sim* s, const int* box, const float* coefs) {
+  static const char* const names[3][4] = {{"Ca_ex_y", "Ca_ex_z", "Cb_ex_y", "Cb_ex_z"},
+                                           {"Ca_ey_z", "Ca_ey_x", "Cb_ey_z", "Cb_ey_x"},
+                                           {"Ca_ez_x", "Ca_ez_y", "Cb_ez_x", "Cb_ez_y"}};
+  if (box[0] < 0 || box[2] < 0 || box[4] < 0 || box[1] > s->nx || box[3] > s->ny || box[5] > s->nz ||
+      box[0] >= box[1] || box[2] >= box[3] || box[4] >= box[5])
+    throw ArgError{FDTD_ERR_ARG, "box must be a non-empty box inside the grid."};
+  int ci[3][4];
+  for (int c = 0; c < 3; ++c)
+    for (int k = 0; k < 4; ++k) {
+      ci[c][k] = coef_index(names[c][k]);
+      if (!s->have_coef[ci[c][k]])
+        throw ArgError{FDTD_ERR_STATE, std::string("Coefficient not set: ") + names[c][k]};
+    }
+  if (s->compiled) check_gradient_box(s, box);
+  const int bny = box[3] - box[2], bnz = box[5] - box[4];
+  const int64_t nb = box_cells(box);
+  auto cell_of = [&](int64_t bi) {
+    const int zz = int(bi % bnz), yy = int((bi / bnz) % bny), xx = int(bi / (int64_t(bnz) * bny));
+    return (size_t(box[0] + xx) * s->ny + (box[2] + yy)) * s->nz + (box[4] + zz);
+  };
+  for (int64_t bi = 0; bi < nb; ++bi) {
+    const size_t cell = cell_of(bi);
+    for (int c = 0; c < 3; ++c) {
+      const float ca = coefs[(3 * c + 0) * nb + bi], cb1 = coefs[(3 * c + 1) * nb + bi],
+                  cb2 = coefs[(3 * c + 2) * nb + bi];
+      s->coef[ci[c][0]][cell] = ca;
+      s->coef[ci[c][1]][cell] = ca;
+      s->coef[ci[c][2]][cell] = cb1;
+      s->coef[ci[c][3]][cell] = cb2;
+    }
+  }
+  if (!s->compiled) return;  // the next run compiles the arrays
+  if (s->engine) CK(cudaStreamSynchronize(s->engine->stream()));
+  std::vector<uint16_t>& ids = s->grid.ids;
+  std::vector<Row>& rows = s->grid.rows;
+  bool new_ids = false;
+  if (s->box_rows_from >= 0 && !std::equal(box, box + 6, s->box_rows_box)) {
+    // another box: the next run compiles the patched arrays afresh
+    s->compiled = false;
+    s->prepared = false;
+    return;
+  }
+  if (s->box_rows_from < 0) {
+    if (int64_t(s->base_rows) + nb > 65536)
+      throw ArgError{FDTD_ERR_LIMIT, "box needs more rows than the 16-bit material index can address."};
+    s->box_rows_from = s->base_rows;
+    std::copy(box, box + 6, s->box_rows_box);
+    rows.resize(size_t(s->base_rows) + size_t(nb));
+    for (int64_t bi = 0; bi < nb; ++bi) {
+      const size_t cell = cell_of(bi);
+      rows[size_t(s->base_rows + bi)] = rows[ids[cell]];
+      ids[cell] = uint16_t(s->base_rows + bi);
+    }
+    new_ids = true;
+  }
+  for (int64_t bi = 0; bi < nb; ++bi) {
+    Row& r = rows[size_t(s->box_rows_from + bi)];
+    for (int c = 0; c < 3; ++c) {
+      const float ca = coefs[(3 * c + 0) * nb + bi], cb1 = coefs[(3 * c + 1) * nb + bi],
+                  cb2 = coefs[(3 * c + 2) * nb + bi];
+      std::memcpy(&r.w[4 * c + 0], &ca, 4);
+      std::memcpy(&r.w[4 * c + 1], &cb1, 4);
+      std::memcpy(&r.w[4 * c + 2], &ca, 4);
+      std::memcpy(&r.w[4 * c + 3], &cb2, 4);
+    }
+  }
+  if (!s->prepared) return;  // the next run uploads the table
+  if (s->rows.n < rows.size() * 8) {
+    // a larger table: every descriptor holding the old pointer is rebuilt
+    s->rows.alloc(rows.size() * 8);
+    h2d(s, s->rows.p, rows.data(), rows.size() * sizeof(Row));
+    s->dev.rows = s->rows.p;
+    h2d(s, s->d_dev.p, &s->dev, sizeof(SimDev));
+    ++s->generation;
+    s->engine.reset();
+  } else {
+    h2d(s, s->rows.p + size_t(s->box_rows_from) * 8, rows.data() + s->box_rows_from, size_t(nb) * sizeof(Row));
+  }
+  if (new_ids) {
+    std::vector<uint16_t> bids(static_cast<size_t>(nb));
+    for (int64_t bi = 0; bi < nb; ++bi) bids[size_t(bi)] = uint16_t(s->box_rows_from + bi);
+    DevBuf<uint16_t> tmp;
+    tmp.alloc(bids.size());
+    h2d(s, tmp.p, bids.data(), bids.size() * 2);
+    set_box_ids_kernel<<<256, 256>>>(s->mat.p, s->ny, s->pitch, box[0], box[2], box[4], box[1] - box[0], bny, bnz,
+                                     tmp.p);
+    CK(cudaGetLastError());
+    CK(cudaDeviceSynchronize());
+  }
+}
+
 extern "C" {
+
+int fdtd_set_box_coefficients(fdtd_sim* s, const int* box, const float* coefs) {
+  if (!s) return FDTD_ERR_ARG;
+  return guarded(&s->err, [&] {
+    if (!box || !coefs) throw ArgError{FDTD_ERR_ARG, "null argument"};
+    set_box_coefficients(s, box, coefs);
+  });
+}
 
 int fdtd_create(int nx, int ny, int nz, fdtd_sim** out) {
   if (!out) {
@@ -1072,6 +1395,16 @@ int fdtd_set_kernel(fdtd_sim* s, int variant, int tile_y, int stages, int zchunk
   });
 }
 
+int fdtd_set_graph(fdtd_sim* s, int enabled) {
+  if (!s) return FDTD_ERR_ARG;
+  s->use_graph = enabled != 0;
+  if (s->engine) {
+    s->engine->use_graph = s->use_graph;
+    s->engine->reset_graph();
+  }
+  return FDTD_OK;
+}
+
 int fdtd_set_stream(fdtd_sim* s, void* stream) {
   if (!s) return FDTD_ERR_ARG;
   s->ext_stream = static_cast<cudaStream_t>(stream);
@@ -1083,21 +1416,13 @@ int fdtd_run_async(fdtd_sim* s, int nt) {
   if (!s) return FDTD_ERR_ARG;
   return guarded(&s->err, [&] {
     if (nt < 1) throw ArgError{FDTD_ERR_ARG, "nt must be positive."};
-    if (s->ckpt_every) {  // leave checkpoint mode: the time loop is captured without snapshots again
-      s->ckpt_every = 0;
-      s->ckpt.free();
-      s->ckpt_nt = -1;
+    if (s->adj_mode) {  // the time loop is captured without snapshots or history again
+      leave_adjoint_mode(s);
       s->engine.reset();
     }
     const bool rebuild = !s->prepared || s->prepared_nt != nt || !s->engine;
     prepare(s, nt);
-    if (rebuild) {
-      s->engine = std::make_unique<Engine>();
-      s->engine->sims = {s};
-      s->engine->cfg = s->cfg;
-      s->engine->ext_stream = s->ext_stream;
-      s->engine->build_tiles();
-    }
+    if (rebuild) new_engine(s);
     s->engine->run_async(nt);
     fill_stats(s, s->engine.get());
   });
@@ -1109,22 +1434,43 @@ int fdtd_run_checkpointed(fdtd_sim* s, int nt, int every) {
     if (nt < 1 || every < 1) throw ArgError{FDTD_ERR_ARG, "nt and the checkpoint interval must be positive."};
     // a re-prepared simulation has new device buffers: the engine (descriptors,
     // tensor maps, graph) must be rebuilt with it
-    const bool rebuild = !s->prepared || s->prepared_nt != nt || !s->engine || s->ckpt_every != every ||
-                         s->ckpt_nt != nt;
+    const bool rebuild = !s->prepared || s->prepared_nt != nt || !s->engine || s->adj_mode != 1 ||
+                         s->ckpt_every != every || s->ckpt_nt != nt;
     prepare(s, nt);
     const size_t N = s->cells_padded;
     const size_t stride = 6 * N + (s->splits.n ? 12 * N : 0);
     const size_t nseg = size_t((nt + every - 1) / every);
     if (rebuild) {
-      s->engine = std::make_unique<Engine>();
-      s->engine->sims = {s};
-      s->engine->cfg = s->cfg;
-      s->engine->ext_stream = s->ext_stream;
-      s->engine->build_tiles();
+      leave_adjoint_mode(s);
+      s->adj_mode = 1;
+      s->ckpt_every = every;
+      s->ckpt_nt = nt;
+      s->ckpt.alloc(nseg * stride);
+      new_engine(s);
     }
-    s->ckpt_every = every;
-    s->ckpt_nt = nt;
-    if (s->ckpt.n != nseg * stride) s->ckpt.alloc(nseg * stride);
+    s->engine->run_async(nt);
+    fill_stats(s, s->engine.get());
+  });
+  if (rc) return rc;
+  return fdtd_synchronize(s);
+}
+
+int fdtd_run_recorded(fdtd_sim* s, int nt, const int* box) {
+  if (!s) return FDTD_ERR_ARG;
+  const int rc = guarded(&s->err, [&] {
+    if (nt < 1 || !box) throw ArgError{FDTD_ERR_ARG, "nt must be positive and the box given."};
+    const bool rebuild = !s->prepared || s->prepared_nt != nt || !s->engine || s->adj_mode != 2 ||
+                         s->ckpt_nt != nt || !std::equal(box, box + 6, s->adj_box);
+    prepare(s, nt);
+    check_gradient_box(s, box);
+    if (rebuild) {
+      leave_adjoint_mode(s);
+      s->hist.alloc(size_t(nt) * 9 * size_t(box_cells(box)));
+      s->adj_mode = 2;
+      s->ckpt_nt = nt;
+      std::copy(box, box + 6, s->adj_box);
+      new_engine(s);
+    }
     s->engine->run_async(nt);
     fill_stats(s, s->engine.get());
   });
@@ -1136,22 +1482,18 @@ int fdtd_adjoint(fdtd_sim* s, const double* dJ_dX, int n_series, int n_freq, con
   if (!s) return FDTD_ERR_ARG;
   return guarded(&s->err, [&] {
     if (!dJ_dX || !box || !grad) throw ArgError{FDTD_ERR_ARG, "null argument"};
-    if (!s->engine || s->ckpt_every < 1 || s->ckpt_nt < 1 || !s->ckpt.n)
-      throw ArgError{FDTD_ERR_STATE, "fdtd_adjoint needs a preceding fdtd_run_checkpointed."};
+    if (!s->engine || s->adj_mode == 0 || s->ckpt_nt < 1)
+      throw ArgError{FDTD_ERR_STATE, "fdtd_adjoint needs a preceding fdtd_run_checkpointed or fdtd_run_recorded."};
     if (n_series != s->n_series || n_freq != s->n_freq || n_series < 1 || n_freq < 1)
       throw ArgError{FDTD_ERR_ARG, "dJ/dX size does not match the DFT of the run."};
     if (s->engine->sims.size() != 1) throw ArgError{FDTD_ERR_STATE, "adjoint runs need a single simulation."};
-    if (box[0] < 0 || box[2] < 0 || box[4] < 0 || box[1] > s->nx || box[3] > s->ny || box[5] > s->nz ||
-        box[0] >= box[1] || box[2] >= box[3] || box[4] >= box[5])
-      throw ArgError{FDTD_ERR_ARG, "gradient box must be a non-empty box inside the grid."};
-    for (int x = box[0]; x < box[1]; ++x)
-      for (int y = box[2]; y < box[3]; ++y)
-        for (int z = box[4]; z < box[5]; ++z) {
-          const uint32_t f = s->grid.rows[s->grid.ids[(size_t(x) * s->ny + y) * s->nz + z]].w[R_FLAGS];
-          if (f & kFlagESplit)
-            throw ArgError{FDTD_ERR_ARG, "gradient box holds split-field (PML or source) cells."};
-        }
-    s->engine->adjoint(s, dJ_dX, box, grad);
+    check_gradient_box(s, box);
+    if (s->adj_mode == 2 && !std::equal(box, box + 6, s->adj_box))
+      throw ArgError{FDTD_ERR_ARG, "gradient box differs from the box recorded by fdtd_run_recorded."};
+    if (s->adj_in_batch) throw ArgError{FDTD_ERR_STATE, "the recorded run was a batch run: use fdtd_batch_adjoint."};
+    s->engine->adjoint({Engine::AdjRequest{s, dJ_dX, box, grad}});
+    s->stats.adjoint_launches = s->engine->adj_launches;
+    s->stats.adjoint_ms = s->engine->adj_ms;
   });
 }
 
@@ -1271,6 +1613,10 @@ int fdtd_batch_run(fdtd_batch* b, int nt) {
     b->dirty = false;
     for (auto* s : b->sims) {
       if (!s->prepared || s->prepared_nt != nt) rebuild = true;
+      if (s->adj_mode) {
+        leave_adjoint_mode(s);
+        rebuild = true;
+      }
       try {
         prepare(s, nt);
       } catch (ArgError& a) {
@@ -1278,9 +1624,11 @@ int fdtd_batch_run(fdtd_batch* b, int nt) {
         throw;
       }
     }
+    if (batch_moved(b)) rebuild = true;
     if (rebuild) {
       b->engine.graph_nt = -1;
       b->engine.build_tiles();
+      note_generations(b);
     }
     b->engine.run_async(nt);
     b->engine.sync();
@@ -1304,6 +1652,67 @@ int fdtd_batch_run(fdtd_batch* b, int nt) {
       st.compile_ms += s->grid.compile_ms;
     }
     st.id_bytes = 2;
+  });
+}
+
+int fdtd_batch_run_recorded(fdtd_batch* b, int nt, const int* boxes) {
+  if (!b) return FDTD_ERR_ARG;
+  return guarded(&b->err, [&] {
+    if (nt < 1 || !boxes) throw ArgError{FDTD_ERR_ARG, "nt must be positive and the boxes given."};
+    bool rebuild = b->engine.graph_nt != nt || b->engine.n_tiles == 0 || b->dirty;
+    b->dirty = false;
+    for (size_t i = 0; i < b->sims.size(); ++i) {
+      fdtd_sim* s = b->sims[i];
+      const int* box = boxes + 6 * i;
+      if (!s->prepared || s->prepared_nt != nt) rebuild = true;
+      try {
+        prepare(s, nt);
+        check_gradient_box(s, box);
+      } catch (ArgError& a) {
+        a.msg = "batch member " + std::to_string(i) + ": " + a.msg;
+        throw;
+      }
+      if (s->adj_mode != 2 || !s->adj_in_batch || s->ckpt_nt != nt || !std::equal(box, box + 6, s->adj_box)) {
+        leave_adjoint_mode(s);
+        s->hist.alloc(size_t(nt) * 9 * size_t(box_cells(box)));
+        s->adj_mode = 2;
+        s->adj_in_batch = true;
+        s->ckpt_nt = nt;
+        std::copy(box, box + 6, s->adj_box);
+        rebuild = true;
+      }
+    }
+    if (batch_moved(b)) rebuild = true;
+    if (rebuild) {
+      b->engine.graph_nt = -1;
+      b->engine.build_tiles();
+      note_generations(b);
+    }
+    b->engine.run_async(nt);
+    b->engine.sync();
+    for (auto* s : b->sims) fill_stats(s, &b->engine);
+    b->stats.nt = nt;
+    b->stats.last_run_ms = b->engine.last_ms;
+    b->stats.step_launches = b->engine.step_launches;
+  });
+}
+
+int fdtd_batch_adjoint(fdtd_batch* b, const double* const* dJ_dX, double* const* grad) {
+  if (!b) return FDTD_ERR_ARG;
+  return guarded(&b->err, [&] {
+    if (!dJ_dX || !grad) throw ArgError{FDTD_ERR_ARG, "null argument"};
+    std::vector<Engine::AdjRequest> req;
+    for (size_t i = 0; i < b->sims.size(); ++i) {
+      fdtd_sim* s = b->sims[i];
+      if (s->adj_mode != 2 || !s->adj_in_batch || b->engine.graph_nt != s->ckpt_nt)
+        throw ArgError{FDTD_ERR_STATE, "fdtd_batch_adjoint needs a preceding fdtd_batch_run_recorded."};
+      if (s->n_series < 1 || s->n_freq < 1) throw ArgError{FDTD_ERR_STATE, "batch member without a DFT."};
+      if (!dJ_dX[i] || !grad[i]) throw ArgError{FDTD_ERR_ARG, "null member array"};
+      req.push_back(Engine::AdjRequest{s, dJ_dX[i], s->adj_box, grad[i]});
+    }
+    b->engine.adjoint(req);
+    b->stats.adjoint_launches = b->engine.adj_launches;
+    b->stats.adjoint_ms = b->engine.adj_ms;
   });
 }
 

@@ -1,6 +1,6 @@
-"""The GPU discrete adjoint (fdtd_run_checkpointed + fdtd_adjoint) against the
-FP64 numpy discrete adjoint of tests/adjoint_model.py, itself checked against
-central finite differences in tests/test_adjoint_model.py.
+"""The GPU discrete adjoint (fdtd_run_checkpointed or fdtd_run_recorded, then
+fdtd_adjoint) against the FP64 numpy discrete adjoint of tests/adjoint_model.py,
+itself checked against central finite differences in tests/test_adjoint_model.py.
 
 Tolerance: relative L2 <= 1e-4 over all gradient entries (FP32 fields and
 adjoint fields on the GPU, FP64 accumulators; FP64 throughout in numpy).
@@ -19,7 +19,14 @@ OMEGA = np.array([0.05, 0.09, 0.13])
 BOX = (7, 10, 6, 9, 4, 6)
 
 
-def _sim(s, variant, every):
+# output line voltage (E probes), input current (H loop around the strip), and
+# the input voltage on the source cells (split E cells)
+TERMS = ([(0, p, 1.0) for p in (4, 5, 6, 7)]
+         + [(1, p, w) for p, w in zip(range(8, 16), (1.0, -1.0, 1.0, -1.0, 1.0, -1.0, 0.5, -0.5))]
+         + [(2, p, -1.0) for p in (0, 1, 2, 3)])
+
+
+def _make(s, variant, terms=None):
     co, pr, mo, mem, Nx, Ny, Nz, Nt = s.pack_inputs(gpu=True)
     sim = _lib.Simulation(Nx, Ny, Nz)
     sim.set_kernel(variant)
@@ -27,13 +34,34 @@ def _sim(s, variant, every):
     for p in pr:
         sim.add_probe(p["field"], p["idx"], p["is_source"], p["values"][:Nt] if p["is_source"] else None)
     out = len(pr) - 1
-    sim.set_dft([(0, out, 1.0)], OMEGA)
-    sim.run_checkpointed(Nt, every)
+    sim.set_dft(terms or [(0, out, 1.0)], OMEGA)
     return sim, pr, Nt, out
 
 
-@pytest.mark.parametrize("variant,every", [(1, 64), (0, 100), (1, 700)])
+def _sim(s, variant, every, terms=None, box=BOX):
+    sim, pr, Nt, out = _make(s, variant, terms)
+    if every:
+        sim.run_checkpointed(Nt, every)
+    else:
+        sim.run_recorded(Nt, box)
+    return sim, pr, Nt, out
+
+
+def _series_objective(rec, terms, omega):
+    """X_s = sum over the series' terms of w DTFT(rec_p); J = sum |X|^2; dJ/drec."""
+    ph = np.exp(-1j * np.outer(omega, np.arange(rec.shape[1])))
+    X = np.zeros((max(t[0] for t in terms) + 1, len(omega)), dtype=complex)
+    for se, p, w in terms:
+        X[se] += w * (ph @ rec[p])
+    g = np.zeros_like(rec)
+    for se, p, w in terms:
+        g[p] += w * 2 * np.real(np.conj(X[se]) @ ph)
+    return X, g
+
+
+@pytest.mark.parametrize("variant,every", [(1, 64), (0, 100), (1, 700), (1, 0), (0, 0)])
 def test_gpu_adjoint_matches_numpy_adjoint(engine_lib, variant, every):
+    """every = 0: recorded box history instead of checkpoints."""
     s = configs.microstrip(n=(18, 16, 14), n_pml=3, nt=700)
     sim, pr, nt, out = _sim(s, variant, every)
     X = sim.dft()
@@ -49,3 +77,80 @@ def test_gpu_adjoint_matches_numpy_adjoint(engine_lib, variant, every):
     ref = am.adjoint(model, probes, dJ, BOX, hist)
     assert np.abs(ref).max() > 0
     assert rel_l2(grad, ref) <= 1e-4, rel_l2(grad, ref)
+
+
+@pytest.mark.parametrize("every", [0, 50])
+def test_gpu_adjoint_of_port_series(engine_lib, every):
+    """Objective over voltage and current series: adjoint sources at split
+    (source) E cells and at H probes."""
+    s = configs.microstrip(n=(18, 16, 14), n_pml=3, nt=500)
+    sim, pr, nt, _ = _sim(s, 1, every, TERMS)
+    X = sim.dft()
+    grad = sim.adjoint(2 * X, BOX)
+    stats = sim.stats()
+    ids, rows = sim.material_table()
+    sim.close()
+    assert stats["adjoint_launches"] == nt and stats["adjoint_ms"] > 0
+    model = am.Model(ids, rows)
+    probes = km.shifted_probes(pr)
+    src = np.array([p["values"][:nt] for p in pr], dtype=np.float64)
+    rec, hist = am.forward(model, probes, src, nt, BOX)
+    Xn, dJ = _series_objective(rec, TERMS, OMEGA)
+    assert rel_l2(X, Xn) < 1e-5
+    ref = am.adjoint(model, probes, dJ, BOX, hist)
+    assert rel_l2(grad, ref) <= 1e-4, rel_l2(grad, ref)
+
+
+def test_gpu_batch_adjoint_equals_single_runs(engine_lib):
+    """Batched recorded runs and one batched adjoint sweep give each member's
+    single-run gradient bit for bit (same arithmetic per cell)."""
+    models = [configs.microstrip(n=(18, 16, 14), n_pml=3, nt=400),
+              configs.microstrip(n=(23, 19, 15), n_pml=3, nt=400)]
+    boxes = [BOX, (9, 13, 7, 10, 4, 6)]
+    single = []
+    for s, box in zip(models, boxes):
+        sim, _, _, _ = _sim(s, 1, 0, TERMS, box)
+        X = sim.dft()
+        single.append((X, sim.adjoint(2 * X, box)))
+        sim.close()
+    sims = [_make(s, 1, TERMS)[0] for s in models]
+    b = _lib.Batch(sims)
+    b.run_recorded(400, boxes)
+    Xs = [sim.dft() for sim in sims]
+    grads = b.adjoint([2 * X for X in Xs])
+    assert b.stats()["adjoint_launches"] == 400
+    b.close()
+    for sim in sims:
+        sim.close()
+    for (X1, g1), X, g in zip(single, Xs, grads):
+        assert np.array_equal(X1, X)
+        assert np.array_equal(g1, g)
+
+
+def test_gpu_box_patch_runs_equal_full_arrays(engine_lib):
+    """Runs after fdtd_set_box_coefficients (table patched in place, captured
+    graph kept) equal runs of a fresh simulation given the patched arrays."""
+    from test_box_coefficients import _coefs, _patched
+    s = configs.microstrip(n=(18, 16, 14), n_pml=3, nt=300)
+    co, pr, mo, mem, Nx, Ny, Nz, Nt = s.pack_inputs(gpu=True)
+
+    def fresh(c):
+        sim = _lib.Simulation(Nx, Ny, Nz)
+        sim.set_coefficients(c)
+        for p in pr:
+            sim.add_probe(p["field"], p["idx"], p["is_source"], p["values"][:Nt] if p["is_source"] else None)
+        return sim
+
+    sim = fresh(co)
+    sim.run(Nt)
+    cur = co
+    for seed in (1, 2, 3):
+        coefs = _coefs(cur, BOX, seed)
+        sim.set_box_coefficients(BOX, coefs)
+        sim.run(Nt)
+        cur = _patched(cur, BOX, coefs)
+        ref = fresh(cur)
+        ref.run(Nt)
+        assert np.array_equal(sim.probe_values(), ref.probe_values())
+        ref.close()
+    sim.close()

@@ -125,10 +125,11 @@ def test_no_nan_after_long_run(engine_lib):
     assert np.abs(pe).max() > 0
 
 
-def _engine_probe_matrix(s, variant, **kw):
+def _engine_probe_matrix(s, variant, graph=True, **kw):
     co, pr, mo, mem, Nx, Ny, Nz, Nt = s.pack_inputs(gpu=True)
     sim = _lib.Simulation(Nx, Ny, Nz)
     sim.set_kernel(variant, **kw)
+    sim.set_graph(graph)
     sim.set_coefficients(co)
     for p in pr:
         sim.add_probe(p["field"], p["idx"], p["is_source"], p["values"] if p["is_source"] else None)
@@ -153,3 +154,13 @@ def test_stream_kernel_bitwise_equals_plain(engine_lib, ty, stages, zchunk):
         assert sa["variant"] == 0 and sb["variant"] == 1
         assert np.abs(a).max() > 0
         assert np.array_equal(a, b)
+
+
+@pytest.mark.parametrize("variant", [0, 1])
+def test_host_launched_steps_equal_graph_replay(engine_lib, variant):
+    """fdtd_set_graph(0): the same launches issued step by step from the host."""
+    s = configs.microstrip(n=(40, 30, 24), n_pml=4, nt=200)
+    a, _ = _engine_probe_matrix(s, variant)
+    b, sb = _engine_probe_matrix(s, variant, graph=False)
+    assert sb["step_launches"] == 200
+    assert np.abs(a).max() > 0 and np.array_equal(a, b)
