@@ -218,8 +218,36 @@ int fdtd_batch_adjoint(fdtd_batch* b, const double* const* dJ_dX, double* const*
 const char* fdtd_batch_last_error(const fdtd_batch* b);
 void fdtd_batch_destroy(fdtd_batch* b);
 
+/* ------------------------------------------------------------- far field */
+
+/* One face of the near-to-far-field integration surface: cells of n0 x n1
+ * on the plane normal to `axis` at `pos` (meters), indexed along the two other
+ * axes in x, y, z order; r0 / r1 their center coordinates along those axes
+ * (meters), ds their areas (m^2); J and M the equivalent electric (n x H) and
+ * magnetic (-n x E) surface currents, complex64 as interleaved (re, im)
+ * floats, [component x y z][frequency][n0][n1]. */
+typedef struct fdtd_nf2ff_face {
+  int axis;
+  int n0, n1;
+  float pos;
+  const float* r0;
+  const float* r1;
+  const float* ds;
+  const float* J;
+  const float* M;
+} fdtd_nf2ff_face;
+
+/* Far-field E of the surface currents, normalised by exp(-j beta r) / r
+ * (rfnetwork/core/src/postprocess.cpp:130-505, postprocess_nf2ff, bound as
+ * core_func.nf2ff at rfnetwork/solver.py:3014): beta [n_freq] wave numbers
+ * (1/m), theta [n_theta] and phi [n_phi] in radians; out = 2 x n_freq x
+ * n_theta x n_phi complex64 (interleaved floats), polarisations theta, phi.
+ * Runs on the current device; errors read with fdtd_global_error. */
+int fdtd_nf2ff(const fdtd_nf2ff_face* faces, int n_faces, int n_freq, const float* beta, int n_theta,
+               const float* theta, int n_phi, const float* phi, float* out);
+
 /* Last error of calls that have no handle (fdtd_create, fdtd_batch_create,
- * fdtd_step_noalloc). */
+ * fdtd_step_noalloc, fdtd_nf2ff). */
 const char* fdtd_global_error(void);
 
 /* ------------------------------------------------ caller-owned buffers */

@@ -23,8 +23,14 @@ EXPORTED = (
     "fdtd_batch_create", "fdtd_batch_run", "fdtd_batch_set_stream", "fdtd_batch_get_stats",
     "fdtd_batch_last_error", "fdtd_batch_destroy", "fdtd_global_error", "fdtd_step_noalloc",
     "fdtd_run_checkpointed", "fdtd_run_recorded", "fdtd_adjoint", "fdtd_batch_run_recorded",
-    "fdtd_batch_adjoint", "fdtd_set_graph", "fdtd_set_box_coefficients",
+    "fdtd_batch_adjoint", "fdtd_set_graph", "fdtd_set_box_coefficients", "fdtd_nf2ff",
 )
+
+
+class Nf2ffFace(ctypes.Structure):
+    _fields_ = [("axis", ctypes.c_int), ("n0", ctypes.c_int), ("n1", ctypes.c_int), ("pos", ctypes.c_float),
+                ("r0", ctypes.c_void_p), ("r1", ctypes.c_void_p), ("ds", ctypes.c_void_p), ("J", ctypes.c_void_p),
+                ("M", ctypes.c_void_p)]
 
 
 class FdtdStats(ctypes.Structure):
@@ -73,6 +79,7 @@ def load():
         "fdtd_set_stream": ([vp, vp], ip),
         "fdtd_set_graph": ([vp, ip], ip),
         "fdtd_set_box_coefficients": ([vp, vp, vp], ip),
+        "fdtd_nf2ff": ([vp, ip, ip, vp, ip, vp, ip, vp, vp], ip),
         "fdtd_get_probe_values": ([vp, vp, ip, ip], ip),
         "fdtd_get_dft": ([vp, vp, ip, ip], ip),
         "fdtd_get_monitor": ([vp, ip, vp, i64], ip),
@@ -369,3 +376,41 @@ class Batch:
             self.close()
         except Exception:
             pass
+
+
+def nf2ff(J_xyz, M_xyz, r_grid, ds_grid, surf_pos, ff_data) -> int:
+    """Far-field transform with the arguments of the reference's core_func.nf2ff
+    (rfnetwork/solver.py:3014, rfnetwork/core/src/postprocess.cpp:130-505).
+
+    J_xyz[axis][side], M_xyz[axis][side]: complex64 [3, n_freq, n0, n1] surface
+    currents; r_grid[axis][0/1]: float32 [n0, n1] cell centers (m) along the two
+    other axes; ds_grid[axis]: [n0, n1] cell areas; surf_pos[axis][side]: face
+    position (m); ff_data: dict with float32 beta, theta, phi (radians) and the
+    complex64 [2, n_freq, n_theta, n_phi] array "data", written in place."""
+    lib = load()
+    keep, faces = [], []
+    beta = np.ascontiguousarray(ff_data["beta"], dtype=np.float32)
+    theta = np.ascontiguousarray(ff_data["theta"], dtype=np.float32)
+    phi = np.ascontiguousarray(ff_data["phi"], dtype=np.float32)
+    data = ff_data["data"]
+    F = len(beta)
+    if data.dtype != np.complex64 or data.shape != (2, F, len(theta), len(phi)) or not data.flags["C_CONTIGUOUS"]:
+        raise ValueError("Invalid far-field data array. Expected complex64 (2, frequency, theta, phi).")
+    for axis in range(3):
+        r0 = np.ascontiguousarray(r_grid[axis][0], dtype=np.float32)
+        r1 = np.ascontiguousarray(r_grid[axis][1], dtype=np.float32)
+        ds = np.ascontiguousarray(np.real(ds_grid[axis]), dtype=np.float32)
+        n0, n1 = ds.shape
+        for side in range(2):
+            J = np.ascontiguousarray(J_xyz[axis][side], dtype=np.complex64)
+            M = np.ascontiguousarray(M_xyz[axis][side], dtype=np.complex64)
+            if J.shape != (3, F, n0, n1) or M.shape != (3, F, n0, n1):
+                raise ValueError("Invalid current array shape.")
+            keep += [r0, r1, ds, J, M]
+            faces.append(Nf2ffFace(axis, n0, n1, float(surf_pos[axis][side]), r0.ctypes.data, r1.ctypes.data,
+                                   ds.ctypes.data, J.ctypes.data, M.ctypes.data))
+    arr = (Nf2ffFace * len(faces))(*faces)
+    rc = lib.fdtd_nf2ff(arr, len(faces), F, _ptr(beta), len(theta), _ptr(theta), len(phi), _ptr(phi), _ptr(data))
+    if rc:
+        raise FdtdError(f"{FDTD_ERRORS.get(rc, rc)}: {lib.fdtd_global_error().decode()}")
+    return 0

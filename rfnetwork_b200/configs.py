@@ -21,14 +21,25 @@ def _grid(n):
     return [np.arange(k + 1) * D for k in n]
 
 
-def microstrip(n=(64, 64, 48), n_pml=10, nt=2000, courant=0.99):
+def _coarsened(k, spans):
+    """Uniform edges 0..k (cells of D) with every other edge dropped inside
+    the given [a, b) cell spans: cells of 2D there, D elsewhere."""
+    drop = set()
+    for a, b in spans:
+        drop.update(range(a + 1, b, 2))
+    return np.array([i * D for i in range(k + 1) if i not in drop])
+
+
+def microstrip(n=(64, 64, 48), n_pml=10, nt=2000, courant=0.99, graded=False):
     """Plain microstrip model (64x64x48, 10-cell PML on all faces, 2000 steps).
 
     eps_r = 3.0 substrate, 4 cells thick, on a PEC ground sheet; PEC strip 6
     cells wide and 1 cell thick along x over 40 cells; 50-ohm lumped ports
     at both strip ends (port 1 driven with a Gaussian-modulated sinusoid,
     10 GHz centre, 16 GHz bandwidth); line voltage probes at both ends.
-    Smaller ``n`` keeps the layout proportions for quick tests.
+    Smaller ``n`` keeps the layout proportions for quick tests. ``graded``
+    coarsens the mesh to 2-cell widths in the air above the strip and towards
+    the y sides (every feature plane stays a cell edge), for a non-uniform grid.
     """
     nx, ny, nz = n
     s = FDTD_Solver(geo.Box(bounds=(0, nx * D, 0, ny * D, 0, nz * D)), courant=courant)
@@ -48,7 +59,13 @@ def microstrip(n=(64, 64, 48), n_pml=10, nt=2000, courant=0.99):
         s.add_lumped_port(k, face, integration_line="z+")
     if n_pml:
         s.assign_PML_boundaries("x-", "x+", "y-", "y+", "z-", "z+", n_pml=n_pml)
-    s.generate_mesh(grid=_grid(n))
+    if graded:
+        grid = [np.arange(nx + 1) * D,
+                _coarsened(ny, [(n_pml + 1, y0 - 1), (y1 + 1, ny - n_pml - 1)]),
+                _coarsened(nz, [(zs + 3, nz - n_pml - 1)])]
+    else:
+        grid = _grid(n)
+    s.generate_mesh(grid=grid)
     for name, xp in (("v1", x0 + 1), ("v2", x1 - 1)):
         s.add_voltage_probe(name, geo.Line(((xp + 0.5) * D, yc * D, zs * D), ((xp + 0.5) * D, yc * D, zg * D)))
     f0, bw = 10e9, 16e9

@@ -25,6 +25,7 @@
 #include "fdtd_compile.h"
 #include "fdtd_kernels.cuh"
 #include "fdtd_adjoint.cuh"
+#include "fdtd_nf2ff.cuh"
 #include "fdtd_step_stream.cuh"
 #include <cudaTypedefs.h>
 
@@ -1731,6 +1732,73 @@ void fdtd_batch_destroy(fdtd_batch* b) {
 }
 
 const char* fdtd_global_error(void) { return g_error.c_str(); }
+
+int fdtd_nf2ff(const fdtd_nf2ff_face* faces, int n_faces, int n_freq, const float* beta, int n_theta,
+               const float* theta, int n_phi, const float* phi, float* out) {
+  return guarded(&g_error, [&] {
+    if (!faces || n_faces < 0 || n_freq < 1 || n_theta < 1 || n_phi < 1 || !beta || !theta || !phi || !out)
+      throw ArgError{FDTD_ERR_ARG, "fdtd_nf2ff: invalid arguments"};
+    if (int64_t(n_theta) * n_phi > (int64_t(1) << 30) || n_freq > 65535)
+      throw ArgError{FDTD_ERR_LIMIT, "fdtd_nf2ff: too many directions or frequencies"};
+    int64_t n_cells = 0;
+    for (int i = 0; i < n_faces; ++i) {
+      const fdtd_nf2ff_face& fc = faces[i];
+      if (fc.axis < 0 || fc.axis > 2 || fc.n0 < 0 || fc.n1 < 0)
+        throw ArgError{FDTD_ERR_ARG, "fdtd_nf2ff: invalid face"};
+      if (int64_t(fc.n0) * fc.n1 > 0 && (!fc.r0 || !fc.r1 || !fc.ds || !fc.J || !fc.M))
+        throw ArgError{FDTD_ERR_ARG, "fdtd_nf2ff: null face array"};
+      n_cells += int64_t(fc.n0) * fc.n1;
+    }
+    if (n_cells * n_freq > (int64_t(1) << 31)) throw ArgError{FDTD_ERR_LIMIT, "fdtd_nf2ff: surface too large"};
+    // cells of all faces, one block per frequency: position and ds J, ds M
+    std::vector<Nf2ffCell> host(size_t(std::max<int64_t>(1, n_cells * n_freq)));
+    int64_t c0 = 0;
+    for (int i = 0; i < n_faces; ++i) {
+      const fdtd_nf2ff_face& fc = faces[i];
+      const int64_t nc = int64_t(fc.n0) * fc.n1;
+      for (int64_t c = 0; c < nc; ++c) {
+        float xyz[3];
+        const int o0 = fc.axis == 0 ? 1 : 0, o1 = fc.axis == 2 ? 1 : 2;
+        xyz[fc.axis] = fc.pos;
+        xyz[o0] = fc.r0[c];
+        xyz[o1] = fc.r1[c];
+        const float ds = fc.ds[c];
+        for (int f = 0; f < n_freq; ++f) {
+          float v[12];
+          for (int q = 0; q < 3; ++q)
+            for (int k = 0; k < 2; ++k) {
+              v[2 * q + k] = ds * fc.J[((size_t(q) * n_freq + f) * nc + c) * 2 + k];
+              v[6 + 2 * q + k] = ds * fc.M[((size_t(q) * n_freq + f) * nc + c) * 2 + k];
+            }
+          Nf2ffCell& cell = host[size_t(f) * n_cells + c0 + c];
+          cell.pos = make_float4(xyz[0], xyz[1], xyz[2], 0.f);
+          cell.j01 = make_float4(v[0], v[1], v[2], v[3]);
+          cell.j2m0 = make_float4(v[4], v[5], v[6], v[7]);
+          cell.m12 = make_float4(v[8], v[9], v[10], v[11]);
+        }
+      }
+      c0 += nc;
+    }
+    DevBuf<Nf2ffCell> d_cells;
+    DevBuf<float> d_beta, d_theta, d_phi;
+    DevBuf<float2> d_out;
+    d_cells.alloc(host.size());
+    CK(cudaMemcpy(d_cells.p, host.data(), host.size() * sizeof(Nf2ffCell), cudaMemcpyHostToDevice));
+    d_beta.alloc(size_t(n_freq));
+    CK(cudaMemcpy(d_beta.p, beta, size_t(n_freq) * 4, cudaMemcpyHostToDevice));
+    d_theta.alloc(size_t(n_theta));
+    CK(cudaMemcpy(d_theta.p, theta, size_t(n_theta) * 4, cudaMemcpyHostToDevice));
+    d_phi.alloc(size_t(n_phi));
+    CK(cudaMemcpy(d_phi.p, phi, size_t(n_phi) * 4, cudaMemcpyHostToDevice));
+    const size_t n_out = size_t(2) * n_freq * n_theta * n_phi;
+    d_out.alloc(n_out);
+    const dim3 grid(unsigned((int64_t(n_theta) * n_phi + kNf2ffThreads - 1) / kNf2ffThreads), unsigned(n_freq));
+    nf2ff_kernel<<<grid, kNf2ffThreads>>>(d_cells.p, int(n_cells), d_beta.p, d_theta.p, n_theta, d_phi.p, n_phi,
+                                          d_out.p);
+    CK(cudaGetLastError());
+    CK(cudaMemcpy(out, d_out.p, n_out * sizeof(float2), cudaMemcpyDeviceToHost));
+  });
+}
 
 }  // extern "C"
 

@@ -55,6 +55,13 @@ def dtft(xn: np.ndarray, frequency: np.ndarray, fs: float, downsample: bool = Fa
     return Xw
 
 
+def _shift(a: np.ndarray, axis: int, lo: int) -> np.ndarray:
+    """a without its first (lo=1) or last (lo=0) entry along ``axis``."""
+    idx = [slice(None)] * a.ndim
+    idx[axis] = slice(1, None) if lo else slice(None, -1)
+    return a[tuple(idx)]
+
+
 class FDTD_Solver:
     """FDTD EM solver for PCB geometries (reference: rfnetwork/solver.py:21)."""
 
@@ -74,6 +81,7 @@ class FDTD_Solver:
         self.lumped_elements = dict()
         self.pml_boundaries = []
         self.monitors = dict()
+        self.farfield = dict()
         self.probes = dict()
         self.ports = []
         self.ports_inv = []
@@ -522,6 +530,119 @@ class FDTD_Solver:
             self.monitors[n] = dict(field=f, axis=axis_i, position=pos, index=idx, n_step=n_step,
                                     shape=tuple(shape),
                                     frequency=np.atleast_1d(frequency) if frequency is not None else None)
+
+    def add_farfield_monitor(self, frequency, padding: int = 2):
+        """Phasor monitors on the faces of a box ``padding`` cells inside the PML
+        (rfnetwork/solver.py:1777-1891): per face with PML, the two tangential E
+        components on the face plane and the two tangential H components on the
+        planes either side of it (averaged onto the face later). Faces on a side
+        without PML sit on the grid boundary and get no monitors."""
+        self.check_mesh()
+        if not len(self.pml_boundaries):
+            raise ValueError("No radiation or PML boundaries found. Unable to create farfield monitor.")
+        ff_idx = np.zeros((3, 2), dtype=np.int64)
+        surf_pos = np.zeros((3, 2), dtype=np.float64)
+        for axis in range(3):
+            a = "xyz"[axis]
+            tangential = [i for i in (0, 1, 2) if i != axis]
+            for j, side in enumerate(("n", "p")):
+                n_edges = len(self.g_edges[axis])
+                has_pml = (a + ("-" if side == "n" else "+")) in self.pml_boundaries
+                if has_pml:
+                    ff_idx[axis, j] = self._n_pml + padding if j == 0 else n_edges - self._n_pml - 1 - padding
+                else:
+                    ff_idx[axis, j] = 0 if j == 0 else n_edges - 1
+                k = int(ff_idx[axis, j])
+                surf_pos[axis, j] = conv.m_in(self.g_edges[axis][k])
+                if not has_pml:
+                    continue
+                for f in tangential:
+                    fs = "xyz"[f]
+                    self.add_field_monitor(f"ff_e{fs}_{side}{a}", f"e{fs}", a, index=k, frequency=frequency)
+                    self.add_field_monitor(f"ff_h{fs}1_{side}{a}", f"h{fs}", a, index=k, frequency=frequency)
+                    self.add_field_monitor(f"ff_h{fs}2_{side}{a}", f"h{fs}", a, index=k - 1 if j == 0 else k + 1,
+                                           frequency=frequency)
+        cell_pos, cell_w = [None] * 3, [None] * 3
+        for axis in range(3):
+            f0, f1 = [i for i in (0, 1, 2) if i != axis]
+            s0 = slice(int(ff_idx[f0, 0]), int(ff_idx[f0, 1]))
+            s1 = slice(int(ff_idx[f1, 0]), int(ff_idx[f1, 1]))
+            cell_pos[axis] = np.meshgrid(conv.m_in(self.g_cells[f0][s0]), conv.m_in(self.g_cells[f1][s1]),
+                                         indexing="ij")
+            cell_w[axis] = np.meshgrid(conv.m_in(self.d_cells[f0][s0]), conv.m_in(self.d_cells[f1][s1]),
+                                       indexing="ij")
+        self.farfield = dict(surf_pos=surf_pos, cell_pos=cell_pos, cell_w=cell_w, idx=ff_idx,
+                             frequency=np.atleast_1d(frequency))
+
+    def farfield_currents(self):
+        """Equivalent surface currents of the far-field monitors at the face
+        cell centers, in the argument layout of the far-field transform
+        (rfnetwork/solver.py:2897-2999): J = n x H, M = -n x E, H averaged
+        between its two planes and both fields averaged onto the cell centers."""
+        self.check_solution()
+        if not len(self.farfield):
+            raise RuntimeError("Far-field monitor not found.")
+        ff_idx = self.farfield["idx"]
+        F = len(self.farfield["frequency"])
+        J_xyz = [[None, None] for _ in range(3)]
+        M_xyz = [[None, None] for _ in range(3)]
+        surf_pos = [[None, None] for _ in range(3)]
+        r_grid = [[None, None] for _ in range(3)]
+        ds_grid = [None] * 3
+        for axis in range(3):
+            a = "xyz"[axis]
+            f0, f1 = [i for i in (0, 1, 2) if i != axis]
+            r_grid[axis][0] = np.array(self.farfield["cell_pos"][axis][0], dtype=np.float32, order="C")
+            r_grid[axis][1] = np.array(self.farfield["cell_pos"][axis][1], dtype=np.float32, order="C")
+            ds_grid[axis] = np.array(self.farfield["cell_w"][axis][0] * self.farfield["cell_w"][axis][1],
+                                     dtype=np.complex64, order="C")
+            shape = self.farfield["cell_pos"][axis][0].shape
+            s0 = slice(int(ff_idx[f0, 0]), int(ff_idx[f0, 1]))
+            s1 = slice(int(ff_idx[f1, 0]), int(ff_idx[f1, 1]))
+            for j, side in enumerate(("n", "p")):
+                surf_pos[axis][j] = self.farfield["surf_pos"][axis, j]
+                e_xyz = np.zeros((3, F) + shape, dtype=np.complex64)
+                h_xyz = np.zeros((3, F) + shape, dtype=np.complex64)
+                for f in (f0, f1):
+                    fs = "xyz"[f]
+                    emon, hmon1, hmon2 = f"ff_e{fs}_{side}{a}", f"ff_h{fs}1_{side}{a}", f"ff_h{fs}2_{side}{a}"
+                    if emon not in self.monitors:
+                        continue
+                    e = self.get_monitor_data(emon)[0]
+                    h1, h2 = self.get_monitor_data(hmon1)[0], self.get_monitor_data(hmon2)[0]
+                    w1 = self.d_cells[axis][self.monitors[hmon1]["index"]]
+                    w2 = self.d_cells[axis][self.monitors[hmon2]["index"]]
+                    h = (h1 * (w1 / 2) + h2 * (w2 / 2)) / ((w1 / 2) + (w2 / 2))
+                    # E: average along the other tangential axis; H: along its own
+                    e_ax = 1 if f == f1 else 2
+                    h_ax = 1 if f == f0 else 2
+                    e_c = (_shift(e, e_ax, 1) + _shift(e, e_ax, 0)) / 2
+                    h_c = (_shift(h, h_ax, 1) + _shift(h, h_ax, 0)) / 2
+                    e_xyz[f] = e_c[:, s0, s1]
+                    h_xyz[f] = h_c[:, s0, s1]
+                normal = np.array([0, 0, 0])
+                normal[axis] = -1 if j == 0 else 1
+                J_xyz[axis][j] = np.array(np.cross(normal, h_xyz, axis=0), order="C", dtype=np.complex64)
+                M_xyz[axis][j] = np.array(np.cross(-normal, e_xyz, axis=0), order="C", dtype=np.complex64)
+        return J_xyz, M_xyz, r_grid, ds_grid, surf_pos
+
+    def get_farfield_rE(self, theta, phi) -> np.ndarray:
+        """Far-field E (theta and phi polarisations) normalised by exp(-j beta r) / r,
+        [2, frequency, theta, phi] complex64, theta and phi in degrees
+        (rfnetwork/solver.py:2870-3021); the transform runs on the GPU engine."""
+        from . import _lib
+
+        theta, phi = np.atleast_1d(theta), np.atleast_1d(phi)
+        J_xyz, M_xyz, r_grid, ds_grid, surf_pos = self.farfield_currents()
+        frequency = self.farfield["frequency"]
+        ff_data = dict(
+            beta=np.array(2 * np.pi * frequency / const.c0, dtype=np.float32),
+            theta=np.array(np.deg2rad(theta), dtype=np.float32),
+            phi=np.array(np.deg2rad(phi), dtype=np.float32),
+            data=np.zeros((2, len(frequency), len(theta), len(phi)), dtype=np.complex64),
+        )
+        _lib.nf2ff(J_xyz, M_xyz, r_grid, ds_grid, surf_pos, ff_data)
+        return ff_data["data"]
 
     def add_current_probe(self, name: str, face):
         """Ampere-loop H probes around a rectangle (rfnetwork/solver.py:1893-2010)."""

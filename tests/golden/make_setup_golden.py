@@ -8,8 +8,8 @@ packing. The reference's third-party imports that are absent here
 (pyvista, np_struct, skimage, matplotlib, the compiled core) are replaced by
 minimal stand-ins:
   * pyvista objects carry only ``points`` / ``n_cells`` / ``faces`` / ``bounds``;
-  * ``_create_grid`` (the mesher, out of scope) is replaced by explicit,
-    uniform grid edges;
+  * ``_create_grid`` (the mesher, out of scope) is replaced by explicit grid
+    edges: uniform (setup_small.npz) or graded (setup_graded.npz);
   * the conductor inclusion tests use axis-aligned box / rectangle
     containment (``utils_mesh.is_point_in_surface`` and pyvista's implicit
     distance are geometry code, not coefficient math).
@@ -17,7 +17,8 @@ Everything else -- grid arrays, material averaging, coefficients, PML,
 conductors, lumped ports, probes, monitors, sources and packing -- is the
 reference code itself. The fixture pins ``rfnetwork_b200.solver`` bit-exactly.
 
-Usage:  python tests/golden/make_setup_golden.py   (needs the reference checkout)
+Usage:  python tests/golden/make_setup_golden.py [setup_small.npz] [setup_graded.npz]
+        (needs the reference checkout; writes the named fixtures, default both)
 """
 from __future__ import annotations
 
@@ -147,7 +148,26 @@ def grid_edges():
     return (np.around(np.arange(17) * d, 5), np.around(np.arange(13) * d, 5), np.around(np.arange(11) * d, 5))
 
 
-def main():
+def grid_edges_graded():
+    """Non-uniform edges for the same model: 0.005 / 0.01 / 0.015 / 0.02 cells
+    that keep every feature plane of build_model on a cell edge, with uniform
+    cells in the PML layers (x+, y-, z+)."""
+    gx = [0, 0.02, 0.03, 0.035, 0.04, 0.05, 0.06, 0.07, 0.075, 0.08, 0.085, 0.09, 0.10, 0.11, 0.12, 0.13,
+          0.14, 0.15, 0.16]
+    gy = [0, 0.01, 0.02, 0.03, 0.04, 0.05, 0.055, 0.06, 0.065, 0.07, 0.08, 0.09, 0.105, 0.12]
+    gz = [0, 0.01, 0.015, 0.02, 0.03, 0.05, 0.06, 0.07, 0.08, 0.09, 0.10]
+    return tuple(np.around(np.array(g), 5) for g in (gx, gy, gz))
+
+
+FIXTURES = {"setup_small.npz": grid_edges, "setup_graded.npz": grid_edges_graded}
+
+
+def main(names):
+    for name in names:
+        generate(name, FIXTURES[name]())
+
+
+def generate(name, edges):
     captured = {}
     ref = _install_stubs(captured)
 
@@ -160,7 +180,7 @@ def main():
         s._create_grid = fake_create_grid
         s.generate_mesh(d_max=0.01)
 
-    s = build_model(ref.FDTD_Solver, geo.Box, geo.Rectangle, geo.Line, grid_edges(), explicit_mesh)
+    s = build_model(ref.FDTD_Solver, geo.Box, geo.Rectangle, geo.Line, edges, explicit_mesh)
     s.solve(n_threads=2, show_progress=False, gpu=False)
     s.solve(n_threads=2, show_progress=False, gpu=True)
 
@@ -184,10 +204,10 @@ def main():
         out[f"port/{i}/meta"] = np.array([p["axis"], p["r0"], p["direction"]])
     out["probe_d"] = np.array([p["d"] for p in s.probes.values()], dtype=np.float64)
     out["probe_names"] = np.array(list(s.probes.keys()))
-    path = HERE / "setup_small.npz"
+    path = HERE / name
     np.savez_compressed(path, **out)
     print(f"wrote {path} ({path.stat().st_size} bytes), {len(captured['gpu']['probes'])} probes")
 
 
 if __name__ == "__main__":
-    main()
+    main(sys.argv[1:] or list(FIXTURES))

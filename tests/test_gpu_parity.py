@@ -48,6 +48,19 @@ def test_small_model_probes(engine_lib, oracle_lib, small):
     _compare_series(se, so, 1e-5)
 
 
+def test_graded_grid_model(engine_lib, oracle_lib):
+    """The same model on a non-uniform grid (cells of 0.005 to 0.02 in), whose
+    setup is pinned to the reference by tests/golden/setup_graded.npz."""
+    graded = mg.build_model(S.FDTD_Solver, geo.Box, geo.Rectangle, geo.Line, mg.grid_edges_graded(),
+                            lambda s, e: s.generate_mesh(grid=e))
+    se, pe = run_engine(graded)
+    so, po = run_oracle(graded)
+    assert rel_l2(pe, po) <= 1e-5
+    _compare_series(se, so, 1e-5)
+    for k in so.monitors:
+        assert rel_l2(se.monitors[k]["values"], so.monitors[k]["values"]) <= 1e-5, k
+
+
 def test_small_model_monitors(engine_lib, oracle_lib, small):
     se, _ = run_engine(small)
     so, _ = run_oracle(small)

@@ -1,9 +1,10 @@
 """The setup API reproduces the reference's own setup code bit for bit.
 
-tests/golden/setup_small.npz holds what rfnetwork/solver.py's solve() passed to
-the engine (coefficient dicts for both packings, probe and monitor lists,
-port records) for the model in make_setup_golden.build_model, generated by
-running the reference's Python code (see make_setup_golden.py).
+tests/golden/setup_small.npz (uniform grid) and setup_graded.npz (non-uniform
+grid) hold what rfnetwork/solver.py's solve() passed to the engine
+(coefficient dicts for both packings, probe and monitor lists, port records)
+for the model in make_setup_golden.build_model, generated by running the
+reference's Python code (see make_setup_golden.py).
 """
 import numpy as np
 import pytest
@@ -12,21 +13,31 @@ import make_setup_golden as mg
 from rfnetwork_b200 import geometry as geo
 from rfnetwork_b200 import solver as S
 
-GOLD = np.load(mg.HERE / "setup_small.npz")
+
+@pytest.fixture(scope="module", params=sorted(mg.FIXTURES))
+def case(request):
+    gold = np.load(mg.HERE / request.param)
+    model = mg.build_model(S.FDTD_Solver, geo.Box, geo.Rectangle, geo.Line, mg.FIXTURES[request.param](),
+                           lambda s, e: s.generate_mesh(grid=e))
+    return model, gold
 
 
 @pytest.fixture(scope="module")
-def model():
-    return mg.build_model(S.FDTD_Solver, geo.Box, geo.Rectangle, geo.Line, mg.grid_edges(),
-                          lambda s, e: s.generate_mesh(grid=e))
+def model(case):
+    return case[0]
 
 
-def test_time_step(model):
+@pytest.fixture(scope="module")
+def GOLD(case):
+    return case[1]
+
+
+def test_time_step(model, GOLD):
     assert np.float32(model.dt) == GOLD["dt"]
 
 
 @pytest.mark.parametrize("kind", ["cpu", "gpu"])
-def test_coefficients_bit_exact(model, kind):
+def test_coefficients_bit_exact(model, GOLD, kind):
     co, pr, mo, mem, Nx, Ny, Nz, Nt = model.pack_inputs(gpu=(kind == "gpu"), n_threads=2)
     assert (Nx, Ny, Nz, Nt) == tuple(GOLD["N"])
     for k, v in co.items():
@@ -37,7 +48,7 @@ def test_coefficients_bit_exact(model, kind):
 
 
 @pytest.mark.parametrize("kind", ["cpu", "gpu"])
-def test_probes_and_monitors(model, kind):
+def test_probes_and_monitors(model, GOLD, kind):
     co, pr, mo, mem, Nx, Ny, Nz, Nt = model.pack_inputs(gpu=(kind == "gpu"), n_threads=2)
     n_ref = len([k for k in GOLD.files if k.startswith(f"{kind}/probe/") and k.endswith("/meta")])
     assert len(pr) == n_ref
@@ -53,7 +64,7 @@ def test_probes_and_monitors(model, kind):
         assert mem.size == int(GOLD["cpu/mem_size"])
 
 
-def test_ports_and_probe_widths(model):
+def test_ports_and_probe_widths(model, GOLD):
     for i, p in enumerate(model.ports):
         assert np.array_equal(np.asarray(p["Vs_a"]), GOLD[f"port/{i}/Vs_a"])
         assert np.array_equal([p["axis"], p["r0"], p["direction"]], GOLD[f"port/{i}/meta"])
