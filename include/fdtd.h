@@ -256,9 +256,11 @@ const char* fdtd_global_error(void);
  * owned by the caller. N = nz * ny * pitch, pitch >= nx.
  *   fields       2 x 6 x N floats: [time buffer][ex ey ez hx hy hz][z][y][pitch];
  *                zero before step 0. Step n reads buffer n & 1 and writes the other.
- *   splits       2 x 12 x N floats: [time buffer][ex_y ex_z ey_z ey_x ez_x ez_y
- *                hx_y hx_z hy_z hy_x hz_x hz_y][z][y][pitch]; zero before step 0.
- *                Touched only at cells whose row flags say split, but required.
+ *   splits       2 x 12 x N floats: [time buffer][(ex_y ex_z) (ey_z ey_x) (ez_x ez_y)
+ *                (hx_y hx_z) (hy_z hy_x) (hz_x hz_y)][z][y][pitch][2], each
+ *                component's two splits interleaved per cell; zero before step 0,
+ *                8-byte aligned. Touched only for the components that a row's
+ *                flags (bits 8..13 of word 30) mark as split, but required.
  *   mat          N uint16 row indices, [z][y][pitch]; columns x >= nx hold 0.
  *                The rows and the per-cell indices (C order [x][y][z]) are what
  *                fdtd_get_material_table returns for a compiled simulation.

@@ -268,10 +268,12 @@ PFN_cuTensorMapEncodeTiled_v12000 get_encode_fn() {
 
 // Tiled tensor map over a field group of simulation s: dims (x, y, z) and,
 // for rank 5, (component, buffer) with the given element strides.
+// xmul = 2 for the split pairs, whose x rows hold 2 floats per cell.
 void encode_map(CUtensorMap* m, const void* base, CUtensorMapDataType type, int elem, const fdtd_sim* s, int rank,
-                int box_x, int box_y, int ncomp, size_t comp_stride, size_t buf_stride) {
-  const cuuint64_t dims[5] = {cuuint64_t(s->pitch), cuuint64_t(s->ny), cuuint64_t(s->nz), cuuint64_t(ncomp), 2};
-  const cuuint64_t strides[4] = {cuuint64_t(s->pitch) * elem, cuuint64_t(s->pitch) * s->ny * elem,
+                int box_x, int box_y, int ncomp, size_t comp_stride, size_t buf_stride, int xmul = 1) {
+  const cuuint64_t row = cuuint64_t(s->pitch) * xmul;
+  const cuuint64_t dims[5] = {row, cuuint64_t(s->ny), cuuint64_t(s->nz), cuuint64_t(ncomp), 2};
+  const cuuint64_t strides[4] = {row * elem, row * s->ny * elem,
                                  cuuint64_t(comp_stride) * elem, cuuint64_t(buf_stride) * elem};
   const cuuint32_t box[5] = {cuuint32_t(box_x), cuuint32_t(box_y), 1, cuuint32_t(ncomp), 1};
   const cuuint32_t estr[5] = {1, 1, 1, 1, 1};
@@ -289,10 +291,11 @@ void encode_stream_maps(StreamMaps& m, const fdtd_sim* s, int ty) {
   encode_map(&m.E, s->fields.p, F, 4, s, 5, 36, ty + 1, 3, N, 6 * N);
   encode_map(&m.H, s->fields.p + 3 * N, F, 4, s, 5, 40, ty + 2, 3, N, 6 * N);
   if (s->splits.n) {
-    encode_map(&m.Es, s->splits.p, F, 4, s, 5, 36, ty + 1, 6, N, 12 * N);
-    encode_map(&m.Hs, s->splits.p + 6 * N, F, 4, s, 5, 36, ty, 6, N, 12 * N);
-    encode_map(&m.Es16, s->splits.p, F, 4, s, 5, kStreamWin, ty + 1, 6, N, 12 * N);
-    encode_map(&m.Hs16, s->splits.p + 6 * N, F, 4, s, 5, kStreamWin, ty, 6, N, 12 * N);
+    // 3 pair components per field, 2N floats apart, x rows of 2 * pitch floats
+    encode_map(&m.Es, s->splits.p, F, 4, s, 5, 2 * 36, ty + 1, 3, 2 * N, 12 * N, 2);
+    encode_map(&m.Hs, s->splits.p + 6 * N, F, 4, s, 5, 2 * 36, ty, 3, 2 * N, 12 * N, 2);
+    encode_map(&m.Es16, s->splits.p, F, 4, s, 5, 2 * kStreamWin, ty + 1, 3, 2 * N, 12 * N, 2);
+    encode_map(&m.Hs16, s->splits.p + 6 * N, F, 4, s, 5, 2 * kStreamWin, ty, 3, 2 * N, 12 * N, 2);
   }
   encode_map(&m.ids, s->mat.p, CU_TENSOR_MAP_DATA_TYPE_UINT16, 2, s, 3, 40, ty + 1, 1, 0, 0);
 }
@@ -994,9 +997,10 @@ void prepare(fdtd_sim* s, int nt) {
       d.E[b][c] = s->fields.p + (size_t(b) * 6 + c) * N;
       d.H[b][c] = s->fields.p + (size_t(b) * 6 + 3 + c) * N;
     }
-    for (int c = 0; c < 6; ++c) {
-      d.Es[b][c] = s->splits.n ? s->splits.p + (size_t(b) * 12 + c) * N : nullptr;
-      d.Hs[b][c] = s->splits.n ? s->splits.p + (size_t(b) * 12 + 6 + c) * N : nullptr;
+    // split pairs: component c of E at float offset (12 b + 2 c) N, of H at (12 b + 6 + 2 c) N
+    for (int c = 0; c < 3; ++c) {
+      d.Es[b][c] = s->splits.n ? reinterpret_cast<float2*>(s->splits.p + (size_t(b) * 12 + 2 * c) * N) : nullptr;
+      d.Hs[b][c] = s->splits.n ? reinterpret_cast<float2*>(s->splits.p + (size_t(b) * 12 + 6 + 2 * c) * N) : nullptr;
     }
   }
   d.mat = s->mat.p;
@@ -1858,6 +1862,10 @@ extern "C" int fdtd_step_noalloc(const fdtd_device_grid* g, int n0, int n_steps,
     g_error = "fdtd_step_noalloc: every buffer pointer must be a device address";
     return FDTD_ERR_ARG;
   }
+  if (reinterpret_cast<uintptr_t>(g->splits) % 8 != 0) {
+    g_error = "fdtd_step_noalloc: the splits buffer must be 8-byte aligned (it holds float pairs)";
+    return FDTD_ERR_ARG;
+  }
   if (n_steps == 0) return FDTD_OK;
   try {
     std::lock_guard<std::mutex> lock(g_noalloc_mutex);
@@ -1892,9 +1900,9 @@ extern "C" int fdtd_step_noalloc(const fdtd_device_grid* g, int n0, int n_steps,
         d.E[b][c] = g->fields + (size_t(b) * 6 + c) * N;
         d.H[b][c] = g->fields + (size_t(b) * 6 + 3 + c) * N;
       }
-      for (int c = 0; c < 6; ++c) {
-        d.Es[b][c] = g->splits + (size_t(b) * 12 + c) * N;
-        d.Hs[b][c] = g->splits + (size_t(b) * 12 + 6 + c) * N;
+      for (int c = 0; c < 3; ++c) {
+        d.Es[b][c] = reinterpret_cast<float2*>(g->splits + (size_t(b) * 12 + 2 * c) * N);
+        d.Hs[b][c] = reinterpret_cast<float2*>(g->splits + (size_t(b) * 12 + 6 + 2 * c) * N);
       }
     }
     d.mat = g->mat;

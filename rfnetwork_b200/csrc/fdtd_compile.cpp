@@ -15,10 +15,13 @@
 //     exactly zero, so it can take its partner split's Ca with Cb = 0 without
 //     changing any result; only a guarded split carrying a source keeps the
 //     literal (Ca = 1, Cb = 0) "keep" row;
-//  3. split-field storage: a cell whose two splits of some component have
-//     different Ca (E) or Da (H) -- the PML slabs -- or that carries a soft
-//     source, is flagged for split storage. Every other cell is advanced in
-//     unsplit form, f' = Ca f + Cb1 d1 + Cb2 d2, which is the same algebra.
+//  3. split-field storage: a component whose two splits have different Ca
+//     (E) or Da (H) -- in the PML slabs -- or that carries a soft source is
+//     stored as its two splits, and its cell is flagged for split storage.
+//     Every other component is advanced in unsplit form,
+//     f' = Ca f + Cb1 d1 + Cb2 d2, which is the same algebra. Inside a
+//     single-axis slab only two of the three components of E and of H need
+//     their splits (in a z slab, ez and hz decay alike along x and y).
 #include "fdtd_compile.h"
 
 #include <algorithm>
@@ -240,12 +243,18 @@ bool compile_grid(int nx, int ny, int nz, const float* const* coef, const std::v
             }
           }
           uint32_t flags = 0;
-          const bool e_diff = r.w[R_CA_EX_Y] != r.w[R_CA_EX_Z] || r.w[R_CA_EY_Z] != r.w[R_CA_EY_X] ||
-                              r.w[R_CA_EZ_X] != r.w[R_CA_EZ_Y];
-          const bool h_diff = r.w[R_DA_HX_Y] != r.w[R_DA_HX_Z] || r.w[R_DA_HY_Z] != r.w[R_DA_HY_X] ||
-                              r.w[R_DA_HZ_X] != r.w[R_DA_HZ_Y];
-          if (e_diff || (src_mask & 7u)) flags |= kFlagESplit;
-          if (h_diff || (src_mask & 0x38u)) flags |= kFlagHSplit;
+          // a component is stored split when its two splits decay differently
+          // (Ca or Da differ: PML) or when it carries a soft source
+          const bool comp_diff[6] = {
+              r.w[R_CA_EX_Y] != r.w[R_CA_EX_Z], r.w[R_CA_EY_Z] != r.w[R_CA_EY_X],
+              r.w[R_CA_EZ_X] != r.w[R_CA_EZ_Y], r.w[R_DA_HX_Y] != r.w[R_DA_HX_Z],
+              r.w[R_DA_HY_Z] != r.w[R_DA_HY_X], r.w[R_DA_HZ_X] != r.w[R_DA_HZ_Y]};
+          for (int c = 0; c < 6; ++c)
+            if (comp_diff[c] || (src_mask & (1u << c))) flags |= kFlagCompSplit0 << c;
+          const bool e_diff = comp_diff[0] || comp_diff[1] || comp_diff[2];
+          const bool h_diff = comp_diff[3] || comp_diff[4] || comp_diff[5];
+          if (flags & (7u * kFlagCompSplit0)) flags |= kFlagESplit;
+          if (flags & (0x38u * kFlagCompSplit0)) flags |= kFlagHSplit;
           if (e_diff || h_diff) flags |= kFlagGraded;
           flags |= uint32_t(probe_count) << 16;
           e_split[t] += (flags & kFlagESplit) ? 1 : 0;

@@ -25,7 +25,8 @@ enum RowSlot : int {
   R_DA_HX_Y = 12, R_DB1_HX_Y, R_DB2_HX_Y, R_DA_HX_Z, R_DB1_HX_Z, R_DB2_HX_Z,
   R_DA_HY_Z, R_DB1_HY_Z, R_DB2_HY_Z, R_DA_HY_X, R_DB1_HY_X, R_DB2_HY_X,
   R_DA_HZ_X, R_DB1_HZ_X, R_DB2_HZ_X, R_DA_HZ_Y, R_DB1_HZ_Y, R_DB2_HZ_Y,
-  R_FLAGS = 30,  // bit 0: E split storage, bit 1: H split storage, bits 16..31: probe entries
+  R_FLAGS = 30,  // bit 0: E split storage, bit 1: H split storage, bits 8..13: which component
+                 // (ex ey ez hx hy hz) is stored split, bits 16..31: probe entries
   R_PROBE = 31,  // first entry of this cell in the per-cell probe list (-1 if none)
   kRowWords = 32
 };
@@ -34,6 +35,9 @@ constexpr uint32_t kFlagHSplit = 2u;
 // the cell's split coefficients differ (a PML cell), as opposed to a cell that
 // is split only because it carries a soft source
 constexpr uint32_t kFlagGraded = 4u;
+// component c (0..5 = ex ey ez hx hy hz) of the cell is stored as its two
+// splits; the other components of a split cell are advanced unsplit
+constexpr uint32_t kFlagCompSplit0 = 1u << 8;
 
 struct Row {
   uint32_t w[kRowWords];

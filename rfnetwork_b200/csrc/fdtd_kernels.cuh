@@ -13,9 +13,11 @@
 //            two buffers per field (step n reads buffer n&1, writes the other),
 //            so a block can recompute its halo from consistent step-n data
 //            while neighbours already write step n+1.
-//   splits   the two split components of E (ex_y, ex_z, ...) and H, same
-//            layout, read and written only for cells flagged in the material
-//            table (PML slabs, source cells); unsplit cells never touch them.
+//   splits   the two split components of E (ex_y, ex_z, ...) and H, stored
+//            as pairs: float2 [component][z][y][x] = (first, second split),
+//            read and written only for the components the material table
+//            flags as split (PML slabs, source cells); the other components
+//            of every cell are stored as totals in the field arrays.
 //   material uint16 [z][y][x] row index into a table of 32-word rows: the
 //            cell's 30 update coefficients + flags + probe-list offset.
 //
@@ -38,6 +40,8 @@ constexpr int kTileY = 7;         // rows owned per tile along y (warp 0 is the 
 constexpr int kBlockY = kTileY + 1;
 
 constexpr uint32_t kESplit = 1u, kHSplit = 2u;
+// bit of component c (0..5 = ex ey ez hx hy hz) stored as its split pair
+constexpr uint32_t kCompSplit0 = 1u << 8;
 
 
 struct SimDev {
@@ -47,8 +51,8 @@ struct SimDev {
   int nt;
   float* E[2][3];         // [buffer][ex, ey, ez]
   float* H[2][3];         // [buffer][hx, hy, hz]
-  float* Es[2][6];        // [buffer][ex_y, ex_z, ey_z, ey_x, ez_x, ez_y]
-  float* Hs[2][6];        // [buffer][hx_y, hx_z, hy_z, hy_x, hz_x, hz_y]
+  float2* Es[2][3];       // [buffer][(ex_y, ex_z), (ey_z, ey_x), (ez_x, ez_y)]
+  float2* Hs[2][3];       // [buffer][(hx_y, hx_z), (hy_z, hy_x), (hz_x, hz_y)]
   const uint16_t* mat;    // [z][y][pitch]
   const float4* rows;     // 8 float4 per row
   const int2* cell_probes;  // (probe, field) grouped per probe cell
@@ -158,34 +162,58 @@ fdtd_step_kernel(const SimDev* __restrict__ sims, const int4* __restrict__ tiles
         ey = upd_e(b.x, __ldg(Ey + idx), b.y, dhx_z, b.w, dhz_x);
         ez = upd_e(d.x, __ldg(Ez + idx), d.y, dhy_x, d.w, dhx_y);
       } else {
-        const float* const* Es = S.Es[cur];
-        float s0 = upd_e_split(a.x, __ldg(Es[0] + idx), a.y, dhz_y);  // ex_y
-        float s1 = upd_e_split(a.z, __ldg(Es[1] + idx), a.w, dhy_z);  // ex_z
-        float s2 = upd_e_split(b.x, __ldg(Es[2] + idx), b.y, dhx_z);  // ey_z
-        float s3 = upd_e_split(b.z, __ldg(Es[3] + idx), b.w, dhz_x);  // ey_x
-        float s4 = upd_e_split(d.x, __ldg(Es[4] + idx), d.y, dhy_x);  // ez_x
-        float s5 = upd_e_split(d.z, __ldg(Es[5] + idx), d.w, dhx_y);  // ez_y
+        // per component: split pair (ex_y, ex_z), ... or unsplit total
+        float2* const* Es = S.Es[cur];
+        float2 p0 = make_float2(0.f, 0.f), p1 = p0, p2 = p0;
+        if (flags & (kCompSplit0 << 0)) {
+          p0 = __ldg(Es[0] + idx);
+          p0.x = upd_e_split(a.x, p0.x, a.y, dhz_y);  // ex_y
+          p0.y = upd_e_split(a.z, p0.y, a.w, dhy_z);  // ex_z
+        } else {
+          ex = upd_e(a.x, __ldg(Ex + idx), a.y, dhz_y, a.w, dhy_z);
+        }
+        if (flags & (kCompSplit0 << 1)) {
+          p1 = __ldg(Es[1] + idx);
+          p1.x = upd_e_split(b.x, p1.x, b.y, dhx_z);  // ey_z
+          p1.y = upd_e_split(b.z, p1.y, b.w, dhz_x);  // ey_x
+        } else {
+          ey = upd_e(b.x, __ldg(Ey + idx), b.y, dhx_z, b.w, dhz_x);
+        }
+        if (flags & (kCompSplit0 << 2)) {
+          p2 = __ldg(Es[2] + idx);
+          p2.x = upd_e_split(d.x, p2.x, d.y, dhy_x);  // ez_x
+          p2.y = upd_e_split(d.z, p2.y, d.w, dhx_y);  // ez_y
+        } else {
+          ez = upd_e(d.x, __ldg(Ez + idx), d.y, dhy_x, d.w, dhx_y);
+        }
         const int np = int(flags >> 16);
         if (np) {
-          // soft sources: s1 += v; s2 += v; f = s1 + s2 (solver.cu:459-488)
+          // soft sources: s1 += v; s2 += v; f = s1 + s2 (solver.cu:459-488);
+          // a sourced component is always stored split
           const int first = __float_as_int(rw7.w);
           for (int e = 0; e < np; ++e) {
             const int2 pe = __ldg(S.cell_probes + first + e);
             if (pe.y < 3 && __ldg(S.is_src + pe.x)) {
               const float v = __ldg(S.src + (size_t)pe.x * S.nt + n);
-              if (pe.y == 0) { s0 = __fadd_rn(s0, v); s1 = __fadd_rn(s1, v); }
-              if (pe.y == 1) { s2 = __fadd_rn(s2, v); s3 = __fadd_rn(s3, v); }
-              if (pe.y == 2) { s4 = __fadd_rn(s4, v); s5 = __fadd_rn(s5, v); }
+              if (pe.y == 0) { p0.x = __fadd_rn(p0.x, v); p0.y = __fadd_rn(p0.y, v); }
+              if (pe.y == 1) { p1.x = __fadd_rn(p1.x, v); p1.y = __fadd_rn(p1.y, v); }
+              if (pe.y == 2) { p2.x = __fadd_rn(p2.x, v); p2.y = __fadd_rn(p2.y, v); }
             }
           }
         }
-        ex = __fadd_rn(s0, s1);
-        ey = __fadd_rn(s2, s3);
-        ez = __fadd_rn(s4, s5);
-        if (own && z >= z0) {
-          float* const* Eo = S.Es[nxt];
-          Eo[0][idx] = s0; Eo[1][idx] = s1; Eo[2][idx] = s2;
-          Eo[3][idx] = s3; Eo[4][idx] = s4; Eo[5][idx] = s5;
+        const bool st = own && z >= z0;
+        float2* const* Eo = S.Es[nxt];
+        if (flags & (kCompSplit0 << 0)) {
+          ex = __fadd_rn(p0.x, p0.y);
+          if (st) Eo[0][idx] = p0;
+        }
+        if (flags & (kCompSplit0 << 1)) {
+          ey = __fadd_rn(p1.x, p1.y);
+          if (st) Eo[1][idx] = p1;
+        }
+        if (flags & (kCompSplit0 << 2)) {
+          ez = __fadd_rn(p2.x, p2.y);
+          if (st) Eo[2][idx] = p2;
         }
       }
     }
@@ -200,11 +228,10 @@ fdtd_step_kernel(const SimDev* __restrict__ sims, const int4* __restrict__ tiles
     if (own && z >= z0 && zin) {
       const float ex_ym = s_ex[buf][w - 1][lane];
       const float ez_ym = s_ez[buf][w - 1][lane];
-      if (!(flags & kESplit)) {
-        S.E[nxt][0][idx] = ex;
-        S.E[nxt][1][idx] = ey;
-        S.E[nxt][2][idx] = ez;
-      }
+      // totals of the components not stored split
+      if (!(flags & (kCompSplit0 << 0))) S.E[nxt][0][idx] = ex;
+      if (!(flags & (kCompSplit0 << 1))) S.E[nxt][1][idx] = ey;
+      if (!(flags & (kCompSplit0 << 2))) S.E[nxt][2][idx] = ez;
       const float4* row = S.rows + 8 * id;
       const float4 p = __ldg(row + 3), q = __ldg(row + 4), u = __ldg(row + 5), v6 = __ldg(row + 6);
       // slots 12..29: (Da, Db1, Db2) for hx_y, hx_z, hy_z, hy_x, hz_x, hz_y
@@ -225,13 +252,29 @@ fdtd_step_kernel(const SimDev* __restrict__ sims, const int4* __restrict__ tiles
         hy = upd_h(da_yz, hy_c, gyz, gyx);
         hz = upd_h(da_zx, hz_c, gzx, gzy);
       } else {
-        const float* const* Hs = S.Hs[cur];
-        float s0 = upd_h_split(da_xy, __ldg(Hs[0] + idx), gxy);
-        float s1 = upd_h_split(da_xz, __ldg(Hs[1] + idx), gxz);
-        float s2 = upd_h_split(da_yz, __ldg(Hs[2] + idx), gyz);
-        float s3 = upd_h_split(da_yx, __ldg(Hs[3] + idx), gyx);
-        float s4 = upd_h_split(da_zx, __ldg(Hs[4] + idx), gzx);
-        float s5 = upd_h_split(da_zy, __ldg(Hs[5] + idx), gzy);
+        const float2* const* Hs = S.Hs[cur];
+        float2 p0 = make_float2(0.f, 0.f), p1 = p0, p2 = p0;
+        if (flags & (kCompSplit0 << 3)) {
+          p0 = __ldg(Hs[0] + idx);
+          p0.x = upd_h_split(da_xy, p0.x, gxy);
+          p0.y = upd_h_split(da_xz, p0.y, gxz);
+        } else {
+          hx = upd_h(da_xy, hx_c, gxy, gxz);
+        }
+        if (flags & (kCompSplit0 << 4)) {
+          p1 = __ldg(Hs[1] + idx);
+          p1.x = upd_h_split(da_yz, p1.x, gyz);
+          p1.y = upd_h_split(da_yx, p1.y, gyx);
+        } else {
+          hy = upd_h(da_yz, hy_c, gyz, gyx);
+        }
+        if (flags & (kCompSplit0 << 5)) {
+          p2 = __ldg(Hs[2] + idx);
+          p2.x = upd_h_split(da_zx, p2.x, gzx);
+          p2.y = upd_h_split(da_zy, p2.y, gzy);
+        } else {
+          hz = upd_h(da_zx, hz_c, gzx, gzy);
+        }
         const int np = int(flags >> 16);
         if (np) {
           const int first = __float_as_int(rw7.w);
@@ -239,18 +282,25 @@ fdtd_step_kernel(const SimDev* __restrict__ sims, const int4* __restrict__ tiles
             const int2 pe = __ldg(S.cell_probes + first + e);
             if (pe.y >= 3 && __ldg(S.is_src + pe.x)) {
               const float v = __ldg(S.src + (size_t)pe.x * S.nt + n);
-              if (pe.y == 3) { s0 = __fadd_rn(s0, v); s1 = __fadd_rn(s1, v); }
-              if (pe.y == 4) { s2 = __fadd_rn(s2, v); s3 = __fadd_rn(s3, v); }
-              if (pe.y == 5) { s4 = __fadd_rn(s4, v); s5 = __fadd_rn(s5, v); }
+              if (pe.y == 3) { p0.x = __fadd_rn(p0.x, v); p0.y = __fadd_rn(p0.y, v); }
+              if (pe.y == 4) { p1.x = __fadd_rn(p1.x, v); p1.y = __fadd_rn(p1.y, v); }
+              if (pe.y == 5) { p2.x = __fadd_rn(p2.x, v); p2.y = __fadd_rn(p2.y, v); }
             }
           }
         }
-        hx = __fadd_rn(s0, s1);
-        hy = __fadd_rn(s2, s3);
-        hz = __fadd_rn(s4, s5);
-        float* const* Ho = S.Hs[nxt];
-        Ho[0][idx] = s0; Ho[1][idx] = s1; Ho[2][idx] = s2;
-        Ho[3][idx] = s3; Ho[4][idx] = s4; Ho[5][idx] = s5;
+        float2* const* Ho = S.Hs[nxt];
+        if (flags & (kCompSplit0 << 3)) {
+          hx = __fadd_rn(p0.x, p0.y);
+          Ho[0][idx] = p0;
+        }
+        if (flags & (kCompSplit0 << 4)) {
+          hy = __fadd_rn(p1.x, p1.y);
+          Ho[1][idx] = p1;
+        }
+        if (flags & (kCompSplit0 << 5)) {
+          hz = __fadd_rn(p2.x, p2.y);
+          Ho[2][idx] = p2;
+        }
       }
       S.H[nxt][0][idx] = hx;
       S.H[nxt][1][idx] = hy;
@@ -362,8 +412,12 @@ __global__ void monitor_kernel(const SimDev* __restrict__ sim, const MonDev* __r
       const uint32_t flags = __float_as_uint(S.rows[8 * S.mat[idx] + 7].z);
       float v;
       if (M.field < 3) {
-        v = (flags & kESplit) ? S.Es[buf][2 * M.field][idx] + S.Es[buf][2 * M.field + 1][idx]
-                              : S.E[buf][M.field][idx];
+        if (flags & (kCompSplit0 << M.field)) {
+          const float2 p = S.Es[buf][M.field][idx];
+          v = p.x + p.y;
+        } else {
+          v = S.E[buf][M.field][idx];
+        }
       } else {
         v = S.H[buf][M.field - 3][idx];
       }

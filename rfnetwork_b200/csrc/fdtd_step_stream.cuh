@@ -17,10 +17,10 @@
 //               H^n     3 components, rows y0-1 .. y0+TY, 40 columns
 //               E^n     3 components, rows y0-1 .. y0+TY-1, 36 columns
 //               index   16-bit material rows, 40 columns
-//               splits  the 6 E and 6 H split components, only for planes the
-//                       host flagged as holding split-field cells (PML slabs,
-//                       soft sources) -- a 64-bit mask per tile; over 36
-//                       columns, or over the 16-column window [wx0, wx0+16)
+//               splits  the 3 E and 3 H split pairs (float2 per cell), only
+//                       for planes the host flagged as holding split-field
+//                       cells (PML slabs, soft sources) -- a 64-bit mask per
+//                       tile; over 36 columns, or over the 16-column window [wx0, wx0+16)
 //                       on planes whose split cells all lie in it (the x-PML
 //                       slab crossing an ordinary tile), a second mask
 //             Every box starts at an x that is a multiple of 16 bytes at or
@@ -114,9 +114,10 @@ __device__ __forceinline__ void prefetch_l1(const void* p) {
 }
 
 // Soft sources of one field group of a cell (solver.cu:459-488, 515-541):
-// s1 += v; s2 += v for every source probe on a component of that group.
+// s1 += v; s2 += v for every source probe on a component of that group (a
+// sourced component is always stored as its split pair).
 __device__ __forceinline__ void stream_inject(const SimDev& Sd, const float4& r7, uint32_t flags, int n, bool e_side,
-                                              float (&s)[6]) {
+                                              float2 (&p)[3]) {
   const int np = int(flags >> 16);
   const int first = __float_as_int(r7.w);
   for (int e = 0; e < np; ++e) {
@@ -128,8 +129,8 @@ __device__ __forceinline__ void stream_inject(const SimDev& Sd, const float4& r7
 #pragma unroll
       for (int k = 0; k < 3; ++k)
         if (c == k) {
-          s[2 * k] = __fadd_rn(s[2 * k], v);
-          s[2 * k + 1] = __fadd_rn(s[2 * k + 1], v);
+          p[k].x = __fadd_rn(p[k].x, v);
+          p[k].y = __fadd_rn(p[k].y, v);
         }
     }
   }
@@ -220,12 +221,13 @@ fdtd_step_stream_kernel(const SimDev* __restrict__ sims, const StreamTile* __res
         if (!last) {
           tma_load_5d(b + G::OFF_E, &maps->E, xs, td.y0 - 1, zp, 0, cur, &full[sq]);
           tma_load_3d(b + G::OFF_I, &maps->ids, xi, td.y0 - 1, zp, &full[sq]);
+          // split pairs are interleaved along x: float column 2x holds cell x
           if (split && win) {
-            tma_load_5d(b + G::OFF_ES, &maps->Es16, td.wx0, td.y0 - 1, zp, 0, cur, &full[sq]);
-            tma_load_5d(b + G::OFF_HS, &maps->Hs16, td.wx0, td.y0, zp, 0, cur, &full[sq]);
+            tma_load_5d(b + G::OFF_ES, &maps->Es16, 2 * td.wx0, td.y0 - 1, zp, 0, cur, &full[sq]);
+            tma_load_5d(b + G::OFF_HS, &maps->Hs16, 2 * td.wx0, td.y0, zp, 0, cur, &full[sq]);
           } else if (split) {
-            tma_load_5d(b + G::OFF_ES, &maps->Es, xs, td.y0 - 1, zp, 0, cur, &full[sq]);
-            tma_load_5d(b + G::OFF_HS, &maps->Hs, xs, td.y0, zp, 0, cur, &full[sq]);
+            tma_load_5d(b + G::OFF_ES, &maps->Es, 2 * xs, td.y0 - 1, zp, 0, cur, &full[sq]);
+            tma_load_5d(b + G::OFF_HS, &maps->Hs, 2 * xs, td.y0, zp, 0, cur, &full[sq]);
           }
         }
         ++q;
@@ -334,26 +336,41 @@ fdtd_step_stream_kernel(const SimDev* __restrict__ sims, const StreamTile* __res
         ey = upd_e(rb.x, sE[EC + eb], rb.y, dhx_z, rb.w, dhz_x);
         ez = upd_e(rd.x, sE[2 * EC + eb], rd.y, dhy_x, rd.w, dhx_y);
       } else {
-        float sp[6];
+        // per component: the split pair (one 8-byte load at the selected
+        // offset) or the unsplit total
+        float2 sp[3];
+        const float2* sP = reinterpret_cast<const float2*>(sEs);
 #pragma unroll
-        for (int m = 0; m < 6; ++m) {
-          const int o = win ? m * G::SECN + ebn : m * EC + eb;  // one load at the selected offset
-          sp[m] = sEs[o];
+        for (int m = 0; m < 3; ++m) sp[m] = make_float2(0.f, 0.f);
+        if (flags & (kCompSplit0 << 0)) {
+          sp[0] = sP[win ? ebn : eb];
+          sp[0].x = upd_e_split(ra.x, sp[0].x, ra.y, dhz_y);  // ex_y
+          sp[0].y = upd_e_split(ra.z, sp[0].y, ra.w, dhy_z);  // ex_z
+        } else {
+          ex = upd_e(ra.x, sE[eb], ra.y, dhz_y, ra.w, dhy_z);
         }
-        sp[0] = upd_e_split(ra.x, sp[0], ra.y, dhz_y);  // ex_y
-        sp[1] = upd_e_split(ra.z, sp[1], ra.w, dhy_z);  // ex_z
-        sp[2] = upd_e_split(rb.x, sp[2], rb.y, dhx_z);  // ey_z
-        sp[3] = upd_e_split(rb.z, sp[3], rb.w, dhz_x);  // ey_x
-        sp[4] = upd_e_split(rd.x, sp[4], rd.y, dhy_x);  // ez_x
-        sp[5] = upd_e_split(rd.z, sp[5], rd.w, dhx_y);  // ez_y
+        if (flags & (kCompSplit0 << 1)) {
+          sp[1] = sP[win ? G::SECN + ebn : EC + eb];
+          sp[1].x = upd_e_split(rb.x, sp[1].x, rb.y, dhx_z);  // ey_z
+          sp[1].y = upd_e_split(rb.z, sp[1].y, rb.w, dhz_x);  // ey_x
+        } else {
+          ey = upd_e(rb.x, sE[EC + eb], rb.y, dhx_z, rb.w, dhz_x);
+        }
+        if (flags & (kCompSplit0 << 2)) {
+          sp[2] = sP[win ? 2 * G::SECN + ebn : 2 * EC + eb];
+          sp[2].x = upd_e_split(rd.x, sp[2].x, rd.y, dhy_x);  // ez_x
+          sp[2].y = upd_e_split(rd.z, sp[2].y, rd.w, dhx_y);  // ez_y
+        } else {
+          ez = upd_e(rd.x, sE[2 * EC + eb], rd.y, dhy_x, rd.w, dhx_y);
+        }
         if (flags >> 16) stream_inject(Sd, r7, flags, n, true, sp);
-        ex = __fadd_rn(sp[0], sp[1]);
-        ey = __fadd_rn(sp[2], sp[3]);
-        ez = __fadd_rn(sp[4], sp[5]);
+        if (flags & (kCompSplit0 << 0)) ex = __fadd_rn(sp[0].x, sp[0].y);
+        if (flags & (kCompSplit0 << 1)) ey = __fadd_rn(sp[1].x, sp[1].y);
+        if (flags & (kCompSplit0 << 2)) ez = __fadd_rn(sp[2].x, sp[2].y);
         if (store) {
-          float* const so = Sd.Es[nxt][0];
 #pragma unroll
-          for (int m = 0; m < 6; ++m) so[m * N + idx] = sp[m];
+          for (int m = 0; m < 3; ++m)
+            if (flags & (kCompSplit0 << m)) Sd.Es[nxt][m][idx] = sp[m];
         }
       }
       xb[w * 32 + lane] = ex;
@@ -370,11 +387,10 @@ fdtd_step_stream_kernel(const SimDev* __restrict__ sims, const StreamTile* __res
       if (store) {
         const float ex_ym = xb[(w - 1) * 32 + lane];
         const float ez_ym = xb[G::ER * 32 + (w - 1) * 32 + lane];
-        if (!(flags & kESplit)) {
-          fo[idx] = ex;
-          fo[N + idx] = ey;
-          fo[2 * N + idx] = ez;
-        }
+        // totals of the components not stored split
+        if (!(flags & (kCompSplit0 << 0))) fo[idx] = ex;
+        if (!(flags & (kCompSplit0 << 1))) fo[N + idx] = ey;
+        if (!(flags & (kCompSplit0 << 2))) fo[2 * N + idx] = ez;
         // slots 12..29: (Da, Db1, Db2) of hx_y, hx_z, hy_z, hy_x, hz_x, hz_y
         const float gxy = h_term(rp.z, ez, rp.y, ez_ym);
         const float gxz = h_term(rq.y, ey, rq.x, ey_p);
@@ -388,25 +404,38 @@ fdtd_step_stream_kernel(const SimDev* __restrict__ sims, const StreamTile* __res
           hy = upd_h(rq.z, hy_c, gyz, gyx);
           hz = upd_h(rv.x, hz_c, gzx, gzy);
         } else {
-          float sp[6];
+          float2 sp[3];
+          const float2* sP = reinterpret_cast<const float2*>(sHs);
 #pragma unroll
-          for (int m = 0; m < 6; ++m) {
-            const int o = win ? m * G::SHCN + sbn : m * G::SHC + sb;
-            sp[m] = sHs[o];
+          for (int m = 0; m < 3; ++m) sp[m] = make_float2(0.f, 0.f);
+          if (flags & (kCompSplit0 << 3)) {
+            sp[0] = sP[win ? sbn : sb];
+            sp[0].x = upd_h_split(rp.x, sp[0].x, gxy);
+            sp[0].y = upd_h_split(rp.w, sp[0].y, gxz);
+          } else {
+            hx = upd_h(rp.x, hx_c, gxy, gxz);
           }
-          sp[0] = upd_h_split(rp.x, sp[0], gxy);
-          sp[1] = upd_h_split(rp.w, sp[1], gxz);
-          sp[2] = upd_h_split(rq.z, sp[2], gyz);
-          sp[3] = upd_h_split(ru.y, sp[3], gyx);
-          sp[4] = upd_h_split(rv.x, sp[4], gzx);
-          sp[5] = upd_h_split(rv.w, sp[5], gzy);
+          if (flags & (kCompSplit0 << 4)) {
+            sp[1] = sP[win ? G::SHCN + sbn : G::SHC + sb];
+            sp[1].x = upd_h_split(rq.z, sp[1].x, gyz);
+            sp[1].y = upd_h_split(ru.y, sp[1].y, gyx);
+          } else {
+            hy = upd_h(rq.z, hy_c, gyz, gyx);
+          }
+          if (flags & (kCompSplit0 << 5)) {
+            sp[2] = sP[win ? 2 * G::SHCN + sbn : 2 * G::SHC + sb];
+            sp[2].x = upd_h_split(rv.x, sp[2].x, gzx);
+            sp[2].y = upd_h_split(rv.w, sp[2].y, gzy);
+          } else {
+            hz = upd_h(rv.x, hz_c, gzx, gzy);
+          }
           if (flags >> 16) stream_inject(Sd, r7, flags, n, false, sp);
-          hx = __fadd_rn(sp[0], sp[1]);
-          hy = __fadd_rn(sp[2], sp[3]);
-          hz = __fadd_rn(sp[4], sp[5]);
-          float* const so = Sd.Hs[nxt][0];
+          if (flags & (kCompSplit0 << 3)) hx = __fadd_rn(sp[0].x, sp[0].y);
+          if (flags & (kCompSplit0 << 4)) hy = __fadd_rn(sp[1].x, sp[1].y);
+          if (flags & (kCompSplit0 << 5)) hz = __fadd_rn(sp[2].x, sp[2].y);
 #pragma unroll
-          for (int m = 0; m < 6; ++m) so[m * N + idx] = sp[m];
+          for (int m = 0; m < 3; ++m)
+            if (flags & (kCompSplit0 << (3 + m))) Sd.Hs[nxt][m][idx] = sp[m];
         }
         fo[3 * N + idx] = hx;
         fo[4 * N + idx] = hy;

@@ -1,7 +1,8 @@
 """Numpy model of the engine's update arithmetic, driven by its material table.
 
 Test helper: it replays what ``fdtd_step_kernel`` computes (unsplit update for
-ordinary cells, split update + soft sources for flagged cells, all in the
+ordinary components, split update + soft sources for the components the table
+flags as split, all in the
 reference's GPU index space) from the table that the library's host compiler
 produced. Comparing it with the CPU oracle checks the table compilation --
 guards, x-end zeroing, split flags, probe shifts -- without a GPU.
@@ -23,8 +24,8 @@ def run_model(ids, rows, cell_probes, probes, src, nt):
     R = rows.copy()
     coef = {s: _f(R, s)[ids] for s in range(30)}
     flags = R[:, 30][ids]
-    es = (flags & FLAG_E) != 0
-    hs = (flags & FLAG_H) != 0
+    # component c (ex ey ez hx hy hz) stored as its split pair: flag bit 8 + c
+    cs = [(flags & (1 << (8 + c))) != 0 for c in range(6)]
     f32 = np.float32
     E = [np.zeros(ids.shape, f32) for _ in range(3)]
     H = [np.zeros(ids.shape, f32) for _ in range(3)]
@@ -73,9 +74,9 @@ def run_model(ids, rows, cell_probes, probes, src, nt):
                 newEs[2 * fld + 1][x, y, z] += v
         for c in range(3):
             tot = newEs[2 * c] + newEs[2 * c + 1]
-            E[c] = np.where(es, tot, newE[c]).astype(f32)
+            E[c] = np.where(cs[c], tot, newE[c]).astype(f32)
         for s in range(6):
-            Es[s] = np.where(es, newEs[s], 0).astype(f32)
+            Es[s] = np.where(cs[s // 2], newEs[s], 0).astype(f32)
         ex, ey, ez = E
         g = [
             coef[14] * ez - coef[13] * bwd(ez, 1),   # hx_y
@@ -95,9 +96,9 @@ def run_model(ids, rows, cell_probes, probes, src, nt):
                 newHs[2 * c][x, y, z] += v
                 newHs[2 * c + 1][x, y, z] += v
         for c in range(3):
-            H[c] = np.where(hs, newHs[2 * c] + newHs[2 * c + 1], newH[c]).astype(f32)
+            H[c] = np.where(cs[3 + c], newHs[2 * c] + newHs[2 * c + 1], newH[c]).astype(f32)
         for s in range(6):
-            Hs[s] = np.where(hs, newHs[s], 0).astype(f32)
+            Hs[s] = np.where(cs[3 + s // 2], newHs[s], 0).astype(f32)
         for i, (fld, x, y, z, is_src) in enumerate(probes):
             rec[i, n] = (E + H)[fld][x, y, z]
     return rec
