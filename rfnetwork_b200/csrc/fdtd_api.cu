@@ -542,6 +542,15 @@ struct Engine {
             c.host_tiles.push_back(t);
           }
     }
+    // Persistent blocks take tiles in list order, so the costliest go first
+    // and the last tiles taken are short ones: a plane with split-field cells
+    // costs about three ordinary planes. Stable, so tiles of equal cost keep
+    // their z-chunk-major order and neighbours still share halos in L2.
+    auto cost = [](const StreamTile& t) {
+      return (t.z1 - t.z0 + 1) + 2 * (__builtin_popcount(t.split_lo) + __builtin_popcount(t.split_hi));
+    };
+    std::stable_sort(c.host_tiles.begin(), c.host_tiles.end(),
+                     [&](const StreamTile& a, const StreamTile& b) { return cost(a) > cost(b); });
     c.n_tiles = int(c.host_tiles.size());
     c.d_maps.alloc(c.host_maps.size());
     CK(cudaMemcpy(c.d_maps.p, c.host_maps.data(), c.host_maps.size() * sizeof(StreamMaps), cudaMemcpyHostToDevice));

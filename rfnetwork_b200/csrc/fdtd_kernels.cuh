@@ -51,6 +51,8 @@ struct SimDev {
   int nt;
   float* E[2][3];         // [buffer][ex, ey, ez]
   float* H[2][3];         // [buffer][hx, hy, hz]
+  // split pairs; Es[b][c] + (3 + c') * cells == Hs[b][c'] and components are
+  // `cells` pairs apart (the streaming kernel indexes them from Es[b][0])
   float2* Es[2][3];       // [buffer][(ex_y, ex_z), (ey_z, ey_x), (ez_x, ez_y)]
   float2* Hs[2][3];       // [buffer][(hx_y, hx_z), (hy_z, hy_x), (hz_x, hz_y)]
   const uint16_t* mat;    // [z][y][pitch]

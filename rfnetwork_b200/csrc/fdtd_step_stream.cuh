@@ -276,6 +276,8 @@ fdtd_step_stream_kernel(const SimDev* __restrict__ sims, const StreamTile* __res
     const int plane = Sd.plane;
     const int64_t N = Sd.cells;
     float* __restrict__ const fo = Sd.E[nxt][0];   // E then H components of step n+1, N apart
+    // split pairs of step n+1: E component m at m N, H component m at (3 + m) N
+    float2* __restrict__ const spo = Sd.Es[nxt][0];
     const int npl = td.z1 - z0 + 1;                // planes z0-1 .. z1-1 computed
     const int hb = w * G::HW + oh + lane;
     const int eb = w * G::EW + oh + lane;
@@ -370,7 +372,7 @@ fdtd_step_stream_kernel(const SimDev* __restrict__ sims, const StreamTile* __res
         if (store) {
 #pragma unroll
           for (int m = 0; m < 3; ++m)
-            if (flags & (kCompSplit0 << m)) Sd.Es[nxt][m][idx] = sp[m];
+            if (flags & (kCompSplit0 << m)) spo[m * N + idx] = sp[m];
         }
       }
       xb[w * 32 + lane] = ex;
@@ -435,7 +437,7 @@ fdtd_step_stream_kernel(const SimDev* __restrict__ sims, const StreamTile* __res
           if (flags & (kCompSplit0 << 5)) hz = __fadd_rn(sp[2].x, sp[2].y);
 #pragma unroll
           for (int m = 0; m < 3; ++m)
-            if (flags & (kCompSplit0 << (3 + m))) Sd.Hs[nxt][m][idx] = sp[m];
+            if (flags & (kCompSplit0 << (3 + m))) spo[(3 + m) * N + idx] = sp[m];
         }
         fo[3 * N + idx] = hx;
         fo[4 * N + idx] = hy;
