@@ -504,6 +504,7 @@ struct Engine {
       c.host_maps.emplace_back();
       encode_stream_maps(c.host_maps.back(), s, ty);
       const GradedIndex split_idx(s->grid, kFlagESplit | kFlagHSplit);
+      const GradedIndex probe_idx(s->grid, 0xFFFF0000u);  // cells with probe entries
       for (int z0 = 0; z0 < s->nz; z0 += zc)
         for (int y0 = 0; y0 < s->ny; y0 += ty)
           for (int x0 = 0; x0 < s->nx; x0 += kStreamOwnX) {
@@ -535,6 +536,7 @@ struct Engine {
             t.z0 = z0;
             t.z1 = z1;
             t.wx0 = std::max(wx0, 0);
+            t.plain = mask == 0 && probe_idx.count(x0, x0 + kStreamOwnX, y0, y0 + ty, z0, z1) == 0;
             t.split_lo = uint32_t(mask);
             t.split_hi = uint32_t(mask >> 32);
             t.narrow_lo = uint32_t(narrow);

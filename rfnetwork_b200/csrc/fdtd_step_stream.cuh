@@ -43,6 +43,8 @@
 #include "fdtd_kernels.cuh"
 #include "tma.cuh"
 
+#include <type_traits>
+
 namespace rfn {
 
 constexpr int kStreamOwnX = 31;           // owned columns per tile (lane 0 is the halo column)
@@ -60,9 +62,11 @@ struct StreamMaps {
 
 // One tile: owned [x0, x0+31) x [y0, y0+TY) x [z0, z1). Bit j of `split` is
 // set when plane z0-1+j holds split-field cells inside the tile's E region;
-// bit j of `narrow` when all of them lie in columns [wx0, wx0+16).
+// bit j of `narrow` when all of them lie in columns [wx0, wx0+16). `plain`
+// marks a tile with no split-field cells and no probe cells, which takes the
+// consumers' interior path (no per-cell flag tests).
 struct StreamTile {
-  int sim, x0, y0, z0, z1, wx0, pad0, pad1;
+  int sim, x0, y0, z0, z1, wx0, plain, pad1;
   uint32_t split_lo, split_hi, narrow_lo, narrow_hi;
 };
 
@@ -289,178 +293,185 @@ fdtd_step_stream_kernel(const SimDev* __restrict__ sims, const StreamTile* __res
     const uint64_t narrow = uint64_t(td.narrow_lo) | (uint64_t(td.narrow_hi) << 32);
     int idx = (z0 - 1) * plane + r * Sd.pitch + c; // cell offset of plane z (owned cells, z >= z0)
 
-    float ex_p = 0.f, ey_p = 0.f;  // E^{n+1} of this cell one plane below
-    for (int i = 0; i < npl; ++i) {
-      int sn = sq + 1;
-      uint32_t pn = pq;
-      if (sn == S) {
-        sn = 0;
-        pn ^= 1u;
-      }
-      // plane z was waited for as the look-ahead of the previous iteration
-      ok = ok && mbar_wait_bounded(&full[sn], pn, kStreamWaitLimit);
-      const unsigned char* st = smem + sq * G::STAGE;
-      const float* sH = reinterpret_cast<const float*>(st);
-      const float* sE = reinterpret_cast<const float*>(st + G::OFF_E);
-      const uint16_t* sI = reinterpret_cast<const uint16_t*>(st + G::OFF_I);
-      const float* sEs = reinterpret_cast<const float*>(st + G::OFF_ES);
-      const float* sHs = reinterpret_cast<const float*>(st + G::OFF_HS);
-      const float* nH = reinterpret_cast<const float*>(smem + sn * G::STAGE);
-      float* xb = xch + (i & 1) * (G::XCH / 4);
-      constexpr int HC = G::HC, EC = G::EC;
-      const bool store = own_xy && i > 0;
-      const bool win = (narrow >> i) & 1u;
+    // The plane loop, instantiated for plain tiles (FAST: every cell unsplit,
+    // no probes, so no per-cell flag tests) and for the general case.
+    auto planes = [&](auto fast_tag) -> bool {
+      constexpr bool FAST = decltype(fast_tag)::value;
+      float ex_p = 0.f, ey_p = 0.f;  // E^{n+1} of this cell one plane below
+      for (int i = 0; i < npl; ++i) {
+        int sn = sq + 1;
+        uint32_t pn = pq;
+        if (sn == S) {
+          sn = 0;
+          pn ^= 1u;
+        }
+        // plane z was waited for as the look-ahead of the previous iteration
+        ok = ok && mbar_wait_bounded(&full[sn], pn, kStreamWaitLimit);
+        const unsigned char* st = smem + sq * G::STAGE;
+        const float* sH = reinterpret_cast<const float*>(st);
+        const float* sE = reinterpret_cast<const float*>(st + G::OFF_E);
+        const uint16_t* sI = reinterpret_cast<const uint16_t*>(st + G::OFF_I);
+        const float* sEs = reinterpret_cast<const float*>(st + G::OFF_ES);
+        const float* sHs = reinterpret_cast<const float*>(st + G::OFF_HS);
+        const float* nH = reinterpret_cast<const float*>(smem + sn * G::STAGE);
+        float* xb = xch + (i & 1) * (G::XCH / 4);
+        constexpr int HC = G::HC, EC = G::EC;
+        const bool store = own_xy && i > 0;
+        const bool win = (narrow >> i) & 1u;
 
-      // ------------------------------------------------------------ E phase
-      // (after an expired wait the values are stale but in bounds; the vote
-      // below then ends the block before anything is stored)
-      const float hx_c = sH[hb], hy_c = sH[HC + hb], hz_c = sH[2 * HC + hb];
-      const float dhz_y = sH[2 * HC + hb + G::HW] - hz_c, dhy_z = nH[HC + hb] - hy_c;
-      const float dhx_z = nH[hb] - hx_c, dhz_x = sH[2 * HC + hb + 1] - hz_c;
-      const float dhy_x = sH[HC + hb + 1] - hy_c, dhx_y = sH[hb + G::HW] - hx_c;
-      const int id = ok ? int(sI[ib]) : 0;  // a stage that never arrived may hold any bits
-      if (i + 1 < npl) {
-        // the next plane's row into L1 while this plane computes
-        const int idn = reinterpret_cast<const uint16_t*>(smem + sn * G::STAGE + G::OFF_I)[ib];
-        if (ok && idn != id) prefetch_l1(rows + 8 * idn);
-      }
-      if (id != row_id) {
-        const float4* row = rows + 8 * id;
-        ra = __ldg(row); rb = __ldg(row + 1); rd = __ldg(row + 2); rp = __ldg(row + 3);
-        rq = __ldg(row + 4); ru = __ldg(row + 5); rv = __ldg(row + 6); r7 = __ldg(row + 7);
-        row_id = id;
-      }
-      const uint32_t flags = __float_as_uint(r7.z);
-      float ex, ey, ez;
-      if (!(flags & kESplit)) {
-        // both splits share Ca: f' = Ca f + Cb1 d1 + Cb2 d2
-        ex = upd_e(ra.x, sE[eb], ra.y, dhz_y, ra.w, dhy_z);
-        ey = upd_e(rb.x, sE[EC + eb], rb.y, dhx_z, rb.w, dhz_x);
-        ez = upd_e(rd.x, sE[2 * EC + eb], rd.y, dhy_x, rd.w, dhx_y);
-      } else {
-        // per component: the split pair (one 8-byte load at the selected
-        // offset) or the unsplit total
-        float2 sp[3];
-        const float2* sP = reinterpret_cast<const float2*>(sEs);
-#pragma unroll
-        for (int m = 0; m < 3; ++m) sp[m] = make_float2(0.f, 0.f);
-        if (flags & (kCompSplit0 << 0)) {
-          sp[0] = sP[win ? ebn : eb];
-          sp[0].x = upd_e_split(ra.x, sp[0].x, ra.y, dhz_y);  // ex_y
-          sp[0].y = upd_e_split(ra.z, sp[0].y, ra.w, dhy_z);  // ex_z
-        } else {
+        // ------------------------------------------------------------ E phase
+        // (after an expired wait the values are stale but in bounds; the vote
+        // below then ends the block before anything is stored)
+        const float hx_c = sH[hb], hy_c = sH[HC + hb], hz_c = sH[2 * HC + hb];
+        const float dhz_y = sH[2 * HC + hb + G::HW] - hz_c, dhy_z = nH[HC + hb] - hy_c;
+        const float dhx_z = nH[hb] - hx_c, dhz_x = sH[2 * HC + hb + 1] - hz_c;
+        const float dhy_x = sH[HC + hb + 1] - hy_c, dhx_y = sH[hb + G::HW] - hx_c;
+        const int id = ok ? int(sI[ib]) : 0;  // a stage that never arrived may hold any bits
+        if (i + 1 < npl) {
+          // the next plane's row into L1 while this plane computes
+          const int idn = reinterpret_cast<const uint16_t*>(smem + sn * G::STAGE + G::OFF_I)[ib];
+          if (ok && idn != id) prefetch_l1(rows + 8 * idn);
+        }
+        if (id != row_id) {
+          const float4* row = rows + 8 * id;
+          ra = __ldg(row); rb = __ldg(row + 1); rd = __ldg(row + 2); rp = __ldg(row + 3);
+          rq = __ldg(row + 4); ru = __ldg(row + 5); rv = __ldg(row + 6); r7 = __ldg(row + 7);
+          row_id = id;
+        }
+        const uint32_t flags = __float_as_uint(r7.z);
+        float ex, ey, ez;
+        if (FAST || !(flags & kESplit)) {
+          // both splits share Ca: f' = Ca f + Cb1 d1 + Cb2 d2
           ex = upd_e(ra.x, sE[eb], ra.y, dhz_y, ra.w, dhy_z);
-        }
-        if (flags & (kCompSplit0 << 1)) {
-          sp[1] = sP[win ? G::SECN + ebn : EC + eb];
-          sp[1].x = upd_e_split(rb.x, sp[1].x, rb.y, dhx_z);  // ey_z
-          sp[1].y = upd_e_split(rb.z, sp[1].y, rb.w, dhz_x);  // ey_x
-        } else {
           ey = upd_e(rb.x, sE[EC + eb], rb.y, dhx_z, rb.w, dhz_x);
-        }
-        if (flags & (kCompSplit0 << 2)) {
-          sp[2] = sP[win ? 2 * G::SECN + ebn : 2 * EC + eb];
-          sp[2].x = upd_e_split(rd.x, sp[2].x, rd.y, dhy_x);  // ez_x
-          sp[2].y = upd_e_split(rd.z, sp[2].y, rd.w, dhx_y);  // ez_y
-        } else {
           ez = upd_e(rd.x, sE[2 * EC + eb], rd.y, dhy_x, rd.w, dhx_y);
-        }
-        if (flags >> 16) stream_inject(Sd, r7, flags, n, true, sp);
-        if (flags & (kCompSplit0 << 0)) ex = __fadd_rn(sp[0].x, sp[0].y);
-        if (flags & (kCompSplit0 << 1)) ey = __fadd_rn(sp[1].x, sp[1].y);
-        if (flags & (kCompSplit0 << 2)) ez = __fadd_rn(sp[2].x, sp[2].y);
-        if (store) {
-#pragma unroll
-          for (int m = 0; m < 3; ++m)
-            if (flags & (kCompSplit0 << m)) spo[m * N + idx] = sp[m];
-        }
-      }
-      xb[w * 32 + lane] = ex;
-      xb[G::ER * 32 + w * 32 + lane] = ez;
-      const float ey_xm = __shfl_up_sync(0xffffffffu, ey, 1);
-      const float ez_xm = __shfl_up_sync(0xffffffffu, ez, 1);
-      // E^{n+1}(z) of the block complete; a consumer whose wait expired votes here
-      if (named_bar_or(kStreamBar, NC, !ok)) {
-        if (tid == 0) atomicExch(err, kStreamErrTimeout);
-        return;
-      }
-
-      // ------------------------------------------------------------ H phase
-      if (store) {
-        const float ex_ym = xb[(w - 1) * 32 + lane];
-        const float ez_ym = xb[G::ER * 32 + (w - 1) * 32 + lane];
-        // totals of the components not stored split
-        if (!(flags & (kCompSplit0 << 0))) fo[idx] = ex;
-        if (!(flags & (kCompSplit0 << 1))) fo[N + idx] = ey;
-        if (!(flags & (kCompSplit0 << 2))) fo[2 * N + idx] = ez;
-        // slots 12..29: (Da, Db1, Db2) of hx_y, hx_z, hy_z, hy_x, hz_x, hz_y
-        const float gxy = h_term(rp.z, ez, rp.y, ez_ym);
-        const float gxz = h_term(rq.y, ey, rq.x, ey_p);
-        const float gyz = h_term(ru.x, ex, rq.w, ex_p);
-        const float gyx = h_term(ru.w, ez, ru.z, ez_xm);
-        const float gzx = h_term(rv.z, ey, rv.y, ey_xm);
-        const float gzy = h_term(r7.y, ex, r7.x, ex_ym);
-        float hx, hy, hz;
-        if (!(flags & kHSplit)) {
-          hx = upd_h(rp.x, hx_c, gxy, gxz);
-          hy = upd_h(rq.z, hy_c, gyz, gyx);
-          hz = upd_h(rv.x, hz_c, gzx, gzy);
         } else {
+          // per component: the split pair (one 8-byte load at the selected
+          // offset) or the unsplit total
           float2 sp[3];
-          const float2* sP = reinterpret_cast<const float2*>(sHs);
-#pragma unroll
+          const float2* sP = reinterpret_cast<const float2*>(sEs);
+  #pragma unroll
           for (int m = 0; m < 3; ++m) sp[m] = make_float2(0.f, 0.f);
-          if (flags & (kCompSplit0 << 3)) {
-            sp[0] = sP[win ? sbn : sb];
-            sp[0].x = upd_h_split(rp.x, sp[0].x, gxy);
-            sp[0].y = upd_h_split(rp.w, sp[0].y, gxz);
+          if (flags & (kCompSplit0 << 0)) {
+            sp[0] = sP[win ? ebn : eb];
+            sp[0].x = upd_e_split(ra.x, sp[0].x, ra.y, dhz_y);  // ex_y
+            sp[0].y = upd_e_split(ra.z, sp[0].y, ra.w, dhy_z);  // ex_z
           } else {
+            ex = upd_e(ra.x, sE[eb], ra.y, dhz_y, ra.w, dhy_z);
+          }
+          if (flags & (kCompSplit0 << 1)) {
+            sp[1] = sP[win ? G::SECN + ebn : EC + eb];
+            sp[1].x = upd_e_split(rb.x, sp[1].x, rb.y, dhx_z);  // ey_z
+            sp[1].y = upd_e_split(rb.z, sp[1].y, rb.w, dhz_x);  // ey_x
+          } else {
+            ey = upd_e(rb.x, sE[EC + eb], rb.y, dhx_z, rb.w, dhz_x);
+          }
+          if (flags & (kCompSplit0 << 2)) {
+            sp[2] = sP[win ? 2 * G::SECN + ebn : 2 * EC + eb];
+            sp[2].x = upd_e_split(rd.x, sp[2].x, rd.y, dhy_x);  // ez_x
+            sp[2].y = upd_e_split(rd.z, sp[2].y, rd.w, dhx_y);  // ez_y
+          } else {
+            ez = upd_e(rd.x, sE[2 * EC + eb], rd.y, dhy_x, rd.w, dhx_y);
+          }
+          if (flags >> 16) stream_inject(Sd, r7, flags, n, true, sp);
+          if (flags & (kCompSplit0 << 0)) ex = __fadd_rn(sp[0].x, sp[0].y);
+          if (flags & (kCompSplit0 << 1)) ey = __fadd_rn(sp[1].x, sp[1].y);
+          if (flags & (kCompSplit0 << 2)) ez = __fadd_rn(sp[2].x, sp[2].y);
+          if (store) {
+  #pragma unroll
+            for (int m = 0; m < 3; ++m)
+              if (flags & (kCompSplit0 << m)) spo[m * N + idx] = sp[m];
+          }
+        }
+        xb[w * 32 + lane] = ex;
+        xb[G::ER * 32 + w * 32 + lane] = ez;
+        const float ey_xm = __shfl_up_sync(0xffffffffu, ey, 1);
+        const float ez_xm = __shfl_up_sync(0xffffffffu, ez, 1);
+        // E^{n+1}(z) of the block complete; a consumer whose wait expired votes here
+        if (named_bar_or(kStreamBar, NC, !ok)) {
+          if (tid == 0) atomicExch(err, kStreamErrTimeout);
+          return false;
+        }
+
+        // ------------------------------------------------------------ H phase
+        if (store) {
+          const float ex_ym = xb[(w - 1) * 32 + lane];
+          const float ez_ym = xb[G::ER * 32 + (w - 1) * 32 + lane];
+          // totals of the components not stored split
+          if (FAST || !(flags & (kCompSplit0 << 0))) fo[idx] = ex;
+          if (FAST || !(flags & (kCompSplit0 << 1))) fo[N + idx] = ey;
+          if (FAST || !(flags & (kCompSplit0 << 2))) fo[2 * N + idx] = ez;
+          // slots 12..29: (Da, Db1, Db2) of hx_y, hx_z, hy_z, hy_x, hz_x, hz_y
+          const float gxy = h_term(rp.z, ez, rp.y, ez_ym);
+          const float gxz = h_term(rq.y, ey, rq.x, ey_p);
+          const float gyz = h_term(ru.x, ex, rq.w, ex_p);
+          const float gyx = h_term(ru.w, ez, ru.z, ez_xm);
+          const float gzx = h_term(rv.z, ey, rv.y, ey_xm);
+          const float gzy = h_term(r7.y, ex, r7.x, ex_ym);
+          float hx, hy, hz;
+          if (FAST || !(flags & kHSplit)) {
             hx = upd_h(rp.x, hx_c, gxy, gxz);
-          }
-          if (flags & (kCompSplit0 << 4)) {
-            sp[1] = sP[win ? G::SHCN + sbn : G::SHC + sb];
-            sp[1].x = upd_h_split(rq.z, sp[1].x, gyz);
-            sp[1].y = upd_h_split(ru.y, sp[1].y, gyx);
-          } else {
             hy = upd_h(rq.z, hy_c, gyz, gyx);
-          }
-          if (flags & (kCompSplit0 << 5)) {
-            sp[2] = sP[win ? 2 * G::SHCN + sbn : 2 * G::SHC + sb];
-            sp[2].x = upd_h_split(rv.x, sp[2].x, gzx);
-            sp[2].y = upd_h_split(rv.w, sp[2].y, gzy);
-          } else {
             hz = upd_h(rv.x, hz_c, gzx, gzy);
+          } else {
+            float2 sp[3];
+            const float2* sP = reinterpret_cast<const float2*>(sHs);
+  #pragma unroll
+            for (int m = 0; m < 3; ++m) sp[m] = make_float2(0.f, 0.f);
+            if (flags & (kCompSplit0 << 3)) {
+              sp[0] = sP[win ? sbn : sb];
+              sp[0].x = upd_h_split(rp.x, sp[0].x, gxy);
+              sp[0].y = upd_h_split(rp.w, sp[0].y, gxz);
+            } else {
+              hx = upd_h(rp.x, hx_c, gxy, gxz);
+            }
+            if (flags & (kCompSplit0 << 4)) {
+              sp[1] = sP[win ? G::SHCN + sbn : G::SHC + sb];
+              sp[1].x = upd_h_split(rq.z, sp[1].x, gyz);
+              sp[1].y = upd_h_split(ru.y, sp[1].y, gyx);
+            } else {
+              hy = upd_h(rq.z, hy_c, gyz, gyx);
+            }
+            if (flags & (kCompSplit0 << 5)) {
+              sp[2] = sP[win ? 2 * G::SHCN + sbn : 2 * G::SHC + sb];
+              sp[2].x = upd_h_split(rv.x, sp[2].x, gzx);
+              sp[2].y = upd_h_split(rv.w, sp[2].y, gzy);
+            } else {
+              hz = upd_h(rv.x, hz_c, gzx, gzy);
+            }
+            if (flags >> 16) stream_inject(Sd, r7, flags, n, false, sp);
+            if (flags & (kCompSplit0 << 3)) hx = __fadd_rn(sp[0].x, sp[0].y);
+            if (flags & (kCompSplit0 << 4)) hy = __fadd_rn(sp[1].x, sp[1].y);
+            if (flags & (kCompSplit0 << 5)) hz = __fadd_rn(sp[2].x, sp[2].y);
+  #pragma unroll
+            for (int m = 0; m < 3; ++m)
+              if (flags & (kCompSplit0 << (3 + m))) spo[(3 + m) * N + idx] = sp[m];
           }
-          if (flags >> 16) stream_inject(Sd, r7, flags, n, false, sp);
-          if (flags & (kCompSplit0 << 3)) hx = __fadd_rn(sp[0].x, sp[0].y);
-          if (flags & (kCompSplit0 << 4)) hy = __fadd_rn(sp[1].x, sp[1].y);
-          if (flags & (kCompSplit0 << 5)) hz = __fadd_rn(sp[2].x, sp[2].y);
-#pragma unroll
-          for (int m = 0; m < 3; ++m)
-            if (flags & (kCompSplit0 << (3 + m))) spo[(3 + m) * N + idx] = sp[m];
-        }
-        fo[3 * N + idx] = hx;
-        fo[4 * N + idx] = hy;
-        fo[5 * N + idx] = hz;
-        const int np = int(flags >> 16);
-        if (np) {  // record the probes of this cell (solver.cu:467, 521)
-          const int first = __float_as_int(r7.w);
-          for (int e = 0; e < np; ++e) {
-            const int2 pe = __ldg(Sd.cell_probes + first + e);
-            const float val = pe.y == 0 ? ex : pe.y == 1 ? ey : pe.y == 2 ? ez : pe.y == 3 ? hx : pe.y == 4 ? hy : hz;
-            Sd.rec[(size_t)pe.x * Sd.nt + n] = val;
+          fo[3 * N + idx] = hx;
+          fo[4 * N + idx] = hy;
+          fo[5 * N + idx] = hz;
+          const int np = FAST ? 0 : int(flags >> 16);
+          if (np) {  // record the probes of this cell (solver.cu:467, 521)
+            const int first = __float_as_int(r7.w);
+            for (int e = 0; e < np; ++e) {
+              const int2 pe = __ldg(Sd.cell_probes + first + e);
+              const float val = pe.y == 0 ? ex : pe.y == 1 ? ey : pe.y == 2 ? ez : pe.y == 3 ? hx : pe.y == 4 ? hy : hz;
+              Sd.rec[(size_t)pe.x * Sd.nt + n] = val;
+            }
           }
         }
+        ex_p = ex;
+        ey_p = ey;
+        // plane z is no longer read by this warp
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&empty[sq]);
+        sq = sn;
+        pq = pn;
+        idx += plane;
       }
-      ex_p = ex;
-      ey_p = ey;
-      // plane z is no longer read by this warp
-      __syncwarp();
-      if (lane == 0) mbar_arrive(&empty[sq]);
-      sq = sn;
-      pq = pn;
-      idx += plane;
-    }
+      return true;
+    };
+    if (!(td.plain ? planes(std::true_type{}) : planes(std::false_type{}))) return;
     // the look-ahead plane z1 was read only by the last iteration
     __syncwarp();
     if (lane == 0) mbar_arrive(&empty[sq]);
