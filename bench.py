@@ -27,6 +27,7 @@ import argparse
 import copy
 import datetime
 import json
+import re
 import os
 import statistics
 import subprocess
@@ -245,13 +246,14 @@ def run_ours(args, rank, world, local_rank):
         mean_sim_ms = statistics.fmean(per_sim_ms)
         step_ms = mean_sim_ms / Nt  # one step-kernel launch per time step (+ the DFT every 256 steps)
         achieved = alg_bytes_step / (step_ms * 1e-3) / 1e9
+        # DRAM bytes of one step launch from the committed ncu summary of this
+        # workload (the line `traffic_bytes_per_launch (variant V): B`)
         traffic = None
-        tp = ROOT / "profiles" / "traffic.json"
+        tp = ROOT / "profiles" / "fdtd_step_stream_c2.md"
         if tp.exists():
-            tj = json.loads(tp.read_text())
-            key = f"variant{st['variant']}"
-            if key in tj:
-                traffic = tj[key]["bytes_per_launch"]
+            m = re.search(r"traffic_bytes_per_launch \(variant %d\): (\d+)" % st["variant"], tp.read_text())
+            if m:
+                traffic = int(m.group(1))
         value = world * cells * Nt * args.steps / (total_ms * 1e-3) / 1e6
         out = {
             "metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": world,

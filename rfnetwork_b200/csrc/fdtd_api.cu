@@ -58,16 +58,22 @@ struct ArgError {
 template <typename T>
 struct DevBuf {
   T* p = nullptr;
-  size_t n = 0;
+  size_t n = 0;    // elements in use
+  size_t cap = 0;  // elements allocated
   void alloc(size_t count) {
     free();
     if (count) CK(cudaMalloc(&p, count * sizeof(T)));
+    n = cap = count;
+  }
+  // Like alloc, but keeps the allocation when it already holds `count`.
+  void reserve(size_t count) {
+    if (count > cap) alloc(count);
     n = count;
   }
   void free() {
     if (p) cudaFree(p);
     p = nullptr;
-    n = 0;
+    n = cap = 0;
   }
   ~DevBuf() { free(); }
   DevBuf() = default;
@@ -610,6 +616,17 @@ struct Engine {
     cap_blocks = int(std::min<int64_t>(1024, std::max<int64_t>(1, (nb_max + 255) / 256)));
   }
 
+  // Adjoint work buffers of each request slot, kept between sweeps.
+  struct AdjBufs {
+    DevBuf<float> lam, lams, radj, seg;
+    DevBuf<int> pidx, pfld;
+    DevBuf<double> grad;
+  };
+  std::vector<std::unique_ptr<AdjBufs>> adj_bufs;
+  DevBuf<AdjSim> adj_d_as;
+  DevBuf<int4> adj_d_t;
+  DevBuf<CapSim> adj_d_c;
+
   static int adj_tiles_per_sm() {
     const char* v = std::getenv("RFN_ADJ_TILES_PER_SM");
     return v ? std::max(1, std::atoi(v)) : 4;
@@ -640,12 +657,9 @@ struct Engine {
     int dev = 0, n_sm = 148;
     CK(cudaGetDevice(&dev));
     CK(cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev));
-    struct Bufs {
-      DevBuf<float> lam, lams, radj, seg;
-      DevBuf<int> pidx, pfld;
-      DevBuf<double> grad;
-    };
-    std::vector<std::unique_ptr<Bufs>> bufs;
+    // work buffers are kept on the engine between sweeps (allocation and
+    // release of ~36 floats per cell would otherwise come with every gradient)
+    if (adj_bufs.size() < req.size()) adj_bufs.resize(req.size());
     std::vector<AdjSim> as(req.size());
     std::vector<CapSim> caps;
     int64_t nb_max = 0;
@@ -653,7 +667,8 @@ struct Engine {
     for (size_t i = 0; i < req.size(); ++i) {
       fdtd_sim* s = req[i].s;
       const int* box = req[i].box;
-      auto B = std::make_unique<Bufs>();
+      if (!adj_bufs[i]) adj_bufs[i] = std::make_unique<AdjBufs>();
+      AdjBufs* B = adj_bufs[i].get();
       const size_t N = s->cells_padded;
       const int64_t nb = box_cells(box);
       nb_max = std::max(nb_max, nb);
@@ -667,19 +682,19 @@ struct Engine {
         pidx[size_t(pr)] = z * s->ny * s->pitch + y * s->pitch + x;
         pfld[size_t(pr)] = s->probes[size_t(pr)].field;
       }
-      B->lam.alloc(12 * N);
+      B->lam.reserve(12 * N);
       CK(cudaMemsetAsync(B->lam.p, 0, 12 * N * sizeof(float), st));
       if (s->splits.n) {
-        B->lams.alloc(24 * N);
+        B->lams.reserve(24 * N);
         CK(cudaMemsetAsync(B->lams.p, 0, 24 * N * sizeof(float), st));
       }
-      B->radj.alloc(radj.size());
+      B->radj.reserve(radj.size());
       CK(cudaMemcpy(B->radj.p, radj.data(), radj.size() * sizeof(float), cudaMemcpyHostToDevice));
-      B->pidx.alloc(pidx.size());
+      B->pidx.reserve(pidx.size());
       CK(cudaMemcpy(B->pidx.p, pidx.data(), pidx.size() * sizeof(int), cudaMemcpyHostToDevice));
-      B->pfld.alloc(pfld.size());
+      B->pfld.reserve(pfld.size());
       CK(cudaMemcpy(B->pfld.p, pfld.data(), pfld.size() * sizeof(int), cudaMemcpyHostToDevice));
-      B->grad.alloc(9 * size_t(nb));
+      B->grad.reserve(9 * size_t(nb));
       CK(cudaMemsetAsync(B->grad.p, 0, 9 * size_t(nb) * sizeof(double), st));
       AdjSim& a = as[i];
       a = AdjSim{};
@@ -700,7 +715,7 @@ struct Engine {
       if (mode == 2) {
         a.hist = s->hist.p;
       } else {
-        B->seg.alloc(size_t(K) * 9 * size_t(nb));
+        B->seg.reserve(size_t(K) * 9 * size_t(nb));
         a.hist = B->seg.p;
         CapSim c{};
         c.s = s->dev;
@@ -709,18 +724,17 @@ struct Engine {
         c.hist = B->seg.p;
         caps.push_back(c);
       }
-      bufs.push_back(std::move(B));
     }
     const std::vector<int4> tiles = plain_tiles(n_sm, 0, nullptr, kAdjTileX, kAdjTileY, adj_tiles_per_sm());
-    DevBuf<AdjSim> d_as;
-    DevBuf<int4> d_t;
-    DevBuf<CapSim> d_c;
-    d_as.alloc(as.size());
+    DevBuf<AdjSim>& d_as = adj_d_as;
+    DevBuf<int4>& d_t = adj_d_t;
+    DevBuf<CapSim>& d_c = adj_d_c;
+    d_as.reserve(as.size());
     CK(cudaMemcpy(d_as.p, as.data(), as.size() * sizeof(AdjSim), cudaMemcpyHostToDevice));
-    d_t.alloc(tiles.size());
+    d_t.reserve(tiles.size());
     CK(cudaMemcpy(d_t.p, tiles.data(), tiles.size() * sizeof(int4), cudaMemcpyHostToDevice));
     if (!caps.empty()) {
-      d_c.alloc(caps.size());
+      d_c.reserve(caps.size());
       CK(cudaMemcpy(d_c.p, caps.data(), caps.size() * sizeof(CapSim), cudaMemcpyHostToDevice));
     }
     const int cap_grid = int(std::min<int64_t>(1024, std::max<int64_t>(1, (nb_max + 255) / 256)));
@@ -781,7 +795,8 @@ struct Engine {
     adj_ms = ms;
     check_error();
     for (size_t i = 0; i < req.size(); ++i)
-      CK(cudaMemcpy(req[i].grad_out, bufs[i]->grad.p, bufs[i]->grad.n * sizeof(double), cudaMemcpyDeviceToHost));
+      CK(cudaMemcpy(req[i].grad_out, adj_bufs[i]->grad.p, adj_bufs[i]->grad.n * sizeof(double),
+                    cudaMemcpyDeviceToHost));
   }
 
   // Enqueue one full run of nt steps on stream st (used for capture and for

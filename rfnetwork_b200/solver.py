@@ -174,6 +174,68 @@ class FDTD_Solver:
             idx += [np.argmax(diff >= -self._tol) if diff[-1] > -self._tol else len(g)]
         return tuple(idx)
 
+    def edge_correction(self, p1, p2, integration_line: str, CFe: float = None, CFh: float = 1):
+        """Analytic correction of the H updates next to a PEC edge (rfnetwork/solver.py:2534-2700).
+
+        The fields near a thin conductor edge vary like 1/sqrt(distance), which
+        the Yee cell integrals miss. Along the edge p1-p2 (parallel to one
+        axis; ``integration_line`` the in-plane direction pointing away from the
+        conductor) the H integration coefficients Db of the affected cells are
+        scaled by CFe (default sqrt(2)) or 1/CFe, in the reference's order, so
+        the packed coefficients match it bit for bit. CFh is accepted and, as in
+        the reference, unused.
+        """
+        self.invalidate_solution()
+        self.check_mesh()
+        cf = 2 * np.sqrt(1 / 2) if CFe is None else CFe
+        p1, p2 = np.array(p1), np.array(p2)
+        length = np.abs(p2 - p1)
+        if np.count_nonzero(length) != 1:
+            raise NotImplementedError("Edge correction is only supported for edges along the cartesian axis.")
+        ax_e = int(np.argmax(length))
+        ax_f = dict(x=0, y=1, z=2)[integration_line[0]]
+        outward = {"+": 1, "-": 0}[integration_line[1]]
+        if ax_e == ax_f:
+            raise ValueError("Integration axis must be perpendicular to the edge.")
+        if p1[ax_e] > p2[ax_e]:
+            p1, p2 = p2, p1
+        i1, i2 = self.pos_to_idx(p1, mode="edge"), self.pos_to_idx(p2, mode="edge")
+        ax_n = 3 - ax_e - ax_f
+        e, f, nrm = ("x", "y", "z")[ax_e], ("x", "y", "z")[ax_f], ("x", "y", "z")[ax_n]
+        Db = self.Db
+
+        def at(along_edge, along_field, along_normal):
+            sl = [None, None, None]
+            sl[ax_e], sl[ax_f], sl[ax_n] = along_edge, along_field, along_normal
+            return tuple(sl)
+
+        centres = slice(i1[ax_e], i2[ax_e])      # components centred between edge nodes
+        nodes = slice(i1[ax_e], i2[ax_e] + 1)    # components on the edge nodes
+        h_f = i1[ax_f] if outward else i1[ax_f] - 1
+        k_n = i1[ax_n]
+        # the normal H in the conductor plane that integrates the field-axis E:
+        # scaled down over the edge, up at the two ends
+        Db[f"h{nrm}_{f}2"][at(centres, h_f, k_n)] *= 1 / cf
+        Db[f"h{nrm}_{f}1"][at(centres, h_f, k_n)] *= 1 / cf
+        if i1[ax_e] > 0:
+            Db[f"h{nrm}_{e}2"][at(i1[ax_e] - 1, h_f, k_n)] *= cf
+        if i2[ax_e] < Db[f"h{nrm}_{e}1"].shape[ax_e]:
+            Db[f"h{nrm}_{e}1"][at(i2[ax_e], h_f, k_n)] *= cf
+        # the edge-parallel H just below and above the conductor plane
+        Db[f"h{e}_{nrm}2"][at(nodes, h_f, k_n - 1)] *= cf
+        Db[f"h{e}_{nrm}1"][at(nodes, h_f, k_n)] *= cf
+        for k in (k_n - 1, k_n):
+            # edge-parallel H on both sides of the normal E under the edge
+            Db[f"h{e}_{f}2"][at(nodes, i1[ax_f] - 1, k)] *= cf
+            Db[f"h{e}_{f}1"][at(nodes, i1[ax_f], k)] *= cf
+            # field-axis H that integrates the normal E below and above the edge
+            Db[f"h{f}_{nrm}1"][at(centres, i1[ax_f], k)] *= 1 / cf
+            Db[f"h{f}_{nrm}2"][at(centres, i1[ax_f], k)] *= 1 / cf
+            if i1[ax_e] > 0:
+                Db[f"h{f}_{e}2"][at(i1[ax_e] - 1, i1[ax_f], k)] *= cf
+            if i2[ax_e] < Db[f"h{f}_{e}1"].shape[ax_e]:
+                Db[f"h{f}_{e}1"][at(i2[ax_e], i1[ax_f], k)] *= cf
+
     def field_pos_to_idx(self, position, field):
         """Index of the ``field`` component on or just past ``position`` (solver.py:404-420)."""
         self.check_mesh()

@@ -9,7 +9,8 @@ packing. The reference's third-party imports that are absent here
 minimal stand-ins:
   * pyvista objects carry only ``points`` / ``n_cells`` / ``faces`` / ``bounds``;
   * ``_create_grid`` (the mesher, out of scope) is replaced by explicit grid
-    edges: uniform (setup_small.npz) or graded (setup_graded.npz);
+    edges: uniform (setup_small.npz, and setup_edge.npz, which adds the PEC
+    edge corrections of the trace) or graded (setup_graded.npz);
   * the conductor inclusion tests use axis-aligned box / rectangle
     containment (``utils_mesh.is_point_in_surface`` and pyvista's implicit
     distance are geometry code, not coefficient math).
@@ -17,7 +18,7 @@ Everything else -- grid arrays, material averaging, coefficients, PML,
 conductors, lumped ports, probes, monitors, sources and packing -- is the
 reference code itself. The fixture pins ``rfnetwork_b200.solver`` bit-exactly.
 
-Usage:  python tests/golden/make_setup_golden.py [setup_small.npz] [setup_graded.npz]
+Usage:  python tests/golden/make_setup_golden.py [setup_small.npz] [setup_graded.npz] [setup_edge.npz]
         (needs the reference checkout; writes the named fixtures, default both)
 """
 from __future__ import annotations
@@ -159,7 +160,23 @@ def grid_edges_graded():
     return tuple(np.around(np.array(g), 5) for g in (gx, gy, gz))
 
 
-FIXTURES = {"setup_small.npz": grid_edges, "setup_graded.npz": grid_edges_graded}
+# PEC edge corrections on the trace (rfnetwork/solver.py:2534-2700): both long
+# edges along x, pointing away from the strip in the substrate plane, and the
+# far end of the strip along y
+TRACE_EDGES = [((0.03, 0.05, 0.02), (0.13, 0.05, 0.02), "y-"),
+               ((0.13, 0.07, 0.02), (0.03, 0.07, 0.02), "y+"),
+               ((0.13, 0.05, 0.02), (0.13, 0.07, 0.02), "x+")]
+
+
+def with_edge_corrections(s):
+    for p1, p2, line in TRACE_EDGES:
+        s.edge_correction(p1, p2, line)
+    return s
+
+
+FIXTURES = {"setup_small.npz": grid_edges, "setup_graded.npz": grid_edges_graded, "setup_edge.npz": grid_edges}
+# applied to the built and meshed model before it is solved
+POST_BUILD = {"setup_edge.npz": with_edge_corrections}
 
 
 def main(names):
@@ -181,6 +198,7 @@ def generate(name, edges):
         s.generate_mesh(d_max=0.01)
 
     s = build_model(ref.FDTD_Solver, geo.Box, geo.Rectangle, geo.Line, edges, explicit_mesh)
+    POST_BUILD.get(name, lambda m: m)(s)
     s.solve(n_threads=2, show_progress=False, gpu=False)
     s.solve(n_threads=2, show_progress=False, gpu=True)
 

@@ -86,6 +86,42 @@ def test_kernel_arithmetic_model_matches_oracle(engine_lib, oracle_lib, small):
     assert rel_l2(rec, ref) < 1e-6
 
 
+def test_kernel_arithmetic_model_edge_corrected(engine_lib, oracle_lib):
+    """PEC edge corrections (H rows with Db1 != Db2 next to the trace edges,
+    pinned to the reference by setup_edge.npz) through the material table."""
+    s = mg.with_edge_corrections(mg.build_model(S.FDTD_Solver, geo.Box, geo.Rectangle, geo.Line, mg.grid_edges(),
+                                                lambda m, e: m.generate_mesh(grid=e)))
+    ids, rows, pr, Nt = _table(s)
+    src = np.array([p["values"] for p in pr])
+    rec = km.run_model(ids, rows, None, km.shifted_probes(pr), src, Nt)
+    _, ref = run_oracle(s)
+    assert rel_l2(rec, ref) < 1e-6
+
+
+def test_component_split_flags(engine_lib):
+    """Bit 8 + c of a row marks component c (ex ey ez hx hy hz) stored as its
+    split pair: exactly where its two decays differ (or it carries a source)."""
+    s = configs.microstrip(n=(24, 24, 20), n_pml=4, nt=10)
+    co, pr, mo, mem, Nx, Ny, Nz, Nt = s.pack_inputs(gpu=True)
+    sim = _lib.Simulation(Nx, Ny, Nz)
+    sim.set_coefficients(co)
+    ids, rows = sim.material_table()
+    flags = rows[:, 30][ids]
+    pairs = (("Ca_ex_y", "Ca_ex_z"), ("Ca_ey_z", "Ca_ey_x"), ("Ca_ez_x", "Ca_ez_y"),
+             ("Da_hx_y", "Da_hx_z"), ("Da_hy_z", "Da_hy_x"), ("Da_hz_x", "Da_hz_y"))
+    inner = (slice(0, -1), slice(0, -1), slice(0, -1))   # away from the zeroed / guarded planes
+    for c, (a, b) in enumerate(pairs):
+        split = (flags & (1 << (8 + c))) != 0
+        assert np.array_equal(split[inner], (co[a] != co[b])[inner]), a
+    # a cell of the z-PML slab away from the x and y slabs: ez and hz decay alike
+    f = int(flags[Nx // 2, Ny // 2, 1])
+    assert f & (1 << 8) and f & (1 << 9) and not f & (1 << 10)
+    assert f & (1 << 11) and f & (1 << 12) and not f & (1 << 13)
+    # the any-component bits follow
+    assert np.array_equal((flags & 1) != 0, (flags & (7 << 8)) != 0)
+    assert np.array_equal((flags & 2) != 0, (flags & (7 << 11)) != 0)
+
+
 def test_split_flags_cover_pml(engine_lib):
     s = configs.microstrip(n=(24, 24, 20), n_pml=4, nt=10)
     co, pr, mo, mem, Nx, Ny, Nz, Nt = s.pack_inputs(gpu=True)

@@ -48,6 +48,17 @@ def test_small_model_probes(engine_lib, oracle_lib, small):
     _compare_series(se, so, 1e-5)
 
 
+def test_edge_corrected_model(engine_lib, oracle_lib):
+    """The small model with PEC edge corrections on the trace (per-cell H rows
+    with Db1 != Db2), whose setup tests/golden/setup_edge.npz pins."""
+    edge = mg.with_edge_corrections(mg.build_model(S.FDTD_Solver, geo.Box, geo.Rectangle, geo.Line,
+                                                   mg.grid_edges(), lambda s, e: s.generate_mesh(grid=e)))
+    se, pe = run_engine(edge)
+    so, po = run_oracle(edge)
+    assert rel_l2(pe, po) <= 1e-5
+    _compare_series(se, so, 1e-5)
+
+
 def test_graded_grid_model(engine_lib, oracle_lib):
     """The same model on a non-uniform grid (cells of 0.005 to 0.02 in), whose
     setup is pinned to the reference by tests/golden/setup_graded.npz."""

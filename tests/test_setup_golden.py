@@ -1,7 +1,7 @@
 """The setup API reproduces the reference's own setup code bit for bit.
 
-tests/golden/setup_small.npz (uniform grid) and setup_graded.npz (non-uniform
-grid) hold what rfnetwork/solver.py's solve() passed to the engine
+tests/golden/setup_small.npz (uniform grid), setup_graded.npz (non-uniform
+grid) and setup_edge.npz (uniform grid with PEC edge corrections) hold what rfnetwork/solver.py's solve() passed to the engine
 (coefficient dicts for both packings, probe and monitor lists, port records)
 for the model in make_setup_golden.build_model, generated by running the
 reference's Python code (see make_setup_golden.py).
@@ -19,6 +19,7 @@ def case(request):
     gold = np.load(mg.HERE / request.param)
     model = mg.build_model(S.FDTD_Solver, geo.Box, geo.Rectangle, geo.Line, mg.FIXTURES[request.param](),
                            lambda s, e: s.generate_mesh(grid=e))
+    mg.POST_BUILD.get(request.param, lambda m: m)(model)
     return model, gold
 
 
