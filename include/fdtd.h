@@ -78,6 +78,13 @@ int fdtd_create(int nx, int ny, int nz, fdtd_sim** out);
  * solver_init_fields does (rfnetwork/core/src/solver.cpp:294-328). */
 int fdtd_set_coefficient(fdtd_sim* s, const char* name, const float* data, int nx, int ny, int nz);
 
+/* As fdtd_set_coefficient, but the array is borrowed, not copied, as the
+ * reference's solver_init_fields borrows the numpy arrays it is given
+ * (rfnetwork/core/src/solver.cpp:80-117): `data` must stay valid and
+ * unchanged until the simulation is destroyed or the coefficient is set
+ * again. fdtd_set_box_coefficients copies a borrowed array before writing. */
+int fdtd_set_coefficient_view(fdtd_sim* s, const char* name, const float* data, int nx, int ny, int nz);
+
 /* Add a probe (solver_init_probes, rfnetwork/core/src/solver.cpp:465-532).
  * values: n_values >= nt floats, the soft-source amplitude per time step when
  * is_source is nonzero (copied). The recorded field series is read back with

@@ -18,7 +18,7 @@ EXPORTED = (
     "fdtd_create", "fdtd_set_coefficient", "fdtd_add_probe", "fdtd_add_monitor", "fdtd_set_dft",
     "fdtd_compile", "fdtd_get_material_table",
     "fdtd_run", "fdtd_run_async", "fdtd_synchronize", "fdtd_set_stream", "fdtd_get_probe_values",
-    "fdtd_set_kernel", "fdtd_batch_set_kernel",
+    "fdtd_set_kernel", "fdtd_batch_set_kernel", "fdtd_set_coefficient_view",
     "fdtd_get_dft", "fdtd_get_monitor", "fdtd_get_stats", "fdtd_last_error", "fdtd_destroy",
     "fdtd_batch_create", "fdtd_batch_run", "fdtd_batch_set_stream", "fdtd_batch_get_stats",
     "fdtd_batch_last_error", "fdtd_batch_destroy", "fdtd_global_error", "fdtd_step_noalloc",
@@ -66,6 +66,7 @@ def load():
     sig = {
         "fdtd_create": ([ip, ip, ip, pp], ip),
         "fdtd_set_coefficient": ([vp, ctypes.c_char_p, vp, ip, ip, ip], ip),
+        "fdtd_set_coefficient_view": ([vp, ctypes.c_char_p, vp, ip, ip, ip], ip),
         "fdtd_add_probe": ([vp, ip, ip, ip, ip, ip, vp, ip, ctypes.POINTER(ip)], ip),
         "fdtd_add_monitor": ([vp, ip, ip, ip, ip, ip, vp, ip, ctypes.POINTER(ip)], ip),
         "fdtd_set_dft": ([vp, ip, ip, vp, vp, vp, ip, vp], ip),
@@ -143,6 +144,7 @@ class Simulation:
         self.n_freq = 0
         self.monitors = []
         self.nt = None
+        self._borrowed = {}   # arrays lent to the engine by set_coefficient(borrow=True)
 
     def _check(self, rc):
         if rc:
@@ -151,15 +153,22 @@ class Simulation:
                 raise ValueError(msg)
             raise FdtdError(f"{FDTD_ERRORS.get(rc, rc)}: {msg}")
 
-    def set_coefficient(self, name: str, arr: np.ndarray):
+    def set_coefficient(self, name: str, arr: np.ndarray, borrow: bool = False):
+        """Copy the array into the engine, or with ``borrow`` lend it (no copy):
+        the simulation then keeps a reference to it until it is closed."""
         a = np.ascontiguousarray(arr, dtype=np.float32)
         if a.ndim != 3:
             raise ValueError("Invalid data array. Wrong number of dimensions.")
-        self._check(self.lib.fdtd_set_coefficient(self.h, name.encode(), _ptr(a), *a.shape))
+        if borrow:
+            self._check(self.lib.fdtd_set_coefficient_view(self.h, name.encode(), _ptr(a), *a.shape))
+            self._borrowed[name] = a
+        else:
+            self._check(self.lib.fdtd_set_coefficient(self.h, name.encode(), _ptr(a), *a.shape))
+            self._borrowed.pop(name, None)
 
-    def set_coefficients(self, coefficients: dict):
+    def set_coefficients(self, coefficients: dict, borrow: bool = False):
         for k, v in coefficients.items():
-            self.set_coefficient(k, v)
+            self.set_coefficient(k, v, borrow)
 
     def add_probe(self, field: int, idx, is_source: bool = False, values=None) -> int:
         out = ctypes.c_int()

@@ -19,6 +19,7 @@
 #include <mutex>
 #include <string>
 #include <thread>
+#include <unordered_set>
 #include <vector>
 
 #include "../../include/fdtd.h"
@@ -129,6 +130,8 @@ struct Engine;
 struct fdtd_sim {
   int nx, ny, nz;
   std::vector<float> coef[kNumCoef];
+  // borrowed caller arrays (fdtd_set_coefficient_view); null: coef[i] holds a copy
+  const float* coef_view[kNumCoef] = {};
   bool have_coef[kNumCoef] = {};
   std::vector<ProbeSpec> probes;
   std::vector<std::vector<float>> probe_values;
@@ -510,7 +513,13 @@ struct Engine {
       c.host_maps.emplace_back();
       encode_stream_maps(c.host_maps.back(), s, ty);
       const GradedIndex split_idx(s->grid, kFlagESplit | kFlagHSplit);
-      const GradedIndex probe_idx(s->grid, 0xFFFF0000u);  // cells with probe entries
+      // tiles (x / 31, y / TY, z / zchunk) that own a probe cell
+      std::unordered_set<int64_t> probe_tiles;
+      const int ntx = (s->nx + kStreamOwnX - 1) / kStreamOwnX, nty = (s->ny + ty - 1) / ty;
+      for (const int64_t cell : s->grid.probe_cell) {
+        const int z = int(cell % s->nz), y = int((cell / s->nz) % s->ny), x = int(cell / (int64_t(s->nz) * s->ny));
+        probe_tiles.insert((int64_t(z / zc) * nty + y / ty) * ntx + x / kStreamOwnX);
+      }
       for (int z0 = 0; z0 < s->nz; z0 += zc)
         for (int y0 = 0; y0 < s->ny; y0 += ty)
           for (int x0 = 0; x0 < s->nx; x0 += kStreamOwnX) {
@@ -542,7 +551,8 @@ struct Engine {
             t.z0 = z0;
             t.z1 = z1;
             t.wx0 = std::max(wx0, 0);
-            t.plain = mask == 0 && probe_idx.count(x0, x0 + kStreamOwnX, y0, y0 + ty, z0, z1) == 0;
+            t.plain = mask == 0 &&
+                      !probe_tiles.count((int64_t(z0 / zc) * nty + y0 / ty) * ntx + x0 / kStreamOwnX);
             t.split_lo = uint32_t(mask);
             t.split_hi = uint32_t(mask >> 32);
             t.narrow_lo = uint32_t(narrow);
@@ -920,7 +930,7 @@ void compile_host(fdtd_sim* s) {
   for (int i = 0; i < kNumCoef; ++i)
     if (!s->have_coef[i]) throw ArgError{FDTD_ERR_STATE, std::string("Coefficient not set: ") + kCoefNames[i]};
   const float* cp[kNumCoef];
-  for (int i = 0; i < kNumCoef; ++i) cp[i] = s->coef[i].data();
+  for (int i = 0; i < kNumCoef; ++i) cp[i] = s->coef_view[i] ? s->coef_view[i] : s->coef[i].data();
   std::string err;
   if (!compile_grid(s->nx, s->ny, s->nz, cp, s->probes, threads_for_host(), s->grid, err))
     throw ArgError{FDTD_ERR_LIMIT, err};
@@ -1178,6 +1188,14 @@ void set_box_coefficients(fdtd_sim* s, const int* box, const float* coefs) {
         throw ArgError{FDTD_ERR_STATE, std::string("Coefficient not set: ") + names[c][k]};
     }
   if (s->compiled) check_gradient_box(s, box);
+  for (int c = 0; c < 3; ++c)  // the patch writes the host arrays: copy borrowed ones first
+    for (int k = 0; k < 4; ++k) {
+      const int i = ci[c][k];
+      if (s->coef_view[i]) {
+        s->coef[i].assign(s->coef_view[i], s->coef_view[i] + size_t(s->nx) * s->ny * s->nz);
+        s->coef_view[i] = nullptr;
+      }
+    }
   const int bny = box[3] - box[2], bnz = box[5] - box[4];
   const int64_t nb = box_cells(box);
   auto cell_of = [&](int64_t bi) {
@@ -1299,6 +1317,26 @@ int fdtd_set_coefficient(fdtd_sim* s, const char* name, const float* data, int n
                                          std::to_string(a) + " of " + std::to_string(expect[a])};
     if (!data) throw ArgError{FDTD_ERR_ARG, "null coefficient data"};
     s->coef[i].assign(data, data + size_t(nx) * ny * nz);
+    s->coef_view[i] = nullptr;
+    s->have_coef[i] = true;
+    s->prepared = false;
+    s->compiled = false;
+  });
+}
+
+int fdtd_set_coefficient_view(fdtd_sim* s, const char* name, const float* data, int nx, int ny, int nz) {
+  if (!s) return FDTD_ERR_ARG;
+  return guarded(&s->err, [&] {
+    const int i = name ? coef_index(name) : -1;
+    if (i < 0) throw ArgError{FDTD_ERR_ARG, std::string("Unknown coefficient array ") + (name ? name : "(null)")};
+    const int expect[3] = {s->nx, s->ny, s->nz}, got[3] = {nx, ny, nz};
+    for (int a = 0; a < 3; ++a)
+      if (expect[a] != got[a])
+        throw ArgError{FDTD_ERR_ARG, std::string("Invalid data array ") + name + ". Expected shape on axis " +
+                                         std::to_string(a) + " of " + std::to_string(expect[a])};
+    if (!data) throw ArgError{FDTD_ERR_ARG, "null coefficient data"};
+    std::vector<float>().swap(s->coef[i]);
+    s->coef_view[i] = data;
     s->have_coef[i] = true;
     s->prepared = false;
     s->compiled = false;

@@ -92,7 +92,9 @@ def _run(coefficients, probes, monitors, Nx, Ny, Nz, Nt, terms=None, omega=None)
     X = None
     try:
         for name in COEFF_NAMES:
-            sim.set_coefficient(name, coefficients[name])
+            # borrowed, as the reference's engine borrows the numpy arrays (solver.cpp:80-117);
+            # they outlive the simulation, which is closed before this call returns
+            sim.set_coefficient(name, coefficients[name], borrow=True)
         for p in probes:
             src = bool(int(p.get("is_source", 0)))
             sim.add_probe(int(p["field"]), p["idx"], src, p["values"][:Nt] if src else None)

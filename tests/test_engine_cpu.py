@@ -138,3 +138,27 @@ def test_split_flags_cover_pml(engine_lib):
         assert not np.any(diff & ~esplit), a
     # the deep interior is unsplit
     assert not esplit[8:-8, 8:-8, 8:-8].any()
+
+
+def test_borrowed_coefficients(engine_lib, small):
+    """fdtd_set_coefficient_view lends the arrays: the same table as copies,
+    and the box patch copies a borrowed array before writing to it."""
+    co, pr, mo, mem, Nx, Ny, Nz, Nt = small.pack_inputs(gpu=True)
+    a = _lib.Simulation(Nx, Ny, Nz)
+    a.set_coefficients(co)
+    lent = {k: v.copy() for k, v in co.items()}
+    b = _lib.Simulation(Nx, Ny, Nz)
+    b.set_coefficients(lent, borrow=True)
+    ids_a, rows_a = a.material_table()
+    ids_b, rows_b = b.material_table()
+    assert np.array_equal(ids_a, ids_b) and np.array_equal(rows_a, rows_b)
+    box = (4, 6, 5, 7, 3, 5)
+    before = {k: v.copy() for k, v in lent.items()}
+    b.set_box_coefficients(box, np.full((3, 3, 2, 2, 2), 0.5))
+    for k in lent:
+        assert np.array_equal(lent[k], before[k]), k
+    ids_p, rows_p = b.material_table()
+    x, y, z = 4, 5, 3
+    assert rows_p[ids_p[x, y, z], 0].view(np.float32) == np.float32(0.5)
+    a.close()
+    b.close()
