@@ -161,6 +161,47 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+# ------------------------------------------------------------------- ranks
+
+class RankSync:
+    """Barrier and max-over-ranks of one process per GPU (torchrun env).
+
+    With world > 1 it joins the process group (NCCL on GPUs; gloo for the
+    CPU tests of this logic) with a short timeout, so ranks that wait on a
+    missing peer fail instead of hanging. With world == 1 it does nothing.
+    Every rank must make the same calls in the same order."""
+
+    def __init__(self, world: int, local_rank: int = 0, backend: str = "nccl", timeout_s: int = 600):
+        import torch
+        self.torch = torch
+        self.dist = None
+        self.cuda = backend == "nccl"
+        if world > 1:
+            import torch.distributed as dist
+            kw = {"device_id": torch.device("cuda", local_rank)} if self.cuda else {}
+            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=timeout_s), **kw)
+            self.dist = dist
+
+    def barrier(self):
+        if self.dist is not None:
+            self.dist.barrier()
+        if self.cuda:
+            self.torch.cuda.synchronize()
+
+    def max(self, v: float) -> float:
+        if self.dist is None:
+            return v
+        t = self.torch.tensor([v], dtype=self.torch.float64, device="cuda" if self.cuda else "cpu")
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def close(self):
+        if self.dist is not None:
+            self.dist.barrier()
+            self.dist.destroy_process_group()
+            self.dist = None
+
+
 # ---------------------------------------------------------------- our arm
 
 def run_ours(args, rank, world, local_rank):
@@ -168,23 +209,8 @@ def run_ours(args, rank, world, local_rank):
     from rfnetwork_b200 import _lib, configs, cuda_func
 
     torch.cuda.set_device(local_rank)
-    dist = None
-    if world > 1:
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
-                                device_id=torch.device("cuda", local_rank))
-
-    def barrier():
-        if dist is not None:
-            dist.barrier()
-        torch.cuda.synchronize()
-
-    def max_over_ranks(v: float) -> float:
-        if dist is None:
-            return v
-        t = torch.tensor([v], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    ranks = RankSync(world, local_rank)
+    barrier, max_over_ranks = ranks.barrier, ranks.max
 
     nt = args.nt
     s = build_model(nt)
@@ -284,9 +310,7 @@ def run_ours(args, rank, world, local_rank):
             "clocks": clk.summary(),
             "finite": finite,
         }
-    if dist is not None:
-        dist.barrier()
-        dist.destroy_process_group()
+    ranks.close()
     return out
 
 
@@ -367,6 +391,7 @@ def run_batch(args, rank, world, local_rank):
     from rfnetwork_b200 import _lib, configs
 
     torch.cuda.set_device(local_rank)
+    ranks = RankSync(world, local_rank)
     nt = args.nt if args.nt != NT else BATCH_NT
     sims, cells = [], 0
     for i in range(BATCH_SIMS):
@@ -418,9 +443,11 @@ def run_batch(args, rank, world, local_rank):
     batch.close()
     for s in sims:
         s.close()
+    # each rank runs its own copy: the job takes as long as the slowest rank
+    ms_b, ms_s, ms_p = (ranks.max(statistics.fmean(t)) for t in (t_batch, t_seq, t_plain))
+    ranks.close()
     if rank != 0:
         return None
-    ms_b, ms_s, ms_p = statistics.fmean(t_batch), statistics.fmean(t_seq), statistics.fmean(t_plain)
     return {
         "metric": "batched sims/s", "value": round(world * BATCH_SIMS / (ms_b * 1e-3), 3), "unit": "sims/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_b, 2),
@@ -457,6 +484,7 @@ def run_adjoint(args, rank, world, local_rank):
     from rfnetwork_b200.adjoint import FDTDDesign
 
     torch.cuda.set_device(local_rank)
+    ranks = RankSync(world, local_rank)
     nt = args.nt if args.nt != NT else 4000
     s = configs.microstrip(n=(128, 128, 96), n_pml=10, nt=nt)
     co, pr, *_ = s.pack_inputs(gpu=True)
@@ -495,7 +523,7 @@ def run_adjoint(args, rank, world, local_rank):
             plain_dev.append(design.sim.stats()["last_run_ms"] / 1e3)
         st = design.sim.stats()
         design.close()
-        tg, tf = statistics.fmean(t_grad), statistics.fmean(t_fwd)
+        tg, tf = ranks.max(statistics.fmean(t_grad)), ranks.max(statistics.fmean(t_fwd))
         dev_grad = statistics.fmean(fwd_dev) + statistics.fmean(adj_dev)
         dev_plain = statistics.fmean(plain_dev)
         return {
@@ -510,6 +538,7 @@ def run_adjoint(args, rank, world, local_rank):
 
     ck = measure(FDTDDesign(s, box, [(0, len(pr) - 1, 1.0)], omega, checkpoint_every=64))
     rec = measure(FDTDDesign(s, box, [(0, len(pr) - 1, 1.0)], omega))
+    ranks.close()
     if rank != 0:
         return None
     return {
@@ -540,6 +569,7 @@ def run_design(args, rank, world, local_rank):
     from rfnetwork_b200.adjoint import FDTDDesignBatch
 
     torch.cuda.set_device(local_rank)
+    ranks = RankSync(world, local_rank)
     nt = args.nt if args.nt != NT else 3000
     n_var = 32
     s = configs.microstrip(n=(96, 96, 64), n_pml=10, nt=nt)
@@ -579,9 +609,10 @@ def run_design(args, rank, world, local_rank):
         adj_ms.append(st["adjoint_ms"])
     st = designs.batch.stats()
     designs.close()
+    ts = ranks.max(statistics.fmean(t))   # wall time of the slowest rank
+    ranks.close()
     if rank != 0:
         return None
-    ts = statistics.fmean(t)
     cells = 96 * 96 * 64
     return {
         "metric": "grad evals/s", "value": round(world * n_var / ts, 3), "unit": "gradient evaluations/s",
