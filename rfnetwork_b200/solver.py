@@ -706,6 +706,27 @@ class FDTD_Solver:
         _lib.nf2ff(J_xyz, M_xyz, r_grid, ds_grid, surf_pos, ff_data)
         return ff_data["data"]
 
+    def get_farfield_gain(self, theta, phi, polarization=None) -> np.ndarray:
+        """Realized gain [polarization, frequency, theta, phi] from the far-field
+        monitor (rfnetwork/solver.py:2804-2868): the far field projected on each
+        polarization ("thetapol", "phipol", "rhcp", "lhcp"; default the first
+        two), radiation intensity |rE|^2 / (2 eta0), over the power the port
+        sources deliver into 50 ohm, |DTFT(v_src)|^2 / 100 summed over sources,
+        times 4 pi."""
+        rE = self.get_farfield_rE(theta, phi)
+        if polarization is None:
+            polarization = ["thetapol", "phipol"]
+        s2 = 1 / np.sqrt(2)
+        basis = dict(thetapol=[1, 0], phipol=[0, 1], rhcp=[s2, 1j * s2], lhcp=[s2, -1j * s2])
+        proj = np.array([basis[k] for k in polarization])
+        rE_pol = np.einsum("ij, j...->i...", proj, rE)
+        frequency = self.farfield["frequency"]
+        sources = [p["src"] for p in self.ports if p["src"] is not None]
+        Vs = np.array([dtft(v, frequency, 1 / self.dt, downsample=False) for v in sources])
+        p_in = np.sum((1 / 2) * (np.abs(Vs) ** 2 / 50), axis=0)
+        U = (1 / (2 * const.eta0)) * np.abs(rE_pol) ** 2
+        return (4 * np.pi / p_in[None, :, None, None]) * U
+
     def add_current_probe(self, name: str, face):
         """Ampere-loop H probes around a rectangle (rfnetwork/solver.py:1893-2010)."""
         dx_h, dy_h, dz_h = [conv.m_in(d) for d in self.dh_cells]
@@ -1092,6 +1113,35 @@ class FDTD_Solver:
         Bp = (Vp - r0 * Ip) / 2
         S = Bp / Ap[source_port - 1][None]
         return S.T[..., None]
+
+    def get_total_monitor_data(self, name: str):
+        """The three E components of an "e_total" monitor at common points of the
+        monitor plane (rfnetwork/solver.py:2750-2802): each in-plane component
+        averaged over its two neighbours along itself, the samples on the plane's
+        edges dropped. Returns ``(values [3 (x, y, z), time, n1, n2], coords)``."""
+        names = [f"{name}_{a}" for a in ("x", "y", "z")]
+        if not all(n in self.monitors for n in names):
+            raise ValueError(f"Monitor {name} does not contain data for all three field components.")
+        m0 = self.monitors[names[0]]
+        if m0["frequency"] is not None:
+            raise NotImplementedError("Phasor monitors not implemented yet for total fields.")
+        axis = m0["axis"]
+        order = [a for a in range(3) if a != axis] + [axis]   # in-plane axes, then the normal
+        data = [self.get_monitor_data(n) for n in names]
+        e1, e2, e3 = [data[a][0] for a in order]
+        cuts = ((slice(1, None), slice(1, -1)), (slice(1, -1), slice(1, None)), (slice(1, -1), slice(1, -1)))
+        e1 = (e1[:, 1:, 1:-1] + e1[:, :-1, 1:-1]) / 2
+        e2 = (e2[:, 1:-1, 1:] + e2[:, 1:-1, :-1]) / 2
+        e3 = e3[:, 1:-1, 1:-1]
+        comps = (e1, e2, e3)
+        values = np.array([comps[order.index(a)] for a in range(3)])
+        # coordinates of the x component's samples, as the reference labels the result
+        vx, cx = data[0]
+        cut = cuts[order.index(0)]
+        coords = {"component": ("x", "y", "z"), "time": cx["time"]}
+        for k, a in enumerate(order[:2]):
+            coords["xyz"[a]] = cx["xyz"[a]][cut[k]]
+        return values, coords
 
     def get_monitor_data(self, name: str):
         """Monitor samples with their coordinates (rfnetwork/solver.py:2703-2747).

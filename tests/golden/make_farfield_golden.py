@@ -9,7 +9,9 @@ phasors, and records what get_farfield_rE (rfnetwork/solver.py:2870-3021)
 hands to core_func.nf2ff: the surface currents, cell positions and areas,
 face positions and the beta / theta / phi arrays. The fixture pins
 rfnetwork_b200.solver's far-field monitor setup and current assembly bit for
-bit; the transform itself is checked against oracle/nf2ff.py.
+bit; the transform itself is checked against oracle/nf2ff.py. A second
+fixture, farfield_gain.npz, holds the reference's get_farfield_gain
+(rfnetwork/solver.py:2804-2868) of a seeded far field.
 
 Usage:  python tests/golden/make_farfield_golden.py   (needs the reference checkout)
 """
@@ -46,6 +48,30 @@ def build_model(FDTD_Solver, Box, Rectangle, explicit_mesh):
     src = s.gaussian_modulated_source(11e9, 150e-12, 150e-12, 60 * float(s.dt))
     s.assign_excitation(src, 1)
     return s
+
+
+GAIN_POLS = ["thetapol", "phipol", "rhcp", "lhcp"]
+
+
+def _install_reference_dtft(ref):
+    """The reference's own utils.dtft (rfnetwork/utils.py:14-71), compiled from its
+    source into the stand-in rfnetwork.utils module (the rest of utils.py needs
+    pyvista and np_struct)."""
+    import ast
+    from scipy import signal
+
+    src = (mg.REF / "rfnetwork/utils.py").read_text()
+    fn = next(n for n in ast.parse(src).body if isinstance(n, ast.FunctionDef) and n.name == "dtft")
+    ns = {"np": np, "signal": signal}
+    exec(compile(ast.Module(body=[fn], type_ignores=[]), str(mg.REF / "rfnetwork/utils.py"), "exec"), ns)
+    ref.utils.dtft = ns["dtft"]
+
+
+def gain_field(n_freq):
+    """Seeded far field rE [2, frequency, theta, phi] for the gain fixture."""
+    rng = np.random.default_rng(12)
+    shape = (2, n_freq, len(THETA), len(PHI))
+    return (rng.standard_normal(shape) + 1j * rng.standard_normal(shape)).astype(np.complex64)
 
 
 def monitor_values(s):
@@ -98,6 +124,16 @@ def main():
         out[k] = c["ff"][k]
     path = mg.HERE / "farfield_small.npz"
     np.savez_compressed(path, **out)
+    print(f"wrote {path} ({path.stat().st_size} bytes)")
+
+    # realized gain (rfnetwork/solver.py:2804-2868) of a seeded far field: the
+    # reference's own projection, port-source DTFT and normalisation
+    _install_reference_dtft(ref)
+    rE = gain_field(len(FREQ))
+    s.get_farfield_rE = lambda theta, phi: rE
+    gain = s.get_farfield_gain(THETA, PHI, polarization=GAIN_POLS)
+    path = mg.HERE / "farfield_gain.npz"
+    np.savez_compressed(path, rE=rE, gain=np.asarray(gain))
     print(f"wrote {path} ({path.stat().st_size} bytes)")
 
 

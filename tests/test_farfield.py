@@ -107,3 +107,46 @@ def test_gpu_farfield_of_a_run(engine_lib):
     nf2ff_oracle.nf2ff(*s.farfield_currents(), ff)
     assert np.abs(rE).max() > 0
     assert rel_l2(rE, ff["data"]) <= 1e-5
+
+
+def test_farfield_gain_matches_reference():
+    """get_farfield_gain on a seeded far field against the reference's own
+    get_farfield_gain (rfnetwork/solver.py:2804-2868) of the same field
+    (tests/golden/farfield_gain.npz): projections, port-source DTFT, 4 pi U / P_in."""
+    g = np.load(mg.HERE / "farfield_gain.npz")
+    s = _model()
+    s.get_farfield_rE = lambda theta, phi: g["rE"]
+    gain = s.get_farfield_gain(fg.THETA, fg.PHI, polarization=fg.GAIN_POLS)
+    assert gain.shape == g["gain"].shape
+    np.testing.assert_allclose(gain, g["gain"], rtol=1e-12, atol=0)
+    default = s.get_farfield_gain(fg.THETA, fg.PHI)
+    np.testing.assert_allclose(default, g["gain"][:2], rtol=1e-12, atol=0)
+
+
+def test_total_monitor_data():
+    """The three components of an e_total monitor brought to common points
+    (rfnetwork/solver.py:2750-2802): in-plane components averaged along
+    themselves, plane-edge samples dropped, ordered x, y, z."""
+    s = mg.build_model(S.FDTD_Solver, geo.Box, geo.Rectangle, geo.Line, mg.grid_edges(),
+                       lambda m, e: m.generate_mesh(grid=e))
+    for axis, index in (("z", 2), ("x", 5)):
+        s.add_field_monitor(f"et{axis}", "e_total", axis, index=index, n_step=2)
+    co, pr, mo, mem, Nx, Ny, Nz, Nt = s.pack_inputs(gpu=True)
+    rng = np.random.default_rng(7)
+    for m in mo:   # seeded samples in place of a run
+        m["values"][...] = rng.standard_normal(m["values"].shape).astype(m["values"].dtype)
+    s.unpack_results(pr, mo, gpu=True, Nt=Nt)
+    s._solved = True
+    ex, ey, ez = [s.monitors[f"etz_{a}"]["values"] for a in "xyz"]
+    vals, coords = s.get_total_monitor_data("etz")
+    assert np.array_equal(vals[0], (ex[:, 1:, 1:-1] + ex[:, :-1, 1:-1]) / 2)
+    assert np.array_equal(vals[1], (ey[:, 1:-1, 1:] + ey[:, 1:-1, :-1]) / 2)
+    assert np.array_equal(vals[2], ez[:, 1:-1, 1:-1])
+    assert coords["component"] == ("x", "y", "z") and len(coords["x"]) == vals.shape[2]
+    ex, ey, ez = [s.monitors[f"etx_{a}"]["values"] for a in "xyz"]
+    vals, _ = s.get_total_monitor_data("etx")   # plane y-z: y, z in the plane, x normal
+    assert np.array_equal(vals[1], (ey[:, 1:, 1:-1] + ey[:, :-1, 1:-1]) / 2)
+    assert np.array_equal(vals[2], (ez[:, 1:-1, 1:] + ez[:, 1:-1, :-1]) / 2)
+    assert np.array_equal(vals[0], ex[:, 1:-1, 1:-1])
+    with pytest.raises(ValueError):
+        s.get_total_monitor_data("mz")
