@@ -198,6 +198,10 @@ bool compile_grid(int nx, int ny, int nz, const float* const* coef, const std::v
       err = "Too many probes on one cell.";
       return false;
     }
+  // the probe cells in increasing cell order, walked alongside the cells below
+  std::vector<std::pair<int64_t, CellInfo>> probe_cells(cell_info.begin(), cell_info.end());
+  std::sort(probe_cells.begin(), probe_cells.end(),
+            [](const auto& a, const auto& b) { return a.first < b.first; });
 
   // ---- rows, built per x slab in parallel with thread-local dedup
   n_threads = std::max(1, std::min(n_threads, nx));
@@ -210,6 +214,10 @@ bool compile_grid(int nx, int ny, int nz, const float* const* coef, const std::v
     std::vector<Row>& rows = local_rows[t];
     Row prev;
     uint32_t prev_id = UINT32_MAX;
+    // next probe cell at or after this slab's first cell
+    size_t pc = size_t(std::lower_bound(probe_cells.begin(), probe_cells.end(), int64_t(xa) * ny * nz,
+                                        [](const auto& a, int64_t c) { return a.first < c; }) -
+                       probe_cells.begin());
     for (int x = xa; x < xb; ++x)
       for (int y = 0; y < ny; ++y)
         for (int z = 0; z < nz; ++z) {
@@ -220,13 +228,11 @@ bool compile_grid(int nx, int ny, int nz, const float* const* coef, const std::v
             for (int s = R_CA_EY_Z; s <= R_DB2_HX_Z; ++s) r.w[s] = 0u;
           unsigned src_mask = 0;
           int probe_first = -1, probe_count = 0;
-          if (!cell_info.empty()) {
-            auto it = cell_info.find(cell);
-            if (it != cell_info.end()) {
-              src_mask = it->second.src_mask;
-              probe_first = it->second.first;
-              probe_count = it->second.count;
-            }
+          if (pc < probe_cells.size() && probe_cells[pc].first == cell) {
+            src_mask = probe_cells[pc].second.src_mask;
+            probe_first = probe_cells[pc].second.first;
+            probe_count = probe_cells[pc].second.count;
+            ++pc;
           }
           // guarded (never updated) E splits: ex_y, ez_y at y max; ex_z, ey_z at
           // z max; ey_x, ez_x at x max (solver.cu:152-185)
