@@ -13,6 +13,7 @@ Tolerances (written per test):
  * device FP64 DFT vs numpy DTFT of the recorded series: 1e-9 relative.
 """
 import copy
+import json
 
 import numpy as np
 import pytest
@@ -137,6 +138,12 @@ def test_microstrip_full_size(engine_lib, oracle_lib):
     keep = mag > -40
     ddb = np.abs(20 * np.log10(np.abs(S32)) - mag)[keep]
     dph = np.abs(np.angle(S32 / S64, deg=True))[keep]
+    # the measured errors of this result (pytest -s prints them)
+    print(json.dumps({"model": "microstrip 64x64x48, 10-cell PML, 2000 steps",
+                      "probes_vs_fp32_oracle_rel_l2": float(rel_l2(pe, po)),
+                      "port_v_vs_fp64_rel_l2": [float(rel_l2(se.port_vi_series(i)[0], s64.port_vi_series(i)[0]))
+                                                for i in range(len(s.ports))],
+                      "s_vs_fp64_max_db": float(ddb.max()), "s_vs_fp64_max_deg": float(dph.max())}))
     assert ddb.max() <= 0.01 and dph.max() <= 0.1, (ddb.max(), dph.max())
     # physical sanity: a matched 50-ohm-ish line transmits most of the power
     assert np.abs(S32[:, 1]).max() > 0.5
