@@ -609,7 +609,28 @@ def run_design(args, rank, world, local_rank):
         adj_ms.append(st["adjoint_ms"])
     st = designs.batch.stats()
     designs.close()
+    # the same gradients one variant after another: one model, one forward
+    # (recorded box history) and one adjoint per variant
+    from rfnetwork_b200.adjoint import FDTDDesign
+    single = FDTDDesign(s, box, [(0, len(pr) - 1, 1.0)], omega)
+    th = theta.detach()
+
+    def sequential_pass():
+        for v in range(n_var):
+            tv = th[v].clone().requires_grad_(True)
+            (single(1 + 9 * torch.sigmoid(tv)).abs() ** 2).sum().backward()
+
+    sequential_pass()  # warm-up
+    t_seq = []
+    for _ in range(args.steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        sequential_pass()
+        torch.cuda.synchronize()
+        t_seq.append(time.perf_counter() - t0)
+    single.close()
     ts = ranks.max(statistics.fmean(t))   # wall time of the slowest rank
+    ts_seq = ranks.max(statistics.fmean(t_seq))
     ranks.close()
     if rank != 0:
         return None
@@ -626,6 +647,10 @@ def run_design(args, rank, world, local_rank):
                    "forward_mcell_updates_per_s": round(n_var * cells * nt / statistics.fmean(fwd_ms) / 1e3, 1),
                    "adjoint_mcell_updates_per_s": round(n_var * cells * nt / statistics.fmean(adj_ms) / 1e3, 1)},
         "objective_mean": [round(float(np.mean(j)), 4) for j in J_hist],
+        "sequential": {"value": round(world * n_var / ts_seq, 3), "unit": "gradient evaluations/s",
+                       "how": f"the {n_var} gradients one after another through FDTDDesign (forward with the "
+                              "recorded box history, then the adjoint), wall time, no optimizer step"},
+        "batched_over_sequential": round(ts_seq / ts, 3),
         "gpu_launches": int(st["step_launches"] + st["adjoint_launches"]),
     }
 
