@@ -198,7 +198,8 @@ int fdtd_set_box_coefficients(fdtd_sim* s, const int* box, const float* coefs);
  *          dict's order (Ca_ex_y with Ca_ex_z held equal, Cb_ex_y, Cb_ex_z, ...)
  * The discrete adjoint runs backwards from the last step, one kernel launch
  * per step, with the transposed update in FP32 and the products accumulated in
- * FP64. */
+ * FP64. Its work buffers (about 36 floats per cell) stay allocated on the
+ * simulation for the next call until fdtd_destroy. */
 int fdtd_adjoint(fdtd_sim* s, const double* dJ_dX, int n_series, int n_freq, const int* box, double* grad);
 
 /* ---------------------------------------------------------------- batches */
