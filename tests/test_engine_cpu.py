@@ -162,3 +162,16 @@ def test_borrowed_coefficients(engine_lib, small):
     assert rows_p[ids_p[x, y, z], 0].view(np.float32) == np.float32(0.5)
     a.close()
     b.close()
+
+
+def test_table_limit_is_reported(engine_lib):
+    """More distinct cell rows than the 16-bit material index addresses is an
+    error of the compile, not a wrap-around."""
+    rng = np.random.default_rng(0)
+    shape = (42, 41, 40)            # 68,880 cells, each its own row
+    sim = _lib.Simulation(*shape)
+    for name in COEFF_NAMES:
+        sim.set_coefficient(name, rng.uniform(0.5, 1.0, shape).astype(np.float32))
+    with pytest.raises(_lib.FdtdError, match="at most 65536"):
+        sim.compile()
+    sim.close()

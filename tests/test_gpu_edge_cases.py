@@ -1,0 +1,69 @@
+"""Edge cases of the engine on the GPU: tiny and ragged grids (smaller than
+one tile, sizes that leave partial tiles in x, y and z), every cell a
+distinct row with split components, a soft source and probes on the grid's
+first and last cells, a run without probes, and a one-step run.
+
+Random coefficients give every cell its own table row and most cells split
+E and H components, so the streaming kernel's split paths, narrow windows,
+halo recomputation and zero-filled edges are all exercised; it must give
+the plain kernel's bits exactly (the plain kernel's parity with the oracle is
+tests/test_gpu_parity.py's)."""
+import numpy as np
+import pytest
+
+from rfnetwork_b200 import _lib
+from rfnetwork_b200.solver_constants import COEFF_NAMES
+
+pytestmark = pytest.mark.gpu
+
+
+def _random_sim(shape, seed, nt, variant, probes=True, **kernel):
+    rng = np.random.default_rng(seed)
+    sim = _lib.Simulation(*shape)
+    sim.set_kernel(variant, **kernel)
+    for name in COEFF_NAMES:
+        if name.startswith("Ca") or name.startswith("Da"):
+            a = rng.uniform(0.9, 1.0, shape)
+        else:
+            a = rng.uniform(0.0, 0.1, shape) * rng.choice([-1.0, 1.0], shape)
+        sim.set_coefficient(name, a.astype(np.float32))
+    nx, ny, nz = shape
+    if probes:
+        t = np.arange(nt, dtype=np.float32)
+        sim.add_probe(2, (nx // 2, ny // 2, nz // 2), True, np.sin(0.3 * t) * np.exp(-((t - 10) / 6) ** 2))
+        # every field on the first and on the last cell the Yee shift allows
+        for f in range(6):
+            lo = [1 if f in (1, 2, 3) else 0, 1 if f in (0, 2, 4) else 0, 1 if f in (0, 1, 5) else 0]
+            sim.add_probe(f, tuple(lo))
+            sim.add_probe(f, (nx - 1, ny - 1, nz - 1))
+    return sim
+
+
+@pytest.mark.parametrize("shape", [(2, 2, 2), (3, 5, 2), (33, 9, 5), (40, 17, 3), (31, 8, 27), (64, 1 + 8, 64)])
+def test_ragged_grids_stream_equals_plain(engine_lib, shape):
+    nt = 40
+    plain = _random_sim(shape, 1, nt, 0)
+    plain.run(nt)
+    ref = plain.probe_values()
+    plain.close()
+    assert np.isfinite(ref).all() and np.abs(ref).max() > 0
+    for ty, stages, zchunk in ((8, 4, 0), (4, 5, 1), (6, 3, 2)):
+        sim = _random_sim(shape, 1, nt, 1, tile_y=ty, stages=stages, zchunk=zchunk)
+        sim.run(nt)
+        got = sim.probe_values()
+        sim.close()
+        assert np.array_equal(got, ref), (shape, ty, stages, zchunk)
+
+
+def test_run_without_probes_and_one_step(engine_lib):
+    sim = _random_sim((20, 12, 10), 2, 5, 1, probes=False)
+    sim.run(5)                      # no probes: nothing recorded, nothing to read
+    assert sim.stats()["step_launches"] == 5
+    sim.close()
+    a = _random_sim((20, 12, 10), 3, 1, 0)
+    b = _random_sim((20, 12, 10), 3, 1, 1)
+    a.run(1)
+    b.run(1)
+    assert np.array_equal(a.probe_values(), b.probe_values())
+    a.close()
+    b.close()
