@@ -75,13 +75,13 @@ struct StreamGeom {
   static constexpr int HW = 40, EW = 36, IW = 40;  // box widths along x
   static constexpr int HR = TY + 2, ER = TY + 1;   // box heights along y
   static constexpr int HC = HR * HW;               // floats per H component
-  static constexpr int EC = ER * EW;               // floats per E (and E split) component
-  static constexpr int SHC = TY * EW;              // floats per H split component
+  static constexpr int EC = ER * EW;               // floats per E component (float2 pairs per E split pair)
+  static constexpr int SHC = TY * EW;              // float2 pairs per H split pair
   static constexpr int HB = 3 * HC * 4;
   static constexpr int EB = 3 * EC * 4;
   static constexpr int IB = ER * IW * 2;
-  static constexpr int SEB = 6 * EC * 4;
-  static constexpr int SHB = 6 * SHC * 4;
+  static constexpr int SEB = 6 * EC * 4;           // 3 E split pairs of 8 bytes per cell
+  static constexpr int SHB = 6 * SHC * 4;          // 3 H split pairs
   static constexpr int A(int b) { return (b + 127) / 128 * 128; }
   static constexpr int OFF_E = A(HB);
   static constexpr int OFF_I = OFF_E + A(EB);
@@ -90,8 +90,8 @@ struct StreamGeom {
   static constexpr int STAGE = OFF_HS + A(SHB);
   static constexpr uint32_t MAIN_BYTES = HB + EB + IB;
   static constexpr uint32_t SPLIT_BYTES = SEB + SHB;
-  static constexpr int SECN = ER * kStreamWin;     // floats per E split component, narrow window
-  static constexpr int SHCN = TY * kStreamWin;     // floats per H split component, narrow window
+  static constexpr int SECN = ER * kStreamWin;     // float2 pairs per E split pair, narrow window
+  static constexpr int SHCN = TY * kStreamWin;     // float2 pairs per H split pair, narrow window
   static constexpr uint32_t SPLIT_BYTES_N = 6 * (SECN + SHCN) * 4;
   static constexpr int NCW = TY + 1;               // consumer warps
   static constexpr int CONSUMERS = 32 * NCW;
