@@ -11,7 +11,8 @@ face positions and the beta / theta / phi arrays. The fixture pins
 rfnetwork_b200.solver's far-field monitor setup and current assembly bit for
 bit; the transform itself is checked against oracle/nf2ff.py. A second
 fixture, farfield_gain.npz, holds the reference's get_farfield_gain
-(rfnetwork/solver.py:2804-2868) of a seeded far field.
+(rfnetwork/solver.py:2804-2868) of a seeded far field, and dtft_small.npz the
+reference's utils.dtft of a seeded series, plain and downsampled.
 
 Usage:  python tests/golden/make_farfield_golden.py   (needs the reference checkout)
 """
@@ -134,6 +135,17 @@ def main():
     gain = s.get_farfield_gain(THETA, PHI, polarization=GAIN_POLS)
     path = mg.HERE / "farfield_gain.npz"
     np.savez_compressed(path, rE=rE, gain=np.asarray(gain))
+    print(f"wrote {path} ({path.stat().st_size} bytes)")
+
+    # the reference's DTFT (rfnetwork/utils.py:14-71) of a seeded series, plain
+    # and low-passed / decimated (downsample=True), at a time step like the models'
+    rng = np.random.default_rng(13)
+    x = (rng.standard_normal(4000) * np.exp(-np.linspace(0, 6, 4000))).astype(np.float32)
+    f = np.linspace(1e9, 20e9, 41)
+    fs = 1 / float(s.dt)
+    path = mg.HERE / "dtft_small.npz"
+    np.savez_compressed(path, x=x, f=f, fs=fs, X=ref.utils.dtft(x, f, fs, downsample=False),
+                        X_ds=ref.utils.dtft(x, f, fs, downsample=True))
     print(f"wrote {path} ({path.stat().st_size} bytes)")
 
 

@@ -150,3 +150,12 @@ def test_total_monitor_data():
     assert np.array_equal(vals[0], ex[:, 1:-1, 1:-1])
     with pytest.raises(ValueError):
         s.get_total_monitor_data("mz")
+
+
+def test_dtft_matches_reference():
+    """dtft against the reference's utils.dtft (rfnetwork/utils.py:14-71) of a
+    seeded series (tests/golden/dtft_small.npz): the direct sum, and the
+    low-passed, decimated form of downsample=True."""
+    g = np.load(mg.HERE / "dtft_small.npz")
+    np.testing.assert_allclose(S.dtft(g["x"], g["f"], float(g["fs"])), g["X"], rtol=1e-12, atol=0)
+    np.testing.assert_allclose(S.dtft(g["x"], g["f"], float(g["fs"]), downsample=True), g["X_ds"], rtol=1e-12, atol=0)
