@@ -63,8 +63,10 @@ def parse_args():
     ap.add_argument("--nt", type=int, default=NT, help="time steps per simulation")
     ap.add_argument("--e2e-steps", type=int, default=None, help="end-to-end calls timed (default: --steps)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", choices=("boxes", "batch", "adjoint", "design"), default="boxes",
-                    help="boxes: the bandwidth model (default); batch: 64 uneven simulations in one launch "
+    ap.add_argument("--workload", choices=("boxes", "microstrip", "batch", "adjoint", "design"), default="boxes",
+                    help="boxes: the bandwidth model (default); microstrip: the 64x64x48 microstrip with its "
+                         "101-frequency S11/S21 (the case the reference runs on the CPU), solve time against the "
+                         "CPU restatement of the reference engine; batch: 64 uneven simulations in one launch "
                          "per step against 64 sequential single-simulation runs; adjoint: forward + discrete "
                          "adjoint gradient of a 48x48x4 permittivity design against one forward solve; "
                          "design: Adam steps on 32 design variants, batched forward and batched adjoint")
@@ -375,6 +377,89 @@ def run_reference(args, rank, world):
     }
 
 
+# ------------------------------------------------------ microstrip workload
+
+def run_microstrip(args, rank, world, local_rank):
+    """64x64x48 microstrip, 10-cell PML on six faces, 2000 steps, two 50-ohm ports, S11 and
+    S21 at 101 frequencies from the device DFT: the reference's small case, which it runs on
+    the CPU. One step is one full solve. Device time (CUDA events), end to end through
+    cuda_func.solver_run_dft with host arrays, and the CPU restatement of the reference
+    engine on the same model beside it (rank 0, N = 1)."""
+    import torch
+    from rfnetwork_b200 import _lib, configs, cuda_func
+
+    torch.cuda.set_device(local_rank)
+    ranks = RankSync(world, local_rank)
+    nt = args.nt if args.nt != NT else 2000
+    s = configs.microstrip(nt=nt)
+    f = configs.microstrip_frequencies()
+    co, pr, mo, mem, Nx, Ny, Nz, Nt = s.pack_inputs(gpu=True)
+    names, terms = s.dft_series()
+    omega = s.dft_omega(f)
+    cells = Nx * Ny * Nz
+    sim = _lib.Simulation(Nx, Ny, Nz)
+    sim.set_coefficients(co)
+    for p in pr:
+        src = bool(p["is_source"])
+        sim.add_probe(int(p["field"]), p["idx"], src, p["values"][:Nt] if src else None)
+    sim.set_dft(terms, omega)
+    stream = torch.cuda.Stream()
+    sim.set_stream(stream.cuda_stream)
+    for _ in range(max(args.warmup, 0)):
+        sim.run_async(Nt)
+        sim.synchronize()
+    ranks.barrier()
+    evs = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
+    evs[0].record(stream)
+    for k in range(args.steps):
+        sim.run_async(Nt)
+        evs[k + 1].record(stream)
+    sim.synchronize()
+    torch.cuda.synchronize()
+    ranks.barrier()
+    dev_ms = ranks.max(sum(evs[k].elapsed_time(evs[k + 1]) for k in range(args.steps)) / args.steps)
+    st = sim.stats()
+    sim.close()
+    pr_h = copy.deepcopy(pr)
+    cuda_func.solver_run_dft(co, pr_h, mo, Nx, Ny, Nz, Nt, terms, omega)  # warm-up
+    ranks.barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        pr_h = copy.deepcopy(pr)
+        cuda_func.solver_run_dft(co, pr_h, mo, Nx, Ny, Nz, Nt, terms, omega)
+    torch.cuda.synchronize()
+    e2e_s = ranks.max((time.perf_counter() - t0) / args.steps)
+    info = cuda_func.last_run_info()
+    ranks.close()
+    if rank != 0:
+        return None
+    out = {
+        "metric": METRIC, "value": round(world * cells * Nt / (dev_ms * 1e-3) / 1e6, 1), "unit": UNIT,
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(dev_ms, 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic: microstrip on a PEC ground plane, Gaussian-modulated port excitation",
+        "config": {"workload": f"microstrip 64x64x48, 10-cell PML, {Nt} steps, 2 ports, 101-freq S11/S21",
+                   "cells": cells, "time_steps": Nt, "step": "one full solve",
+                   "kernel": {k: st[k] for k in ("variant", "tile_y", "stages", "zchunk", "grid", "n_tiles")}},
+        "e2e": {"value": round(world * cells * Nt / e2e_s / 1e6, 1), "unit": UNIT,
+                "h2d_bytes_per_step": int(info.get("h2d_bytes", 0)),
+                "d2h_bytes_per_step": int(info.get("d2h_bytes", 0)),
+                "s_per_step": round(e2e_s, 4), "call": "cuda_func.solver_run_dft"},
+        "gpu_launches": int(st["step_launches"] + st["dft_launches"]) * args.steps,
+    }
+    if world == 1 and not args.no_cpu_baseline:
+        from oracle import cpu_engine
+        n_thr = cpu_engine.default_threads()
+        cpu_engine.build()
+        c_co, c_pr, c_mo, c_mem, cNx, cNy, cNz, cNt = s.pack_inputs(gpu=False)
+        t0 = time.perf_counter()
+        cpu_engine.solver_run(c_co, c_pr, c_mo, c_mem, cNx, cNy, cNz, cNt, n_thr, 0)
+        cpu_s = time.perf_counter() - t0
+        out["cpu_baseline"] = {"value": round(cells * Nt / cpu_s / 1e6, 2), "unit": UNIT, "cores": n_thr,
+                               "kind": "port", "sample": f"the full {Nt}-step solve ({cpu_s:.2f} s)"}
+    return out
+
+
 # ------------------------------------------------------------ batched workload
 
 BATCH_SIMS = 64
@@ -662,6 +747,8 @@ def main():
     local_rank = int(os.environ.get("LOCAL_RANK", 0))
     if args.impl == "reference":
         out = run_reference(args, rank, world)
+    elif args.workload == "microstrip":
+        out = run_microstrip(args, rank, world, local_rank)
     elif args.workload == "batch":
         out = run_batch(args, rank, world, local_rank)
     elif args.workload == "adjoint":
