@@ -214,6 +214,8 @@ bool compile_grid(int nx, int ny, int nz, const float* const* coef, const std::v
     std::vector<Row>& rows = local_rows[t];
     Row prev;
     uint32_t prev_id = UINT32_MAX;
+    std::vector<uint32_t> prev_col(static_cast<size_t>(nz), UINT32_MAX);  // ids of the previous (x, y) column
+    int64_t n_esplit = 0, n_hsplit = 0;
     // next probe cell at or after this slab's first cell
     size_t pc = size_t(std::lower_bound(probe_cells.begin(), probe_cells.end(), int64_t(xa) * ny * nz,
                                         [](const auto& a, int64_t c) { return a.first < c; }) -
@@ -263,22 +265,36 @@ bool compile_grid(int nx, int ny, int nz, const float* const* coef, const std::v
           if (flags & (0x38u * kFlagCompSplit0)) flags |= kFlagHSplit;
           if (e_diff || h_diff) flags |= kFlagGraded;
           flags |= uint32_t(probe_count) << 16;
-          e_split[t] += (flags & kFlagESplit) ? 1 : 0;
-          h_split[t] += (flags & kFlagHSplit) ? 1 : 0;
+          n_esplit += (flags & kFlagESplit) ? 1 : 0;  // thread-local: the shared counters sit in one cache line
+          n_hsplit += (flags & kFlagHSplit) ? 1 : 0;
           r.w[R_FLAGS] = flags;
           r.w[R_PROBE] = uint32_t(probe_first);
+          // the row is usually that of the cell below (z - 1) or of the cell
+          // at the same z one column back (y - 1; e.g. a z-PML slab, whose
+          // rows change with z only); the hash table is the last resort
           uint32_t id;
+          const uint32_t back = prev_col[size_t(z)];
           if (prev_id != UINT32_MAX && RowEq()(r, prev)) {
             id = prev_id;
+          } else if (back != UINT32_MAX && RowEq()(r, rows[back])) {
+            id = back;
+            prev = r;
+            prev_id = id;
           } else {
-            auto ins = map.emplace(r, uint32_t(rows.size()));
-            if (ins.second) rows.push_back(r);
-            id = ins.first->second;
+            auto it = map.find(r);
+            if (it == map.end()) {
+              it = map.emplace(r, uint32_t(rows.size())).first;
+              rows.push_back(r);
+            }
+            id = it->second;
             prev = r;
             prev_id = id;
           }
+          prev_col[size_t(z)] = id;
           local_ids[size_t(cell)] = id;
         }
+    e_split[t] = n_esplit;
+    h_split[t] = n_hsplit;
   };
   {
     std::vector<std::thread> pool;
