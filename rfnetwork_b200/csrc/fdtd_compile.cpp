@@ -71,19 +71,39 @@ using RowMap = std::unordered_map<Row, uint32_t, RowHash, RowEq>;
 }  // namespace
 
 GradedIndex::GradedIndex(const CompiledGrid& g, uint32_t mask) : nx(g.nx), ny(g.ny), nz(g.nz) {
-  // summed-volume table of flagged cells, indexed [x][y][z] with a zero border
+  // summed-volume table of flagged cells, indexed [x][y][z] with a zero border:
+  // the 2D sums over (y, z) of every x plane (planes in parallel), then the
+  // running sum along x (plane positions in parallel)
   sy_ = nz + 1;
   sx_ = int64_t(ny + 1) * sy_;
   sv_.assign(size_t(nx + 1) * sx_, 0);
-  for (int x = 0; x < nx; ++x)
-    for (int y = 0; y < ny; ++y)
-      for (int z = 0; z < nz; ++z) {
-        const uint32_t f = g.rows[g.ids[(size_t(x) * ny + y) * nz + z]].w[R_FLAGS];
-        const int32_t v = (f & mask) ? 1 : 0;
-        const int64_t i = (x + 1) * sx_ + (y + 1) * sy_ + (z + 1);
-        sv_[i] = v + sv_[i - sx_] + sv_[i - sy_] + sv_[i - 1] - sv_[i - sx_ - sy_] - sv_[i - sx_ - 1] -
-                 sv_[i - sy_ - 1] + sv_[i - sx_ - sy_ - 1];
+  const int n_threads = int(std::max(1u, std::min(std::thread::hardware_concurrency(), 32u)));
+  auto parallel = [n_threads](int64_t n, auto&& body) {  // body(a, b) over [a, b) slices of [0, n)
+    const int k = int(std::max<int64_t>(1, std::min<int64_t>(n_threads, n)));
+    std::vector<std::thread> pool;
+    for (int t = 0; t < k; ++t) pool.emplace_back(body, n * t / k, n * (t + 1) / k);
+    for (auto& th : pool) th.join();
+  };
+  parallel(nx, [&](int64_t xa, int64_t xb) {
+    for (int64_t x = xa; x < xb; ++x) {
+      int32_t* P = sv_.data() + (x + 1) * sx_;
+      for (int y = 0; y < ny; ++y) {
+        const uint16_t* id = g.ids.data() + (size_t(x) * ny + y) * nz;
+        int32_t run = 0;
+        for (int z = 0; z < nz; ++z) {
+          run += (g.rows[id[z]].w[R_FLAGS] & mask) ? 1 : 0;
+          P[(y + 1) * sy_ + z + 1] = run + P[y * sy_ + z + 1];
+        }
       }
+    }
+  });
+  parallel(sx_, [&](int64_t ja, int64_t jb) {
+    for (int x = 1; x <= nx; ++x) {
+      int32_t* cur = sv_.data() + x * sx_;
+      const int32_t* prev = cur - sx_;
+      for (int64_t j = ja; j < jb; ++j) cur[j] += prev[j];
+    }
+  });
 }
 
 int64_t GradedIndex::count(int x0, int x1, int y0, int y1, int z0, int z1) const {
