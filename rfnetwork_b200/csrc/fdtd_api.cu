@@ -56,6 +56,29 @@ struct ArgError {
   std::string msg;
 };
 
+// The engine's device memory comes from a stream-ordered pool of its own per
+// device that keeps freed blocks (release threshold: never), so the ~1 GB of
+// one solve is reused by the next instead of being unmapped and mapped again
+// (which otherwise adds a few hundred ms to some solves).
+cudaMemPool_t engine_pool() {
+  static std::mutex mu;
+  static cudaMemPool_t pools[64] = {};
+  int dev = 0;
+  CK(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) throw ArgError{FDTD_ERR_CUDA, "device index out of range"};
+  std::lock_guard<std::mutex> lock(mu);
+  if (!pools[dev]) {
+    cudaMemPoolProps props{};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = dev;
+    CK(cudaMemPoolCreate(&pools[dev], &props));
+    uint64_t keep = UINT64_MAX;
+    CK(cudaMemPoolSetAttribute(pools[dev], cudaMemPoolAttrReleaseThreshold, &keep));
+  }
+  return pools[dev];
+}
+
 template <typename T>
 struct DevBuf {
   T* p = nullptr;
@@ -63,7 +86,10 @@ struct DevBuf {
   size_t cap = 0;  // elements allocated
   void alloc(size_t count) {
     free();
-    if (count) CK(cudaMalloc(&p, count * sizeof(T)));
+    if (count) {
+      CK(cudaMallocFromPoolAsync(reinterpret_cast<void**>(&p), count * sizeof(T), engine_pool(), 0));
+      CK(cudaStreamSynchronize(0));  // usable on every stream from here
+    }
     n = cap = count;
   }
   // Like alloc, but keeps the allocation when it already holds `count`.
@@ -72,7 +98,11 @@ struct DevBuf {
     n = count;
   }
   void free() {
-    if (p) cudaFree(p);
+    if (p) {
+      cudaDeviceSynchronize();  // no stream may still use it (cudaFree would wait the same way)
+      cudaFreeAsync(p, 0);
+      cudaStreamSynchronize(0);
+    }
     p = nullptr;
     n = cap = 0;
   }
