@@ -376,6 +376,8 @@ struct Engine {
   cudaGraphExec_t graph = nullptr;
   int graph_nt = -1;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  cudaStream_t cap_stream = nullptr;                   // box-history captures beside the steps
+  cudaEvent_t cap_fork = nullptr, cap_join = nullptr;
   int64_t step_launches = 0, dft_launches = 0, adj_launches = 0;
   double adj_ms = 0;
   bool use_graph = true;  // replay the time loop as a captured CUDA graph
@@ -388,11 +390,17 @@ struct Engine {
     if (!own_stream) CK(cudaStreamCreateWithFlags(&own_stream, cudaStreamNonBlocking));
     if (!ev0) CK(cudaEventCreate(&ev0));
     if (!ev1) CK(cudaEventCreate(&ev1));
+    if (!cap_stream) CK(cudaStreamCreateWithFlags(&cap_stream, cudaStreamNonBlocking));
+    if (!cap_fork) CK(cudaEventCreateWithFlags(&cap_fork, cudaEventDisableTiming));
+    if (!cap_join) CK(cudaEventCreateWithFlags(&cap_join, cudaEventDisableTiming));
   }
   ~Engine() {
     if (graph) cudaGraphExecDestroy(graph);
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
+    if (cap_fork) cudaEventDestroy(cap_fork);
+    if (cap_join) cudaEventDestroy(cap_join);
+    if (cap_stream) cudaStreamDestroy(cap_stream);
     if (own_stream) cudaStreamDestroy(own_stream);
   }
 
@@ -864,11 +872,17 @@ struct Engine {
                                cudaMemcpyDeviceToDevice, st));
         }
       if (n_caps) {
-        adj_capture_kernel<<<dim3(cap_blocks, unsigned(n_caps)), 256, 0, st>>>(d_caps.p, n, 0);
+        // the box history of step n reads buffer n & 1, which step n only
+        // reads and step n+1 overwrites: it runs on a side stream beside step n
+        CK(cudaEventRecord(cap_fork, st));
+        CK(cudaStreamWaitEvent(cap_stream, cap_fork, 0));
+        adj_capture_kernel<<<dim3(cap_blocks, unsigned(n_caps)), 256, 0, cap_stream>>>(d_caps.p, n, 0);
         CK(cudaGetLastError());
+        CK(cudaEventRecord(cap_join, cap_stream));
       }
       launch_step(st, n);
       ++step_launches;
+      if (n_caps) CK(cudaStreamWaitEvent(st, cap_join, 0));
       for (auto* s : sims)
         if (!s->monitors.empty()) {
           monitor_kernel<<<64, 256, 0, st>>>(s->d_dev.p, s->d_mons.p, int(s->monitors.size()), n, (n + 1) & 1);
