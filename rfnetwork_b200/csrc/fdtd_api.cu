@@ -824,10 +824,14 @@ struct Engine {
           CK(cudaMemcpyAsync(scls.d_counter.p, &c0, sizeof(unsigned), cudaMemcpyHostToDevice, st));
           CK(cudaStreamSynchronize(st));  // c0 lives on this stack frame
         }
-        for (int n = n0; n < n1; ++n) {
-          adj_capture_kernel<<<dim3(cap_grid, unsigned(caps.size())), 256, 0, st>>>(d_c.p, n, n0);
+        for (int n = n0; n < n1; ++n) {  // the capture beside the step, as in a recorded run
+          CK(cudaEventRecord(cap_fork, st));
+          CK(cudaStreamWaitEvent(cap_stream, cap_fork, 0));
+          adj_capture_kernel<<<dim3(cap_grid, unsigned(caps.size())), 256, 0, cap_stream>>>(d_c.p, n, n0);
           CK(cudaGetLastError());
+          CK(cudaEventRecord(cap_join, cap_stream));
           launch_step(st, n);
+          CK(cudaStreamWaitEvent(st, cap_join, 0));
         }
         for (int n = n1 - 1; n >= n0; --n) {
           adj_fn<<<int(tiles.size()), blk, 0, st>>>(d_as.p, d_t.p, n, n0);
