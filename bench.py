@@ -102,6 +102,16 @@ def peaks():
     return FALLBACK_HBM_GBS, "fallback"
 
 
+def profiled_traffic(variant: int, path: Path = None):
+    """DRAM bytes of one step launch of this workload from the committed ncu
+    summary (its line `traffic_bytes_per_launch (variant V): B`), or None."""
+    tp = path or ROOT / "profiles" / "fdtd_step_stream_c2.md"
+    if not tp.exists():
+        return None
+    m = re.search(r"traffic_bytes_per_launch \(variant %d\): (\d+)" % variant, tp.read_text())
+    return int(m.group(1)) if m else None
+
+
 # ------------------------------------------------------------------- clocks
 
 class ClockSampler:
@@ -274,14 +284,7 @@ def run_ours(args, rank, world, local_rank):
         mean_sim_ms = statistics.fmean(per_sim_ms)
         step_ms = mean_sim_ms / Nt  # one step-kernel launch per time step (+ the DFT every 256 steps)
         achieved = alg_bytes_step / (step_ms * 1e-3) / 1e9
-        # DRAM bytes of one step launch from the committed ncu summary of this
-        # workload (the line `traffic_bytes_per_launch (variant V): B`)
-        traffic = None
-        tp = ROOT / "profiles" / "fdtd_step_stream_c2.md"
-        if tp.exists():
-            m = re.search(r"traffic_bytes_per_launch \(variant %d\): (\d+)" % st["variant"], tp.read_text())
-            if m:
-                traffic = int(m.group(1))
+        traffic = profiled_traffic(st["variant"])
         value = world * cells * Nt * args.steps / (total_ms * 1e-3) / 1e6
         out = {
             "metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": world,
