@@ -67,3 +67,25 @@ def test_run_without_probes_and_one_step(engine_lib):
     assert np.array_equal(a.probe_values(), b.probe_values())
     a.close()
     b.close()
+
+
+def test_batch_of_tiny_grids_equals_single_runs(engine_lib):
+    """A batch whose members are smaller than one tile or leave ragged tiles
+    gives each member the bits of its own run."""
+    shapes = [(2, 2, 2), (3, 5, 2), (33, 9, 5), (40, 17, 3), (31, 8, 27)]
+    nt = 30
+    singles = []
+    for k, shape in enumerate(shapes):
+        sim = _random_sim(shape, 10 + k, nt, 1, tile_y=8, stages=4, zchunk=0)
+        sim.run(nt)
+        singles.append(sim.probe_values())
+        sim.close()
+    sims = [_random_sim(shape, 10 + k, nt, 1) for k, shape in enumerate(shapes)]
+    batch = _lib.Batch(sims)
+    batch.set_kernel(1, 8, 4, 0)
+    batch.run(nt)
+    for sim, ref in zip(sims, singles):
+        assert np.array_equal(sim.probe_values(), ref)
+    batch.close()
+    for sim in sims:
+        sim.close()
