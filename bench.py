@@ -105,7 +105,7 @@ def peaks():
 def profiled_traffic(variant: int, path: Path = None):
     """DRAM bytes of one step launch of this workload from the committed ncu
     summary (its line `traffic_bytes_per_launch (variant V): B`), or None."""
-    tp = path or ROOT / "profiles" / "fdtd_step_stream_c2.md"
+    tp = path or ROOT / "profiles" / "fdtd_step_stream_boxes256.md"
     if not tp.exists():
         return None
     m = re.search(r"traffic_bytes_per_launch \(variant %d\): (\d+)" % variant, tp.read_text())
