@@ -141,7 +141,8 @@ struct KernelConfig {
 
 // Streaming-kernel shapes the autotuner times, and its choices per set of grid
 // sizes (process-wide).
-constexpr int kTuneCandidates[][3] = {{8, 4, 0}, {8, 4, 32}, {8, 3, 0}, {12, 3, 0}, {6, 3, 0}, {4, 4, 0}, {4, 4, 16}};
+constexpr int kTuneCandidates[][3] = {{8, 4, 0}, {8, 4, 32}, {8, 3, 0}, {12, 3, 0}, {6, 3, 0}, {4, 4, 0},
+                                      {4, 4, 16}, {8, 4, 4}, {4, 4, 4}};
 std::mutex g_tune_mutex;
 std::map<std::vector<int>, std::array<int, 3>> g_tune_cache;
 
