@@ -76,13 +76,13 @@ def parse_args():
 # --------------------------------------------------------------------- model
 
 def build_model(nt: int):
-    from rfnetwork_b200 import configs
+    from modelgen import configs
     return configs.boxes(n=GRID, n_pml=N_PML, nt=nt)
 
 
 def dft_spec(s, pr):
     """Port V/I series of the S-parameter post-processing plus one series per point probe."""
-    from rfnetwork_b200 import configs
+    from modelgen import configs
     names, terms = s.dft_series()
     n_lead = len(pr) - len(s.probes)
     for i, k in enumerate(s.probes.keys()):
@@ -218,7 +218,8 @@ class RankSync:
 
 def run_ours(args, rank, world, local_rank):
     import torch
-    from rfnetwork_b200 import _lib, configs, cuda_func
+    from rfnetwork_b200 import _lib, cuda_func
+    from modelgen import configs
 
     torch.cuda.set_device(local_rank)
     ranks = RankSync(world, local_rank)
@@ -389,7 +390,8 @@ def run_microstrip(args, rank, world, local_rank):
     cuda_func.solver_run_dft with host arrays, and the CPU restatement of the reference
     engine on the same model beside it (rank 0, N = 1)."""
     import torch
-    from rfnetwork_b200 import _lib, configs, cuda_func
+    from rfnetwork_b200 import _lib, cuda_func
+    from modelgen import configs
 
     torch.cuda.set_device(local_rank)
     ranks = RankSync(world, local_rank)
@@ -476,7 +478,8 @@ def run_batch(args, rank, world, local_rank):
     launch per time step for all of them, the time loop as one CUDA graph) and one after
     another (fdtd_run per simulation). Each rank runs its own copy."""
     import torch
-    from rfnetwork_b200 import _lib, configs
+    from rfnetwork_b200 import _lib
+    from modelgen import configs
 
     torch.cuda.set_device(local_rank)
     ranks = RankSync(world, local_rank)
@@ -568,7 +571,7 @@ def run_adjoint(args, rank, world, local_rank):
     One step = one gradient evaluation (forward with checkpoints + adjoint sweep). The same
     gradient with the box history recorded instead of checkpoints is reported beside it."""
     import torch
-    from rfnetwork_b200 import configs
+    from modelgen import configs
     from rfnetwork_b200.adjoint import FDTDDesign
 
     torch.cuda.set_device(local_rank)
@@ -653,7 +656,7 @@ def run_design(args, rank, world, local_rank):
     One step = one Adam step (lr 0.05) on all 32 designs: a batched forward solve with the
     box histories recorded, a batched adjoint sweep, the optimizer update."""
     import torch
-    from rfnetwork_b200 import configs
+    from modelgen import configs
     from rfnetwork_b200.adjoint import FDTDDesignBatch
 
     torch.cuda.set_device(local_rank)

@@ -255,7 +255,7 @@ int fdtd_nf2ff(const fdtd_nf2ff_face* faces, int n_faces, int n_freq, const floa
                const float* theta, int n_phi, const float* phi, float* out);
 
 /* Last error of calls that have no handle (fdtd_create, fdtd_batch_create,
- * fdtd_step_noalloc, fdtd_nf2ff). */
+ * fdtd_step_noalloc, fdtd_nf2ff), kept per calling thread. */
 const char* fdtd_global_error(void);
 
 /* ------------------------------------------------ caller-owned buffers */
@@ -278,7 +278,13 @@ const char* fdtd_global_error(void);
  *                fdtd_add_probe, ties in probe order; a row's word 31 is the
  *                index of its cell's first pair, bits 16..31 of word 30 the count.
  *   src, rec     n_probes x nt floats: source amplitudes in, recorded values out.
- *   is_src       n_probes int32 flags. */
+ *   is_src       n_probes int32 flags.
+ *   n_rows       rows in `rows` (1 .. 65536); every index in `mat` must be below it.
+ *   n_probes     probes (>= 0); every probe range a row names (word 31, count in
+ *                bits 16..31 of word 30) must lie in [0, n_probes) of cell_probes.
+ * The entry point checks the sizes and pointers it is given but cannot read
+ * the caller's buffers: an index or probe range outside these bounds makes
+ * the kernel read outside them. */
 typedef struct fdtd_device_grid {
   int nx, ny, nz, pitch;
   int nt;
@@ -290,6 +296,8 @@ typedef struct fdtd_device_grid {
   const float* src;
   float* rec;
   const int32_t* is_src;
+  int n_rows;
+  int n_probes;
 } fdtd_device_grid;
 
 /* Advance steps n0 .. n0+n_steps-1 of a grid held in caller-owned buffers,
@@ -310,8 +318,11 @@ typedef struct fdtd_device_grid {
  *  - The first call on a device looks up the array's device address. Make that
  *    first call before any stream capture on the device.
  *  - All calls share the array. Each call rewrites the descriptor and tile list
- *    it uses, so nothing in it needs to start at zero. Calls whose work
- *    overlaps on the GPU, for example on two streams, race on it.
+ *    it uses (a small set-up kernel on `stream`, before the steps), so nothing
+ *    in it needs to start at zero. Calls whose work overlaps on the GPU, for
+ *    example on two streams, race on it.
+ *  - Everything the GPU reads comes from the caller's device buffers and from
+ *    launch parameters; no host memory is read after the call returns.
  * Errors are reported through fdtd_global_error(). No counterpart exists in the
  * reference, which allocates its device buffers itself in every
  * solver_run_cu call. */

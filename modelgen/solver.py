@@ -1,16 +1,22 @@
-"""FDTD setup API: grid, materials, PML, lumped ports, probes, monitors.
+"""Input builder for tests and benchmarks: the reference's FDTD setup, restated.
 
-This is the Python-facing side of the solver, kept to the reference's
-interface (rfnetwork/solver.py, class ``FDTD_Solver``): the same method names,
-arguments, units (inches) and the same float32 coefficient formulas, so a
-script written for the reference builds the same update coefficients here.
-``solve()`` then runs the time loop on the GPU through the C-ABI library
-(``rfnetwork_b200.cuda_func``) instead of the reference's CPU/CUDA engines.
+Test and benchmark infrastructure, not part of the engine package. The
+reference's own Python package (rfnetwork/solver.py, class ``FDTD_Solver``)
+cannot be imported on this machine (pyvista, np_struct, skimage and
+matplotlib are absent), so this module restates its setup code -- grid,
+materials, PML grading, lumped ports, sources, probes, monitors and the
+packing of ``solve()`` -- to produce, bit for bit, the coefficient arrays and
+probe/monitor lists the reference's ``solve()`` hands its engine (pinned by
+the fixtures under tests/golden/). The expressions and their order follow the
+reference so that the float32 arrays are bit-equal; that is the reason for
+the likeness. ``solve()`` runs the packed inputs through the engine's drop-in
+``rfnetwork_b200.cuda_func``, as the reference's ``solve()`` does once the
+shim is installed.
 
 What is not carried over: the pyvista mesher (``generate_mesh`` takes the grid
 edges, or a uniform cell width that divides the solve box exactly), gerber
 image layers, rendering and the far-field transform. Geometry objects are the
-axis-aligned primitives of ``rfnetwork_b200.geometry``.
+axis-aligned primitives of ``modelgen.geometry``.
 """
 from __future__ import annotations
 
@@ -19,8 +25,9 @@ from copy import copy
 
 import numpy as np
 
+from rfnetwork_b200.units import const, conv
+
 from . import geometry as geo
-from .units import const, conv
 
 u0 = const.u0
 e0 = const.e0
@@ -1036,7 +1043,7 @@ class FDTD_Solver:
         With ``frequency`` the port voltages and currents are also transformed
         on the device (FP64 running DFT); ``get_sparameters_device`` reads them.
         """
-        from . import cuda_func
+        from rfnetwork_b200 import cuda_func
 
         coefficients, probes, monitors, mem, Nx, Ny, Nz, Nt = self.pack_inputs(gpu=True, n_threads=n_threads)
         if frequency is None:

@@ -1,12 +1,16 @@
 """Gradients of DFT objectives with respect to a permittivity / conductivity design.
 
-``FDTDDesign`` wraps one model (an ``FDTD_Solver`` with its mesh, ports,
-probes and sources) and a box of design cells. Called with the relative
-permittivity (and optionally the conductivity) of the design cells as torch
-tensors, it returns the complex device DFT of the chosen probe series as a
-torch tensor that autograd can differentiate:
+``FDTDDesign`` wraps one model and a box of design cells. The model is what
+the reference's ``FDTD_Solver.solve()`` hands its engine (the packed
+coefficient dict, the probe list, the grid shape and the number of steps,
+rfnetwork/solver.py:1441-1575) plus the cell material it was built from
+(``dt``, ``eps``, ``sigma``, ``d_cells``): a ``PackedModel``, or any object
+with a ``pack_inputs(gpu=True)`` method and those attributes. Called with the
+relative permittivity (and optionally the conductivity) of the design cells as
+torch tensors, it returns the complex device DFT of the chosen probe series as
+a torch tensor that autograd can differentiate:
 
-    design = FDTDDesign(solver, (x0, x1, y0, y1, z0, z1), terms, omega)
+    design = FDTDDesign(model, (x0, x1, y0, y1, z0, z1), terms, omega)
     X = design(1 + 9 * torch.sigmoid(theta))          # complex [series, frequency]
     J = (X.abs() ** 2).sum()
     J.backward()                                        # theta.grad
@@ -28,6 +32,7 @@ the affected E sites; torch chains them to the design tensors.
 from __future__ import annotations
 
 import math
+from dataclasses import dataclass
 
 import numpy as np
 import torch
@@ -58,12 +63,42 @@ class _Run(torch.autograd.Function):
         return torch.from_numpy(g), None
 
 
+@dataclass
+class PackedModel:
+    """The engine inputs of one model and the material they were built from.
+
+    coefficients: the 30 float32 (Nx, Ny, Nz) arrays keyed as the reference's
+    packing names them (rfnetwork/solver.py:1473-1518); probes: its probe
+    dicts (``values``, ``field``, ``idx``, ``is_source``); shape (Nx, Ny, Nz);
+    nt time steps; dt seconds; eps, sigma: per-cell permittivity (F/m) and
+    conductivity (S/m), shape (Nx, Ny, Nz); d_cells: cell widths per axis in
+    inches, as the reference's ``FDTD_Solver.d_cells``.
+    """
+    coefficients: dict
+    probes: list
+    shape: tuple
+    nt: int
+    dt: float
+    eps: np.ndarray
+    sigma: np.ndarray
+    d_cells: tuple
+
+    @classmethod
+    def of(cls, model) -> "PackedModel":
+        """A PackedModel as is, or one read off an object with ``pack_inputs``."""
+        if isinstance(model, cls):
+            return model
+        co, pr, mo, mem, Nx, Ny, Nz, Nt = model.pack_inputs(gpu=True)
+        return cls(co, pr, (Nx, Ny, Nz), Nt, float(model.dt), model.eps, model.sigma, tuple(model.d_cells))
+
+
 class FDTDDesign:
     """A model whose design cells' material enters the time loop differentiably."""
 
-    def __init__(self, solver, design_box, terms, omega, checkpoint_every: int | None = None,
+    def __init__(self, model, design_box, terms, omega, checkpoint_every: int | None = None,
                  history_budget: float = 8 * 2**30):
-        co, pr, mo, mem, Nx, Ny, Nz, Nt = solver.pack_inputs(gpu=True)
+        m = PackedModel.of(model)
+        co, pr, (Nx, Ny, Nz), Nt = m.coefficients, m.probes, m.shape, m.nt
         self.shape = (Nx, Ny, Nz)
         self.nt = Nt
         self.base = {k: np.ascontiguousarray(v, dtype=np.float32) for k, v in co.items()}
@@ -82,14 +117,14 @@ class FDTDDesign:
             src = bool(p["is_source"])
             self.sim.add_probe(int(p["field"]), p["idx"], src, p["values"][:Nt] if src else None)
         self.sim.set_dft(terms, omega)
-        self.dt = float(solver.dt)
+        self.dt = float(m.dt)
         # cell material and half widths around the box (float64), one cell of margin above
         sl = (slice(bx0, min(bx1 + 1, Nx)), slice(by0, min(by1 + 1, Ny)), slice(bz0, min(bz1 + 1, Nz)))
         self._sl = sl
-        self._eps = torch.from_numpy(np.asarray(solver.eps, dtype=np.float64)[sl].copy())
-        self._sig = torch.from_numpy(np.asarray(solver.sigma, dtype=np.float64)[sl].copy())
+        self._eps = torch.from_numpy(np.asarray(m.eps, dtype=np.float64)[sl].copy())
+        self._sig = torch.from_numpy(np.asarray(m.sigma, dtype=np.float64)[sl].copy())
         self._d = [torch.from_numpy(np.asarray(conv.m_in(d), dtype=np.float64)[s].copy())
-                   for d, s in zip(solver.d_cells, sl)]
+                   for d, s in zip(m.d_cells, sl)]
         # design cells inside the margin array
         self._dsl = (slice(x0 - bx0, x1 - bx0), slice(y0 - by0, y1 - by0), slice(z0 - bz0, z1 - bz0))
         # the packing's scale of each Cb (inverse widths and sign), read off the base model
@@ -192,15 +227,15 @@ class FDTDDesignBatch:
     """Several designs (variants of models, one design box each) whose forward
     solves run as one batch and whose adjoints run as one batched sweep.
 
-        designs = FDTDDesignBatch([solver] * 32, box, terms, omega)
+        designs = FDTDDesignBatch([model] * 32, box, terms, omega)
         X = designs([1 + 9 * torch.sigmoid(t) for t in thetas])   # complex [member, series, freq]
 
     Every member keeps the box history of its forward run (fdtd_batch_run_recorded);
     the gradient boxes must have one shape so the coefficients stack."""
 
-    def __init__(self, solvers, design_box, terms, omega):
-        self.members = [FDTDDesign(s, design_box, terms, omega, checkpoint_every=None, history_budget=float("inf"))
-                        for s in solvers]
+    def __init__(self, models, design_box, terms, omega):
+        self.members = [FDTDDesign(m, design_box, terms, omega, checkpoint_every=None, history_budget=float("inf"))
+                        for m in models]
         shapes = {tuple(b - a for a, b in zip(m.box[0::2], m.box[1::2])) for m in self.members}
         if len(shapes) != 1 or len({m.nt for m in self.members}) != 1:
             raise ValueError("batch members need one gradient-box shape and one number of time steps")
@@ -224,4 +259,4 @@ class FDTDDesignBatch:
             m.close()
 
 
-__all__ = ["FDTDDesign", "FDTDDesignBatch", "COEFF_NAMES"]
+__all__ = ["PackedModel", "FDTDDesign", "FDTDDesignBatch", "COEFF_NAMES"]

@@ -38,7 +38,8 @@ constexpr int kDftChunk = 256;  // steps between DFT accumulation passes
 constexpr int kMaxProbes = 1 << 20;
 constexpr int kMaxMonitors = 50;  // MAX_MONITORS, rfnetwork/core/inc/solver.h:15
 
-std::string g_error;
+// error text of the calls without a handle, kept per calling thread
+thread_local std::string g_error;
 
 struct CudaError {
   cudaError_t code;
@@ -1926,7 +1927,10 @@ int fdtd_nf2ff(const fdtd_nf2ff_face* faces, int n_faces, int n_freq, const floa
 // engine-built arrays besides the caller's data: the grid descriptor (SimDev)
 // and the tile list. The other entry points cudaMalloc them per simulation;
 // here they live in one file-scope device array of fixed size, so the call
-// allocates nothing on the device.
+// allocates nothing on the device. A set-up kernel writes both into the array
+// on the caller's stream from its launch parameters (the descriptor by value,
+// the tiles from the grid sizes), so the call leaves no host memory behind
+// that the GPU still has to read after it returns.
 namespace {
 
 constexpr int kNoallocMaxTiles = 65536;          // tile-list capacity (16 B per tile)
@@ -1940,7 +1944,20 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoallocScratch
 constexpr int kNoallocMaxDevices = 64;
 std::mutex g_noalloc_mutex;
 unsigned char* g_noalloc_ptr[kNoallocMaxDevices] = {};   // device address of the array, per device
-int4 g_noalloc_tiles[kNoallocMaxTiles];                  // host staging of the tile list
+
+// Writes the descriptor and the tile list of one call into the scratch array:
+// tiles of 31 x 7 columns in z chunks of zlen planes, x fastest, then y, then
+// the chunk (the plain kernel's tile order), as (0, x0 | y0 << 16, z0 | z1 << 16, 0).
+__global__ void noalloc_setup_kernel(SimDev d, int zlen, int n_tiles, unsigned char* scratch) {
+  if (blockIdx.x == 0 && threadIdx.x == 0) *reinterpret_cast<SimDev*>(scratch) = d;
+  int4* tiles = reinterpret_cast<int4*>(scratch + kNoallocDescBytes);
+  const int ntx = (d.nx + kTileX - 1) / kTileX, nty = (d.ny + kTileY - 1) / kTileY;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n_tiles; i += gridDim.x * blockDim.x) {
+    const int xt = i % ntx, yt = (i / ntx) % nty, zc = i / (ntx * nty);
+    const int x0 = xt * kTileX, y0 = yt * kTileY, z0 = zc * zlen, z1 = min(d.nz, z0 + zlen);
+    tiles[i] = make_int4(0, x0 | (y0 << 16), z0 | (z1 << 16), 0);
+  }
+}
 
 }  // namespace
 
@@ -1956,6 +1973,10 @@ extern "C" int fdtd_step_noalloc(const fdtd_device_grid* g, int n0, int n_steps,
   }
   if (g->nt < 1 || n0 < 0 || n_steps < 0 || int64_t(n0) + n_steps > g->nt) {
     g_error = "fdtd_step_noalloc: steps n0 .. n0+n_steps-1 must lie in [0, nt)";
+    return FDTD_ERR_ARG;
+  }
+  if (g->n_rows < 1 || g->n_rows > 65536 || g->n_probes < 0) {
+    g_error = "fdtd_step_noalloc: n_rows must be 1..65536 (a 16-bit index) and n_probes >= 0";
     return FDTD_ERR_ARG;
   }
   const size_t N = size_t(nz) * ny * pitch;
@@ -1975,23 +1996,27 @@ extern "C" int fdtd_step_noalloc(const fdtd_device_grid* g, int n0, int n_steps,
     g_error = "fdtd_step_noalloc: every buffer pointer must be a device address";
     return FDTD_ERR_ARG;
   }
-  if (reinterpret_cast<uintptr_t>(g->splits) % 8 != 0) {
-    g_error = "fdtd_step_noalloc: the splits buffer must be 8-byte aligned (it holds float pairs)";
+  if (reinterpret_cast<uintptr_t>(g->splits) % 8 != 0 || reinterpret_cast<uintptr_t>(g->rows) % 16 != 0 ||
+      reinterpret_cast<uintptr_t>(g->cell_probes) % 8 != 0) {
+    g_error = "fdtd_step_noalloc: splits and cell_probes must be 8-byte aligned, rows 16-byte aligned";
     return FDTD_ERR_ARG;
   }
   if (n_steps == 0) return FDTD_OK;
   try {
-    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
     int dev = 0;
     CK(cudaGetDevice(&dev));
     if (dev < 0 || dev >= kNoallocMaxDevices) throw ArgError{FDTD_ERR_LIMIT, "device ordinal out of range"};
-    if (!g_noalloc_ptr[dev]) {
-      // once per device: host code cannot name the array's device address directly
-      void* p = nullptr;
-      CK(cudaGetSymbolAddress(&p, g_noalloc_scratch));
-      g_noalloc_ptr[dev] = static_cast<unsigned char*>(p);
+    unsigned char* scratch = nullptr;
+    {
+      std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+      if (!g_noalloc_ptr[dev]) {
+        // once per device: host code cannot name the array's device address directly
+        void* p = nullptr;
+        CK(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+        g_noalloc_ptr[dev] = static_cast<unsigned char*>(p);
+      }
+      scratch = g_noalloc_ptr[dev];
     }
-    unsigned char* scratch = g_noalloc_ptr[dev];
     int n_sm = 148;
     CK(cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev));
     const int64_t want = int64_t(n_sm) * 8;
@@ -1999,13 +2024,7 @@ extern "C" int fdtd_step_noalloc(const fdtd_device_grid* g, int n0, int n_steps,
     chunks = std::min(chunks, std::max(1, nz / 8));
     chunks = int(std::min<int64_t>(chunks, kNoallocMaxTiles / xy_tiles));
     const int zlen = (nz + chunks - 1) / chunks;
-    int n_tiles = 0;
-    for (int z0 = 0; z0 < nz; z0 += zlen)
-      for (int y0 = 0; y0 < ny; y0 += kTileY)
-        for (int x0 = 0; x0 < nx; x0 += kTileX) {
-          const int z1 = std::min(nz, z0 + zlen);
-          g_noalloc_tiles[n_tiles++] = make_int4(0, x0 | (y0 << 16), z0 | (z1 << 16), 0);
-        }
+    const int n_tiles = int(xy_tiles) * ((nz + zlen - 1) / zlen);
     SimDev d{};
     d.nx = nx; d.ny = ny; d.nz = nz; d.pitch = pitch; d.plane = ny * pitch; d.nt = g->nt;
     for (int b = 0; b < 2; ++b) {
@@ -2026,11 +2045,8 @@ extern "C" int fdtd_step_noalloc(const fdtd_device_grid* g, int n0, int n_steps,
     d.is_src = g->is_src;
     d.cells = int64_t(N);
     cudaStream_t st = static_cast<cudaStream_t>(stream);
-    // both copies come from pageable host memory, so they are staged before
-    // they return and the host arrays may be refilled by the next call
-    CK(cudaMemcpyAsync(scratch, &d, sizeof(SimDev), cudaMemcpyHostToDevice, st));
-    CK(cudaMemcpyAsync(scratch + kNoallocDescBytes, g_noalloc_tiles, size_t(n_tiles) * sizeof(int4),
-                       cudaMemcpyHostToDevice, st));
+    noalloc_setup_kernel<<<std::min(1024, (n_tiles + 255) / 256), 256, 0, st>>>(d, zlen, n_tiles, scratch);
+    CK(cudaGetLastError());
     const SimDev* d_desc = reinterpret_cast<const SimDev*>(scratch);
     const int4* d_tiles = reinterpret_cast<const int4*>(scratch + kNoallocDescBytes);
     for (int n = n0; n < n0 + n_steps; ++n) {

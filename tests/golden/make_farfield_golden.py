@@ -1,14 +1,14 @@
 """Golden inputs of the far-field transform from the reference's own Python.
 
 Builds a small radiating model with PML on all six faces through
-rfnetwork/solver.py (the reference checkout, default /root/reference or
-$RFNETWORK_REF, with the stand-ins of make_setup_golden.py), adds the
+rfnetwork/solver.py (the reference checkout that make_setup_golden.py
+finds, with its stand-ins), adds the
 far-field monitor (rfnetwork/solver.py:1777-1891), "solves" it through the
 captured engine call, fills the far-field monitors with seeded random
 phasors, and records what get_farfield_rE (rfnetwork/solver.py:2870-3021)
 hands to core_func.nf2ff: the surface currents, cell positions and areas,
 face positions and the beta / theta / phi arrays. The fixture pins
-rfnetwork_b200.solver's far-field monitor setup and current assembly bit for
+modelgen.solver's far-field monitor setup and current assembly bit for
 bit; the transform itself is checked against oracle/nf2ff.py. A second
 fixture, farfield_gain.npz, holds the reference's get_farfield_gain
 (rfnetwork/solver.py:2804-2868) of a seeded far field, and dtft_small.npz the
@@ -23,7 +23,7 @@ import sys
 import numpy as np
 
 import make_setup_golden as mg
-from rfnetwork_b200 import geometry as geo
+from modelgen import geometry as geo
 
 FREQ = np.array([9e9, 14e9])
 THETA = np.linspace(0, 180, 7)

@@ -1,7 +1,8 @@
 """Generate golden setup fixtures from the reference's own Python setup code.
 
-Runs rfnetwork/solver.py from the reference checkout (default
-/root/reference, or $RFNETWORK_REF) in this container and records exactly what
+Runs rfnetwork/solver.py from the reference checkout (the location the
+oracle's build recipe uses: oracle/ref_cuda.py ``REF_ROOT``, which
+$RFN_REFERENCE_ROOT overrides) and records exactly what
 ``FDTD_Solver.solve()`` hands to the engine (the coefficient dict, probe list
 and monitor list of rfnetwork/solver.py:1473-1641), for the CPU and the GPU
 packing. The reference's third-party imports that are absent here
@@ -16,7 +17,7 @@ minimal stand-ins:
     distance are geometry code, not coefficient math).
 Everything else -- grid arrays, material averaging, coefficients, PML,
 conductors, lumped ports, probes, monitors, sources and packing -- is the
-reference code itself. The fixture pins ``rfnetwork_b200.solver`` bit-exactly.
+reference code itself. The fixture pins ``modelgen.solver`` bit-exactly.
 
 Usage:  python tests/golden/make_setup_golden.py [setup_small.npz] [setup_graded.npz] [setup_edge.npz]
         (needs the reference checkout; writes the named fixtures, default both)
@@ -32,10 +33,10 @@ from pathlib import Path
 import numpy as np
 
 HERE = Path(__file__).resolve().parent
-REF = Path(os.environ.get("RFNETWORK_REF", "/root/reference"))
 sys.path.insert(0, str(HERE.parent.parent))
+from oracle.ref_cuda import REF_ROOT as REF  # noqa: E402  (the one place that names the checkout)
 
-from rfnetwork_b200 import geometry as geo  # noqa: E402  (stand-in geometry shared with the mirror)
+from modelgen import geometry as geo  # noqa: E402  (stand-in geometry shared with the mirror)
 
 
 # --------------------------------------------------------------- stand-ins

@@ -9,7 +9,8 @@ import pytest
 
 import adjoint_model as am
 import kernel_model as km
-from rfnetwork_b200 import _lib, configs
+from modelgen import configs
+from rfnetwork_b200 import _lib
 
 
 def _setup():

@@ -4,7 +4,8 @@ arrays gives (host side, no GPU)."""
 import numpy as np
 import pytest
 
-from rfnetwork_b200 import _lib, configs
+from modelgen import configs
+from rfnetwork_b200 import _lib
 
 NAMES = (("Ca_ex_y", "Ca_ex_z", "Cb_ex_y", "Cb_ex_z"), ("Ca_ey_z", "Ca_ey_x", "Cb_ey_z", "Cb_ey_x"),
          ("Ca_ez_x", "Ca_ez_y", "Cb_ez_x", "Cb_ez_y"))

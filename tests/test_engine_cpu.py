@@ -9,9 +9,10 @@ import pytest
 import kernel_model as km
 import make_setup_golden as mg
 from helpers import rel_l2, run_oracle
-from rfnetwork_b200 import _lib, configs
-from rfnetwork_b200 import geometry as geo
-from rfnetwork_b200 import solver as S
+from modelgen import configs
+from rfnetwork_b200 import _lib
+from modelgen import geometry as geo
+from modelgen import solver as S
 from rfnetwork_b200.solver_constants import COEFF_NAMES
 
 HEADER = mg.HERE.parent.parent / "include" / "fdtd.h"

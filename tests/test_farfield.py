@@ -13,8 +13,8 @@ import make_farfield_golden as fg
 import make_setup_golden as mg
 from helpers import rel_l2
 from oracle import nf2ff as nf2ff_oracle
-from rfnetwork_b200 import geometry as geo
-from rfnetwork_b200 import solver as S
+from modelgen import geometry as geo
+from modelgen import solver as S
 
 GOLD = np.load(mg.HERE / "farfield_small.npz")
 

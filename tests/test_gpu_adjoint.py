@@ -11,7 +11,8 @@ import pytest
 import adjoint_model as am
 import kernel_model as km
 from helpers import rel_l2
-from rfnetwork_b200 import _lib, configs
+from modelgen import configs
+from rfnetwork_b200 import _lib
 
 pytestmark = pytest.mark.gpu
 

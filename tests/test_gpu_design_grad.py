@@ -17,7 +17,8 @@ import torch
 
 import adjoint_model as am
 import kernel_model as km
-from rfnetwork_b200 import _lib, configs
+from modelgen import configs
+from rfnetwork_b200 import _lib
 from rfnetwork_b200.adjoint import FDTDDesign
 
 pytestmark = pytest.mark.gpu

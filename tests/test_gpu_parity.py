@@ -20,9 +20,10 @@ import pytest
 
 import make_setup_golden as mg
 from helpers import derived_series, rel_l2, run_engine, run_oracle
-from rfnetwork_b200 import _lib, configs
-from rfnetwork_b200 import geometry as geo
-from rfnetwork_b200 import solver as S
+from modelgen import configs
+from rfnetwork_b200 import _lib
+from modelgen import geometry as geo
+from modelgen import solver as S
 
 pytestmark = pytest.mark.gpu
 
@@ -114,7 +115,7 @@ def test_device_dft_matches_numpy(engine_lib, small):
     # port series in float32 (solver.py:2482-2496) -- agreement to ~1e-6
     assert rel_l2(S_dev, S_np) < 1e-5
     names, X = se.dft["names"], se.dft["X"]
-    from rfnetwork_b200.solver import dtft
+    from modelgen.solver import dtft
     vp, ip = se.port_vi_series(0)
     Xv = dtft(vp.astype(np.float64), f, 1 / se.dt)
     assert rel_l2(X[names.index("V1")], Xv) < 1e-6

@@ -6,8 +6,8 @@ import pytest
 
 import make_setup_golden as mg
 from helpers import derived_series, rel_l2, run_oracle
-from rfnetwork_b200 import geometry as geo
-from rfnetwork_b200 import solver as S
+from modelgen import geometry as geo
+from modelgen import solver as S
 
 
 @pytest.fixture(scope="module")

@@ -15,7 +15,7 @@ import numpy as np
 import pytest
 
 from oracle import ref_cuda
-from rfnetwork_b200 import configs
+from modelgen import configs
 from helpers import rel_l2, run_engine, run_oracle
 
 pytestmark = [pytest.mark.gpu,

@@ -10,8 +10,8 @@ import numpy as np
 import pytest
 
 import make_setup_golden as mg
-from rfnetwork_b200 import geometry as geo
-from rfnetwork_b200 import solver as S
+from modelgen import geometry as geo
+from modelgen import solver as S
 
 
 @pytest.fixture(scope="module", params=sorted(mg.FIXTURES))

@@ -5,8 +5,10 @@ memory. A framework whose caching allocator owns the GPU memory, or a service
 with a fixed memory budget, needs every byte to come from its own pool; a
 cudaMalloc would escape that accounting, and a cudaFree waits for the whole
 device. The test plays such a caller: torch allocates every buffer, the
-entry point allocates nothing, and two calls in a row must reproduce what the
-ordinary entry point (fdtd_run) records for the same model.
+entry point allocates nothing (device memory in use and torch's reserved
+pool are unchanged across a call), and two calls in a row must reproduce, bit
+for bit, what the ordinary entry point (fdtd_run, with the same plain step
+kernel) records for the same model.
 
 This file is collected last, so a run that stops at the first failure has
 already run every other test.
@@ -18,7 +20,8 @@ import pytest
 
 import kernel_model as km
 from helpers import rel_l2
-from rfnetwork_b200 import _lib, configs
+from modelgen import configs
+from rfnetwork_b200 import _lib
 
 TOL = 1e-5
 
@@ -31,6 +34,7 @@ class DeviceGrid(ctypes.Structure):
         ("fields", ctypes.c_void_p), ("splits", ctypes.c_void_p), ("mat", ctypes.c_void_p),
         ("rows", ctypes.c_void_p), ("cell_probes", ctypes.c_void_p), ("src", ctypes.c_void_p),
         ("rec", ctypes.c_void_p), ("is_src", ctypes.c_void_p),
+        ("n_rows", ctypes.c_int), ("n_probes", ctypes.c_int),
     ]
 
 
@@ -51,14 +55,19 @@ def _cell_probes(probe_dicts, ny, nz):
 
 def test_rejects_bad_sizes_without_touching_the_gpu(engine_lib):
     fn = _entry(engine_lib)
-    g = DeviceGrid(nx=4000, ny=4000, nz=8, pitch=4000, nt=10)
+    g = DeviceGrid(nx=4000, ny=4000, nz=8, pitch=4000, nt=10, n_rows=1)
     assert fn(ctypes.byref(g), 0, 1, None) == 4           # FDTD_ERR_LIMIT: tile list over capacity
     assert b"tiles" in engine_lib.fdtd_global_error()
-    g = DeviceGrid(nx=16, ny=16, nz=8, pitch=16, nt=10)
+    g = DeviceGrid(nx=16, ny=16, nz=8, pitch=16, nt=10, n_rows=1)
     assert fn(ctypes.byref(g), 0, 1, None) == 1           # FDTD_ERR_ARG: no buffers
     assert fn(ctypes.byref(g), 5, 6, None) == 1           # steps beyond nt
     g.pitch = 8
     assert fn(ctypes.byref(g), 0, 1, None) == 1           # pitch < nx
+    g = DeviceGrid(nx=16, ny=16, nz=8, pitch=32, nt=10, n_rows=0)
+    assert fn(ctypes.byref(g), 0, 1, None) == 1           # no material rows
+    assert b"n_rows" in engine_lib.fdtd_global_error()
+    g.n_rows, g.n_probes = 70000, 0
+    assert fn(ctypes.byref(g), 0, 1, None) == 1           # more rows than a 16-bit index addresses
 
 
 @pytest.mark.gpu
@@ -69,8 +78,9 @@ def test_two_calls_match_fdtd_run(engine_lib):
     s = configs.microstrip(n=(40, 30, 26), n_pml=4, nt=160)
     co, pr, mo, mem, Nx, Ny, Nz, Nt = s.pack_inputs(gpu=True)
 
-    # the existing entry point on the same model
+    # the existing entry point on the same model, with the same (plain) step kernel
     sim = _lib.Simulation(Nx, Ny, Nz)
+    sim.set_kernel(0)
     sim.set_coefficients(co)
     for p in pr:
         sim.add_probe(p["field"], p["idx"], p["is_source"], p["values"][:Nt] if p["is_source"] else None)
@@ -103,19 +113,28 @@ def test_two_calls_match_fdtd_run(engine_lib):
         "rec": torch.zeros(P * Nt, dtype=torch.float32, device=dev),
         "is_src": torch.from_numpy(is_src).to(dev),
     }
-    g = DeviceGrid(nx=Nx, ny=Ny, nz=Nz, pitch=pitch, nt=Nt, **{k: v.data_ptr() for k, v in t.items()})
+    g = DeviceGrid(nx=Nx, ny=Ny, nz=Nz, pitch=pitch, nt=Nt, n_rows=rows.shape[0], n_probes=P,
+                   **{k: v.data_ptr() for k, v in t.items()})
     stream = torch.cuda.current_stream(dev).cuda_stream
 
+    def memory():
+        torch.cuda.synchronize(dev)
+        free, total = torch.cuda.mem_get_info(dev)
+        return total - free, torch.cuda.memory_reserved(dev)
+
     half = Nt // 2
-    # first call: steps 0 .. half-1
+    # first call: steps 0 .. half-1 (its set-up may load the library's kernels)
     assert fn(ctypes.byref(g), 0, half, ctypes.c_void_p(stream)) == 0, engine_lib.fdtd_global_error()
     torch.cuda.synchronize(dev)
     rec = t["rec"].cpu().numpy().reshape(P, Nt)
-    assert rel_l2(rec[:, :half], ref[:, :half]) <= TOL
+    np.testing.assert_array_equal(rec[:, :half], ref[:, :half])
     assert not rec[:, half:].any()
-    # second call continues the same grid: steps half .. Nt-1
+    # second call continues the same grid: steps half .. Nt-1, allocating nothing
+    before = memory()
     assert fn(ctypes.byref(g), half, Nt - half, ctypes.c_void_p(stream)) == 0, engine_lib.fdtd_global_error()
-    torch.cuda.synchronize(dev)
+    after = memory()
+    assert after == before, f"device memory in use / torch reserved changed: {before} -> {after}"
     rec = t["rec"].cpu().numpy().reshape(P, Nt)
+    np.testing.assert_array_equal(rec, ref)
     assert rel_l2(rec, ref) <= TOL
     assert np.isfinite(rec).all()
