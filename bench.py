@@ -18,6 +18,15 @@ compilation, host-to-device copies, the run and the read-back of probes and
 DFT inside the timed region). ``--impl reference`` times the CPU restatement
 of the reference's threaded C++ solver on the host cores instead.
 
+After the timed region, at N = 1, the line also carries its baselines and the
+other workloads: ``cpu_baseline`` (the CPU restatement on a bounded sample),
+``reference_cuda`` (the reference's own CUDA engine, solver.cu built from the
+reference's sources, on the same model and steps: the drop-in comparison,
+with the relative L2 difference of the two engines' probe series) and
+``workloads`` (one timed run each of the microstrip solve uniform and graded,
+the 64-simulation batch, the adjoint gradient and the design loop; each is also
+``--workload NAME`` on its own).
+
 With N > 1 (torchrun) every rank runs its own replica of the model (the
 solver has no cross-GPU exchange); ``value`` is the sum over ranks.
 """
@@ -63,6 +72,8 @@ def parse_args():
     ap.add_argument("--nt", type=int, default=NT, help="time steps per simulation")
     ap.add_argument("--e2e-steps", type=int, default=None, help="end-to-end calls timed (default: --steps)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-reference-cuda", action="store_true", help="skip the reference CUDA engine comparison")
+    ap.add_argument("--no-workloads", action="store_true", help="skip the other workloads after the timed region")
     ap.add_argument("--workload", choices=("boxes", "microstrip", "batch", "adjoint", "design"), default="boxes",
                     help="boxes: the bandwidth model (default); microstrip: the 64x64x48 microstrip with its "
                          "101-frequency S11/S21 (the case the reference runs on the CPU), solve time against the "
@@ -74,6 +85,15 @@ def parse_args():
 
 
 # --------------------------------------------------------------------- model
+
+def bench_config(nt: int, world: int, n_series: int, n_probes: int) -> dict:
+    """The workload's `config`, the same for both arms."""
+    cells = GRID[0] * GRID[1] * GRID[2]
+    return {"workload": WORKLOAD, "grid": list(GRID), "n_pml": N_PML, "time_steps": nt,
+            "dft_frequencies": N_FREQ, "dft_series": n_series, "probes": n_probes,
+            "l2": "inputs larger than L2 (fields+splits+index %.2f GB per replica)" % ((cells * (48 + 96) + cells * 2) / 1e9),
+            "parallelism": f"replicas{world}" if world > 1 else "single"}
+
 
 def build_model(nt: int):
     from modelgen import configs
@@ -279,6 +299,8 @@ def run_ours(args, rank, world, local_rank):
         e2e_s = max_over_ranks(time.perf_counter() - t0)
         info = cuda_func.last_run_info()
 
+    ctx = {"co": co, "pr": pr, "shape": (Nx, Ny, Nz), "nt": Nt, "rec": rec, "e2e_s": e2e_s / max(e2e_steps, 1),
+           "step_ms": statistics.fmean(per_sim_ms) / Nt}
     out = None
     if rank == 0:
         hbm, peak_kind = peaks()
@@ -293,13 +315,9 @@ def run_ours(args, rank, world, local_rank):
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic: seeded 64-box dielectric model (eps_r~U[1,10], sigma~U[0,0.05] S/m), "
                     "Gaussian-pulse ports",
-            "config": {"workload": WORKLOAD, "grid": list(GRID), "n_pml": N_PML, "time_steps": Nt,
-                       "dft_frequencies": N_FREQ, "dft_series": len(names), "probes": len(pr),
-                       "step": f"one full simulation ({Nt} Yee time steps)",
-                       "l2": "inputs larger than L2 (fields+splits+index %.2f GB per replica)"
-                             % ((cells * (48 + 96) + cells * 2) / 1e9),
-                       "parallelism": f"replicas{world}" if world > 1 else "single",
-                       "kernel": {k: st[k] for k in ("variant", "tile_y", "stages", "zchunk", "grid", "n_tiles")}},
+            "config": bench_config(Nt, world, len(names), len(pr)),
+            "step": f"one full simulation ({Nt} Yee time steps)",
+            "kernel": {k: st[k] for k in ("variant", "tile_y", "stages", "zchunk", "grid", "n_tiles")},
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s",
                          "frac": round(achieved / hbm, 4), "traffic": traffic,
                          "peak_source": peak_kind,
@@ -317,7 +335,7 @@ def run_ours(args, rank, world, local_rank):
             "finite": finite,
         }
     ranks.close()
-    return out
+    return out, ctx
 
 
 # ----------------------------------------------------------- CPU baseline
@@ -353,32 +371,125 @@ def cpu_baseline_entry():
 
 
 def run_reference(args, rank, world):
-    """CPU restatement of the reference's threaded C++ solver (solver.cpp), all usable host threads."""
+    """CPU restatement of the reference's threaded C++ solver (solver.cpp), all usable host threads.
+
+    Each step is a bounded sample of the workload (a few dozen time steps of the
+    full grid); ``ms_per_step`` is the measured wall time of one sample."""
     if rank != 0:
         return None
     from oracle import cpu_engine
+    from modelgen import configs
     n = cpu_engine.default_threads()
     for _ in range(max(args.warmup, 0)):
         cpu_sample(2, n)
     nt_sample = sample_steps(n)
-    vals = []
+    vals, secs = [], []
     for _ in range(args.steps):
-        v, _dt = cpu_sample(nt_sample, n)
+        v, dt = cpu_sample(nt_sample, n)
         vals.append(v)
+        secs.append(dt)
     value = statistics.fmean(vals)
-    cells = GRID[0] * GRID[1] * GRID[2]
+    s = build_model(2)
+    co, pr, *_ = s.pack_inputs(gpu=True)
+    names, _terms, _omega = dft_spec(s, pr)
     return {
         "impl": "reference", "metric": METRIC, "value": round(value, 2), "unit": UNIT, "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": round(cells * args.nt / (value * 1e6) * 1e3, 1),
+        "ms_per_step": round(statistics.fmean(secs) * 1e3, 1),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-        "data": "synthetic: seeded 64-box dielectric model, Gaussian-pulse ports",
-        "config": {"workload": WORKLOAD, "grid": list(GRID), "n_pml": N_PML, "time_steps": args.nt,
-                   "step": f"a sample of {nt_sample} time steps per step; ms_per_step extrapolated to {args.nt}"},
+        "data": "synthetic: seeded 64-box dielectric model (eps_r~U[1,10], sigma~U[0,0.05] S/m), "
+                "Gaussian-pulse ports",
+        "config": bench_config(args.nt, world, len(names), len(pr)),
+        "step": f"a sample of {nt_sample} time steps of the full grid (ms_per_step is its measured wall time)",
         "cpu_baseline": {"value": round(value, 2), "unit": UNIT, "cores": n, "kind": "port",
                          "sample": f"{nt_sample} time steps of the full grid per step"},
         "e2e": {"value": round(value, 2), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
+
+
+def reference_cuda_entry(ctx):
+    """The drop-in comparison: the reference's own CUDA engine (rfnetwork/core/src/solver.cu,
+    built unmodified from the reference's sources into oracle/_ref) on the same packed
+    model and the same number of steps, outside the timed region. Wall time of its
+    solver_run_cu (allocation, copies, four launches per step, read-back), its kernels'
+    device time per step from a CUPTI trace, and the relative L2 difference between its
+    probe series and this engine's end-to-end probe series."""
+    try:
+        from oracle import ref_cuda
+        if not ref_cuda.available():
+            return {"unavailable": "oracle/_ref/libref_cuda.so not built (needs the reference checkout at build time)"}
+        import torch
+        from torch.profiler import ProfilerActivity, profile
+        co, pr, (Nx, Ny, Nz), nt = ctx["co"], ctx["pr"], ctx["shape"], ctx["nt"]
+        mem = np.zeros(0, np.float32)
+        ref_cuda.solver_run_cu(co, copy.deepcopy(pr), [], mem, Nx, Ny, Nz, nt, 0, 0)  # warm-up
+        pr_ref = copy.deepcopy(pr)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        ref_cuda.solver_run_cu(co, pr_ref, [], mem, Nx, Ny, Nz, nt, 0, 0)
+        torch.cuda.synchronize()
+        wall = time.perf_counter() - t0
+        nt_prof = min(nt, 200)
+        with profile(activities=[ProfilerActivity.CUDA]) as prof:
+            ref_cuda.solver_run_cu(co, copy.deepcopy(pr), [], mem, Nx, Ny, Nz, nt_prof, 0, 0)
+        kern_us = sum(e.time_range.elapsed_us() for e in prof.events() if "update_kernel" in e.name)
+        ref_step_ms = kern_us / nt_prof / 1e3
+        ref_rec = np.stack([p["values"][:nt] for p in pr_ref])
+        ours = ctx["rec"]
+        rel = float(np.linalg.norm(ours - ref_rec) / np.linalg.norm(ref_rec))
+        cells = Nx * Ny * Nz
+        return {
+            "kind": "reference", "engine": "rfnetwork/core/src/solver.cu solver_run_cu, unmodified, sm_100a",
+            "time_steps": nt, "wall_s": round(wall, 3), "e2e_mcell_updates_per_s": round(cells * nt / wall / 1e6, 1),
+            "kernel_ms_per_step": round(ref_step_ms, 4),
+            "kernel_mcell_updates_per_s": round(cells / ref_step_ms / 1e3, 1),
+            "kernel_timing": f"CUPTI kernel trace (torch.profiler) over {nt_prof} steps",
+            "ours_e2e_s": round(ctx["e2e_s"], 3), "ours_step_ms": round(ctx["step_ms"], 4),
+            "e2e_speedup": round(wall / ctx["e2e_s"], 2), "step_speedup": round(ref_step_ms / ctx["step_ms"], 2),
+            "probe_rel_l2_vs_ours": rel,
+        }
+    except Exception as e:  # a baseline, not the measurement: report why it is missing
+        return {"unavailable": f"{type(e).__name__}: {e}"}
+
+
+def workloads_entry(args, local_rank):
+    """One timed run of each other workload (N = 1), summarised."""
+    import argparse as _ap
+    out = {}
+    base = dict(vars(args))
+    base.update(steps=1, warmup=1, nt=NT, no_cpu_baseline=True)
+
+    def ns(**kw):
+        d = dict(base)
+        d.update(kw)
+        return _ap.Namespace(**d)
+
+    def keep(line, keys):
+        return {k: line[k] for k in keys if k in line}
+
+    common = ("value", "unit", "ms_per_step", "e2e", "cpu_baseline", "gpu_launches")
+    for name, fn, kw, keys in (
+            ("microstrip", run_microstrip, dict(no_cpu_baseline=False), common),
+            ("microstrip_graded", run_microstrip, dict(graded=True), common),
+            ("batch", run_batch, {}, ("value", "unit", "ms_per_step", "sequential", "batched_over_sequential",
+                                      "sequential_plain_launches", "batched_over_sequential_plain_launches",
+                                      "mcell_updates_per_s", "bit_identical_to_sequential", "gpu_launches")),
+            ("adjoint", run_adjoint, {}, ("value", "unit", "ms_per_step", "forward_s", "gradient_over_forward",
+                                          "device", "recorded_history", "gpu_launches")),
+            ("design", run_design, {}, ("value", "unit", "ms_per_step", "device", "sequential",
+                                        "batched_over_sequential", "gpu_launches"))):
+        t0 = time.perf_counter()
+        try:
+            line = fn(ns(**kw), 0, 1, local_rank)
+            out[name] = dict(keep(line, keys), config=line["config"]["workload"] if "config" in line else None,
+                             wall_s=round(time.perf_counter() - t0, 1))
+        except Exception as e:
+            out[name] = {"error": f"{type(e).__name__}: {e}"}
+    u, g = out.get("microstrip", {}), out.get("microstrip_graded", {})
+    if "value" in u and "value" in g:
+        # cell-update throughput of the non-uniform mesh against the uniform one
+        g["mcell_rate_vs_uniform"] = round(g["value"] / u["value"], 3)
+    return out
 
 
 # ------------------------------------------------------ microstrip workload
@@ -396,7 +507,8 @@ def run_microstrip(args, rank, world, local_rank):
     torch.cuda.set_device(local_rank)
     ranks = RankSync(world, local_rank)
     nt = args.nt if args.nt != NT else 2000
-    s = configs.microstrip(nt=nt)
+    graded = bool(getattr(args, "graded", False))
+    s = configs.microstrip(nt=nt, graded=graded)
     f = configs.microstrip_frequencies()
     co, pr, mo, mem, Nx, Ny, Nz, Nt = s.pack_inputs(gpu=True)
     names, terms = s.dft_series()
@@ -443,7 +555,9 @@ def run_microstrip(args, rank, world, local_rank):
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(dev_ms, 3),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic: microstrip on a PEC ground plane, Gaussian-modulated port excitation",
-        "config": {"workload": f"microstrip 64x64x48, 10-cell PML, {Nt} steps, 2 ports, 101-freq S11/S21",
+        "config": {"workload": f"microstrip 64x64x48{' graded mesh (2-cell widths above the strip and '
+                               'towards the y sides)' if graded else ''}, 10-cell PML, {Nt} steps, 2 ports, "
+                               f"101-freq S11/S21", "grid": [Nx, Ny, Nz],
                    "cells": cells, "time_steps": Nt, "step": "one full solve",
                    "kernel": {k: st[k] for k in ("variant", "tile_y", "stages", "zchunk", "grid", "n_tiles")}},
         "e2e": {"value": round(world * cells * Nt / e2e_s / 1e6, 1), "unit": UNIT,
@@ -762,11 +876,15 @@ def main():
     elif args.workload == "design":
         out = run_design(args, rank, world, local_rank)
     else:
-        out = run_ours(args, rank, world, local_rank)
+        out, ctx = run_ours(args, rank, world, local_rank)
         if rank == 0 and world == 1 and not args.no_cpu_baseline:
             out["cpu_baseline"] = cpu_baseline_entry()
         elif rank == 0:
             out["cpu_baseline"] = None
+        if rank == 0 and world == 1 and not args.no_reference_cuda:
+            out["reference_cuda"] = reference_cuda_entry(ctx)
+        if rank == 0 and world == 1 and not args.no_workloads:
+            out["workloads"] = workloads_entry(args, local_rank)
     if rank == 0 and out is not None:
         print(json.dumps(out), flush=True)
 

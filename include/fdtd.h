@@ -38,7 +38,8 @@ extern "C" {
 #define FDTD_ERR_CUDA 2       /* CUDA runtime error */
 #define FDTD_ERR_STATE 3      /* call out of order (e.g. run before coefficients) */
 #define FDTD_ERR_LIMIT 4      /* a size limit was exceeded */
-#define FDTD_ERR_DEVICE 5     /* the kernel reported an error status */
+#define FDTD_ERR_DEVICE 5     /* the kernel reported an error status (a bounded wait expired) */
+#define FDTD_ERR_NONFINITE 6  /* the run diverged: a recorded probe value or a final field is NaN or infinite */
 
 typedef struct fdtd_sim fdtd_sim;
 typedef struct fdtd_batch fdtd_batch;
@@ -128,13 +129,16 @@ int fdtd_synchronize(fdtd_sim* s);
 
 /* Step-kernel selection: variant 0 = plain loads (1 cell per thread, 31 x 7
  * tiles), 1 = TMA streaming, one thread per cell (31 x tile_y tiles, tile_y in
- * {4, 6, 8, 12}). stages = shared-memory plane buffers. zchunk = z planes per
- * tile (0: derived from the grid). tile_y = 0 with variant 1 autotunes: the
- * first run times a few candidate (tile_y, stages, zchunk) shapes on the
- * simulation itself for a few steps and keeps the fastest, remembered per set
- * of grid sizes for the life of the process. The default comes from
- * RFN_FDTD_KERNEL (plain / stream) / RFN_FDTD_TY / RFN_FDTD_STAGES /
- * RFN_FDTD_ZCHUNK or is (1, 0, 4, 0): autotuned streaming.
+ * {4, 6, 8, 12}; stages = shared-memory plane buffers), 2 = TMA row marching,
+ * each warp walking `stages` rows of a 31 x tile_y tile ((tile_y, stages) in
+ * {(16, 4), (32, 4), (32, 8), (16, 8)}). zchunk = z planes per tile (0:
+ * derived from the grid). tile_y = 0 autotunes: the first run times a few
+ * candidate shapes on the simulation itself for a few steps and keeps the
+ * fastest, remembered per set of grid sizes for the life of the process --
+ * streaming and marching shapes with variant 1, marching shapes only with
+ * variant 2. The default comes from RFN_FDTD_KERNEL (plain / stream / march)
+ * / RFN_FDTD_TY / RFN_FDTD_STAGES / RFN_FDTD_ZCHUNK or is (1, 0, 4, 0):
+ * autotuned.
  * All variants give bit-identical results. The reference has one fixed 8x8x8
  * launch shape (solver.cu:549-557). */
 int fdtd_set_kernel(fdtd_sim* s, int variant, int tile_y, int stages, int zchunk);
@@ -146,6 +150,16 @@ int fdtd_set_stream(fdtd_sim* s, void* stream);
  * the default) or issue every launch from the host step by step (0), as the
  * reference's solver_run_cu does (rfnetwork/core/src/solver.cu:1005-1120). */
 int fdtd_set_graph(fdtd_sim* s, int enabled);
+
+/* Failure-path testing of the row-marching step kernel (variant 2), not for
+ * production runs. wait_limit: sleeping polls (each at most ~2 us) after
+ * which a shared-memory pipeline wait gives up (0 restores the default of
+ * 2^20, about 2 s); withhold_plane >= 0: every block's producer skips the
+ * loads of its plane number withhold_plane, so the waits for that plane
+ * expire and the run returns FDTD_ERR_DEVICE; -1 issues every plane. The
+ * next run captures its time loop again with these values. No counterpart
+ * in the reference, whose kernels have no bounded waits. */
+int fdtd_set_debug(fdtd_sim* s, unsigned wait_limit, int withhold_plane);
 
 /* Results of the last run. out: n_probes x nt floats, probe-major. */
 int fdtd_get_probe_values(fdtd_sim* s, float* out, int n_probes, int nt);

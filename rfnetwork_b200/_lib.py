@@ -12,7 +12,8 @@ import numpy as np
 
 LIB_PATH = Path(__file__).resolve().parent / "librfn_fdtd.so"
 
-FDTD_ERRORS = {1: "invalid argument", 2: "CUDA error", 3: "call out of order", 4: "size limit", 5: "device error"}
+FDTD_ERRORS = {1: "invalid argument", 2: "CUDA error", 3: "call out of order", 4: "size limit", 5: "device error",
+               6: "non-finite result"}
 
 EXPORTED = (
     "fdtd_create", "fdtd_set_coefficient", "fdtd_add_probe", "fdtd_add_monitor", "fdtd_set_dft",
@@ -23,7 +24,7 @@ EXPORTED = (
     "fdtd_batch_create", "fdtd_batch_run", "fdtd_batch_set_stream", "fdtd_batch_get_stats",
     "fdtd_batch_last_error", "fdtd_batch_destroy", "fdtd_global_error", "fdtd_step_noalloc",
     "fdtd_run_checkpointed", "fdtd_run_recorded", "fdtd_adjoint", "fdtd_batch_run_recorded",
-    "fdtd_batch_adjoint", "fdtd_set_graph", "fdtd_set_box_coefficients", "fdtd_nf2ff",
+    "fdtd_batch_adjoint", "fdtd_set_graph", "fdtd_set_box_coefficients", "fdtd_nf2ff", "fdtd_set_debug",
 )
 
 
@@ -79,6 +80,7 @@ def load():
         "fdtd_synchronize": ([vp], ip),
         "fdtd_set_stream": ([vp, vp], ip),
         "fdtd_set_graph": ([vp, ip], ip),
+        "fdtd_set_debug": ([vp, ctypes.c_uint, ip], ip),
         "fdtd_set_box_coefficients": ([vp, vp, vp], ip),
         "fdtd_nf2ff": ([vp, ip, ip, vp, ip, vp, ip, vp, vp], ip),
         "fdtd_get_probe_values": ([vp, vp, ip, ip], ip),
@@ -113,7 +115,11 @@ def _ptr(a: np.ndarray):
 
 
 class FdtdError(RuntimeError):
-    pass
+    """An engine call failed; ``code`` is its FDTD_ERR_* status (include/fdtd.h)."""
+
+    def __init__(self, msg: str, code: int = 0):
+        super().__init__(msg)
+        self.code = code
 
 
 def _dj_pairs(dJ_dX) -> np.ndarray:
@@ -151,7 +157,7 @@ class Simulation:
             msg = self.lib.fdtd_last_error(self.h).decode()
             if rc == 1:
                 raise ValueError(msg)
-            raise FdtdError(f"{FDTD_ERRORS.get(rc, rc)}: {msg}")
+            raise FdtdError(f"{FDTD_ERRORS.get(rc, rc)}: {msg}", rc)
 
     def set_coefficient(self, name: str, arr: np.ndarray, borrow: bool = False):
         """Copy the array into the engine, or with ``borrow`` lend it (no copy):
@@ -240,6 +246,12 @@ class Simulation:
     def set_graph(self, enabled: bool):
         """Replay the time loop as a CUDA graph (default) or launch every step from the host."""
         self._check(self.lib.fdtd_set_graph(self.h, int(bool(enabled))))
+
+    def set_debug(self, wait_limit: int = 0, withhold_plane: int = -1):
+        """Failure-path testing of the marching kernel: pipeline waits give up
+        after ``wait_limit`` polls (0: the default, about 2 s) and, with
+        ``withhold_plane`` >= 0, that plane's loads are never issued."""
+        self._check(self.lib.fdtd_set_debug(self.h, int(wait_limit), int(withhold_plane)))
 
     def run(self, nt: int):
         self._check(self.lib.fdtd_run(self.h, int(nt)))
@@ -342,7 +354,7 @@ class Batch:
             msg = self.lib.fdtd_batch_last_error(self.h).decode()
             if rc == 1:
                 raise ValueError(msg)
-            raise FdtdError(f"{FDTD_ERRORS.get(rc, rc)}: {msg}")
+            raise FdtdError(f"{FDTD_ERRORS.get(rc, rc)}: {msg}", rc)
 
     def run_recorded(self, nt: int, boxes):
         """Batched ``Simulation.run_recorded``: boxes[i] is member i's gradient box."""

@@ -28,6 +28,7 @@
 #include "fdtd_adjoint.cuh"
 #include "fdtd_nf2ff.cuh"
 #include "fdtd_step_stream.cuh"
+#include "fdtd_step_march.cuh"
 #include <cudaTypedefs.h>
 
 using namespace rfn;
@@ -131,26 +132,28 @@ int threads_for_host() {
 
 }  // namespace
 
-// Kernel selection of an engine: the plain-load kernel (one cell per thread)
-// or the TMA-pipelined kernel with its tile height, stage count and z chunk.
+// Kernel selection of an engine: the plain-load kernel (one cell per thread),
+// the TMA-pipelined streaming kernel (tile height, stage count) or the
+// row-marching kernel (tile height, rows per warp), and the z chunk.
 struct KernelConfig {
-  int variant = 1;  // 0 plain loads, 1 TMA streaming
-  int ty = 0;       // streaming tile height; 0: autotuned (ty, stages, zchunk) per set of grid sizes
-  int stages = 4;
+  int variant = 1;  // 0 plain loads, 1 TMA streaming, 2 TMA row marching
+  int ty = 0;       // tile height; 0 (with variant 1 or 2): autotuned (variant, ty, stages, zchunk)
+  int stages = 4;   // streaming: shared-memory stages; marching: rows per warp
   int zchunk = 0;   // 0: pick from the grid size
 };
 
-// Streaming-kernel shapes the autotuner times, and its choices per set of grid
-// sizes (process-wide).
-constexpr int kTuneCandidates[][3] = {{8, 4, 0}, {8, 4, 32}, {8, 3, 0}, {12, 3, 0}, {6, 3, 0}, {4, 4, 0},
-                                      {4, 4, 16}, {8, 4, 4}, {4, 4, 4}};
+// Step-kernel shapes the autotuner times, (variant, tile height, stages or
+// rows per warp, z chunk), and its choices per set of grid sizes (process-wide).
+constexpr int kTuneCandidates[][4] = {{2, 16, 4, 0}, {2, 32, 4, 0}, {2, 32, 8, 0}, {2, 16, 8, 0},
+                                      {2, 16, 4, 8}, {1, 8, 4, 0},  {1, 8, 4, 32}, {1, 8, 3, 0},
+                                      {1, 4, 4, 0},  {1, 4, 4, 16}, {1, 8, 4, 4},  {1, 4, 4, 4}};
 std::mutex g_tune_mutex;
-std::map<std::vector<int>, std::array<int, 3>> g_tune_cache;
+std::map<std::vector<int>, std::array<int, 4>> g_tune_cache;
 
 KernelConfig default_config() {
   KernelConfig c;
   if (const char* v = std::getenv("RFN_FDTD_KERNEL"))
-    c.variant = std::string(v) == "plain" ? 0 : 1;
+    c.variant = std::string(v) == "plain" ? 0 : std::string(v) == "march" ? 2 : 1;
   if (const char* v = std::getenv("RFN_FDTD_TY")) c.ty = std::atoi(v);
   if (const char* v = std::getenv("RFN_FDTD_STAGES")) c.stages = std::atoi(v);
   if (const char* v = std::getenv("RFN_FDTD_ZCHUNK")) c.zchunk = std::atoi(v);
@@ -199,6 +202,8 @@ struct fdtd_sim {
   std::unique_ptr<Engine> engine;  // batch of one for fdtd_run
   KernelConfig cfg = default_config();
   cudaStream_t ext_stream = nullptr;
+  uint32_t dbg_wait_limit = kStreamWaitLimit;  // fdtd_set_debug
+  int dbg_withhold = -1;
   std::string err;
   fdtd_stats stats{};
   int64_t h2d_bytes = 0, d2h_bytes = 0;  // bytes copied over PCIe/C2C by this simulation
@@ -288,10 +293,63 @@ const StreamVariant* find_stream_variant(int ty, int stages) {
   return nullptr;
 }
 
+using MarchKernelFn = void (*)(const SimDev*, const StreamTile*, int, int, unsigned*, unsigned, int*, int, int,
+                               uint32_t, int);
+
+// One instantiation of the row-marching step kernel: tile height XW*TY,
+// TY rows per warp, and the bytes of its plane and split slots.
+struct MarchVariant {
+  int rows, ty, threads;
+  uint32_t main_bytes, split_bytes;
+  MarchKernelFn fn;
+};
+
+template <int XW, int TY>
+MarchVariant march_variant() {
+  using G = MarchGeom<XW, TY>;
+  return MarchVariant{G::ROWS, TY, G::THREADS, G::MAIN, G::SPLIT, &fdtd_step_march_kernel<XW, TY>};
+}
+
+const std::vector<MarchVariant>& march_variants() {
+  static const std::vector<MarchVariant> v = {march_variant<4, 4>(), march_variant<8, 4>(), march_variant<4, 8>(),
+                                              march_variant<2, 8>()};
+  return v;
+}
+
+const MarchVariant* find_march_variant(int rows, int ty) {
+  for (auto& v : march_variants())
+    if (v.rows == rows && v.ty == ty) return &v;
+  return nullptr;
+}
+
+// Plane and split slots of a marching block: as many blocks per SM as its
+// registers allow (at most two), each block's shared memory split into
+// plane slots (at least three: the plane, its look-ahead and one load in
+// flight) and split slots (at least two). Returns the dynamic shared bytes.
+uint32_t march_slots(const MarchVariant& v, int* n_main, int* n_split) {
+  constexpr uint32_t kSmemPerSm = 233472, kPerBlockReserve = 1024 + 512, kMaxPerBlock = 232448 - 512;
+  cudaFuncAttributes fa{};
+  CK(cudaFuncGetAttributes(&fa, reinterpret_cast<const void*>(v.fn)));
+  const int regs_per_block = ((fa.numRegs * 32 + 255) / 256 * 256) * (v.threads / 32);
+  int bps = std::max(1, std::min(2, 65536 / std::max(regs_per_block, 1)));
+  for (; bps >= 1; --bps) {
+    const uint32_t budget = std::min(kSmemPerSm / bps - kPerBlockReserve, kMaxPerBlock);
+    if (budget < 3 * v.main_bytes + 2 * v.split_bytes) continue;
+    uint32_t m = std::min<uint32_t>(6, (budget - 2 * v.split_bytes) / v.main_bytes);
+    const uint32_t sp = std::min<uint32_t>(kMarchSplitSlots, (budget - m * v.main_bytes) / v.split_bytes);
+    m = std::min<uint32_t>(kMarchSlots, (budget - sp * v.split_bytes) / v.main_bytes);
+    *n_main = int(m);
+    *n_split = int(sp);
+    return m * v.main_bytes + sp * v.split_bytes;
+  }
+  throw ArgError{FDTD_ERR_LIMIT, "Marching kernel's plane slots do not fit in shared memory."};
+}
+
 // Whether a (variant, tile height, stages) triple names an instantiated kernel.
 bool kernel_exists(int variant, int ty, int stages) {
   if (variant == 0) return true;
   if (variant == 1) return ty == 0 || find_stream_variant(ty, stages) != nullptr;
+  if (variant == 2) return ty == 0 || find_march_variant(ty, stages) != nullptr;
   return false;
 }
 
@@ -341,9 +399,12 @@ void encode_stream_maps(StreamMaps& m, const fdtd_sim* s, int ty) {
   encode_map(&m.ids, s->mat.p, CU_TENSOR_MAP_DATA_TYPE_UINT16, 2, s, 3, 40, ty + 1, 1, 0, 0);
 }
 
-// Everything one launch of the streaming kernel needs.
+// Everything one launch of the streaming or the marching kernel needs.
 struct StreamClass {
   const StreamVariant* v = nullptr;
+  const MarchVariant* mv = nullptr;  // the marching kernel (v is then null)
+  uint32_t ring = 0;                 // its dynamic shared bytes: plane slots, then split slots
+  int n_main = 0, n_split = 0;
   std::vector<StreamTile> host_tiles;
   std::vector<StreamMaps> host_maps;
   DevBuf<StreamMaps> d_maps;
@@ -353,6 +414,8 @@ struct StreamClass {
   int n_tiles = 0, grid = 0;
   void reset() {
     v = nullptr;
+    mv = nullptr;
+    ring = 0;
     host_tiles.clear();
     host_maps.clear();
     d_maps.free();
@@ -382,6 +445,8 @@ struct Engine {
   cudaEvent_t cap_fork = nullptr, cap_join = nullptr;
   int64_t step_launches = 0, dft_launches = 0, adj_launches = 0;
   double adj_ms = 0;
+  uint32_t wait_limit = kStreamWaitLimit;  // polls per mbarrier wait of the marching kernel
+  int withhold = -1;                       // test hook: plane the marching kernel's producers never issue
   bool use_graph = true;  // replay the time loop as a captured CUDA graph
   double last_ms = 0;
   bool timing_pending = false;
@@ -421,7 +486,7 @@ struct Engine {
       d_err.alloc(1);
       CK(cudaMemset(d_err.p, 0, sizeof(int)));
     }
-    if (cfg.variant == 1) {
+    if (cfg.variant == 1 || cfg.variant == 2) {
       if (cfg.ty == 0)
         autotune(n_sm);
       else
@@ -465,38 +530,45 @@ struct Engine {
     return tiles;
   }
 
-  // Picks the streaming kernel's (tile height, stages, z chunk) for this set
-  // of grids: each candidate runs a few time steps on the simulations
-  // themselves (their fields are cleared again by the next run), the fastest
-  // is kept and remembered for the same grid sizes.
+  // Picks the step kernel's (variant, tile height, stages or rows per warp,
+  // z chunk) for this set of grids: each candidate runs a few time steps on
+  // the simulations themselves (their fields are cleared again by the next
+  // run), the fastest is kept and remembered for the same grid sizes. With
+  // variant 2 requested only the marching shapes are timed.
   void autotune(int n_sm) {
     std::vector<int> key;
     int nt_min = 1 << 30;
+    const bool march_only = cfg.variant == 2;
+    key.push_back(march_only ? 2 : 1);
     for (auto* s : sims) {
       key.insert(key.end(), {s->nx, s->ny, s->nz});
       nt_min = std::min(nt_min, s->prepared_nt);
     }
+    auto apply = [&](const std::array<int, 4>& c) {
+      cfg.variant = c[0];
+      cfg.ty = c[1];
+      cfg.stages = c[2];
+      cfg.zchunk = c[3];
+    };
     {
       std::lock_guard<std::mutex> lock(g_tune_mutex);
       auto it = g_tune_cache.find(key);
       if (it != g_tune_cache.end()) {
-        cfg.ty = it->second[0];
-        cfg.stages = it->second[1];
-        cfg.zchunk = it->second[2];
+        apply(it->second);
         build_stream_tiles(n_sm);
         return;
       }
     }
     const int warm = 2, timed = std::min(8, nt_min - warm);
-    std::array<int, 3> best = {kTuneCandidates[0][0], kTuneCandidates[0][1], kTuneCandidates[0][2]};
+    std::array<int, 4> best = {kTuneCandidates[0][0], kTuneCandidates[0][1], kTuneCandidates[0][2],
+                               kTuneCandidates[0][3]};
     if (timed >= 2) {
       init();
       cudaStream_t st = stream();
       float best_ms = 1e30f;
       for (const auto& cand : kTuneCandidates) {
-        cfg.ty = cand[0];
-        cfg.stages = cand[1];
-        cfg.zchunk = cand[2];
+        if (march_only && cand[0] != 2) continue;
+        apply({cand[0], cand[1], cand[2], cand[3]});
         build_stream_tiles(n_sm);
         CK(cudaMemsetAsync(scls.d_counter.p, 0, sizeof(unsigned), st));
         for (int n = 0; n < warm; ++n) launch_step(st, n);
@@ -508,7 +580,7 @@ struct Engine {
         CK(cudaEventElapsedTime(&ms, ev0, ev1));
         if (ms < best_ms) {
           best_ms = ms;
-          best = {cand[0], cand[1], cand[2]};
+          best = {cand[0], cand[1], cand[2], cand[3]};
         }
       }
       check_error();
@@ -517,25 +589,38 @@ struct Engine {
       std::lock_guard<std::mutex> lock(g_tune_mutex);
       g_tune_cache[key] = best;
     }
-    cfg.ty = best[0];
-    cfg.stages = best[1];
-    cfg.zchunk = best[2];
+    apply(best);
     build_stream_tiles(n_sm);
   }
 
-  // Streaming kernel: 31 x TY column tiles cut in z chunks of at most 62
-  // planes, each with the mask of its planes that hold split-field cells.
+  // Streaming and marching kernels: 31 x TY column tiles cut in z chunks of
+  // at most 62 planes, each with the mask of its planes that hold split-field
+  // cells (TY: the tile height).
   void build_stream_tiles(int n_sm) {
     StreamClass& c = scls;
     c.reset();
-    c.v = find_stream_variant(cfg.ty, cfg.stages);
-    if (!c.v) throw ArgError{FDTD_ERR_ARG, "No streaming kernel instantiated for this tile height / stage count."};
-    const StreamVariant& v = *c.v;
-    CK(cudaFuncSetAttribute(reinterpret_cast<const void*>(v.fn), cudaFuncAttributeMaxDynamicSharedMemorySize, v.smem));
+    const void* fn = nullptr;
+    int threads = 0, smem = 0, ty = 0;
+    if (cfg.variant == 2) {
+      c.mv = find_march_variant(cfg.ty, cfg.stages);
+      if (!c.mv) throw ArgError{FDTD_ERR_ARG, "No marching kernel instantiated for this tile height / rows per warp."};
+      c.ring = march_slots(*c.mv, &c.n_main, &c.n_split);
+      fn = reinterpret_cast<const void*>(c.mv->fn);
+      threads = c.mv->threads;
+      smem = int(c.ring);
+      ty = c.mv->rows;
+    } else {
+      c.v = find_stream_variant(cfg.ty, cfg.stages);
+      if (!c.v) throw ArgError{FDTD_ERR_ARG, "No streaming kernel instantiated for this tile height / stage count."};
+      fn = reinterpret_cast<const void*>(c.v->fn);
+      threads = c.v->threads;
+      smem = c.v->smem;
+      ty = c.v->ty;
+    }
+    CK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     int per_sm = 0;
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, reinterpret_cast<const void*>(v.fn), v.threads, v.smem));
-    if (per_sm < 1) throw ArgError{FDTD_ERR_LIMIT, "Streaming kernel does not fit on an SM."};
-    const int ty = v.ty;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, threads, smem));
+    if (per_sm < 1) throw ArgError{FDTD_ERR_LIMIT, "Step kernel does not fit on an SM."};
     int64_t cols = 0;
     for (auto* s : sims) cols += int64_t((s->nx + kStreamOwnX - 1) / kStreamOwnX) * ((s->ny + ty - 1) / ty);
     const int64_t slots = int64_t(per_sm) * n_sm;
@@ -628,11 +713,15 @@ struct Engine {
   }
 
   void launch_step(cudaStream_t st, int n) {
-    if (cfg.variant == 1) {
+    if (cfg.variant == 1 || cfg.variant == 2) {
       StreamClass& c = scls;
       const unsigned base = unsigned(n) * unsigned(c.n_tiles + c.grid);
-      c.v->fn<<<c.grid, c.v->threads, c.v->smem, st>>>(c.d_sims.p, c.d_tiles.p, c.n_tiles, n, c.d_counter.p, base,
-                                                        d_err.p);
+      if (c.mv)
+        c.mv->fn<<<c.grid, c.mv->threads, c.ring, st>>>(c.d_sims.p, c.d_tiles.p, c.n_tiles, n, c.d_counter.p, base,
+                                                         d_err.p, c.n_main, c.n_split, wait_limit, withhold);
+      else
+        c.v->fn<<<c.grid, c.v->threads, c.v->smem, st>>>(c.d_sims.p, c.d_tiles.p, c.n_tiles, n, c.d_counter.p, base,
+                                                          d_err.p);
       CK(cudaGetLastError());
     } else {
       fdtd_step_kernel<kTileY><<<n_tiles, dim3(32, kBlockY), 0, st>>>(d_sims.p, d_tiles.p, n);
@@ -820,7 +909,7 @@ struct Engine {
             CK(cudaMemcpyAsync(s->splits.p + b * 12 * N, src + 6 * N, 12 * N * sizeof(float),
                                cudaMemcpyDeviceToDevice, st));
         }
-        if (cfg.variant == 1) {
+        if (cfg.variant == 1 || cfg.variant == 2) {
           // the streaming kernel's tile counter as it stood before step n0
           const unsigned c0 = unsigned(n0) * unsigned(scls.n_tiles + scls.grid);
           CK(cudaMemcpyAsync(scls.d_counter.p, &c0, sizeof(unsigned), cudaMemcpyHostToDevice, st));
@@ -906,6 +995,18 @@ struct Engine {
         dft_from = n + 1;
       }
     }
+    // sentinel: a diverged run ends with non-finite records or fields
+    for (auto* s : sims) {
+      const int64_t nrec = int64_t(s->probes.size()) * nt;
+      if (nrec > 0) {
+        nonfinite_check_kernel<<<int(std::min<int64_t>(256, (nrec + 255) / 256)), 256, 0, st>>>(s->rec.p, nrec,
+                                                                                              d_err.p);
+        CK(cudaGetLastError());
+      }
+      const size_t b = size_t(nt & 1) * 6 * s->cells_padded;  // buffer the last step wrote
+      nonfinite_check_kernel<<<296, 256, 0, st>>>(s->fields.p + b, int64_t(6 * s->cells_padded), d_err.p);
+      CK(cudaGetLastError());
+    }
   }
 
   void run_async(int nt) {
@@ -960,13 +1061,16 @@ struct Engine {
     check_error();
   }
 
-  // Reads (and clears) the error code the step kernel records when a bounded wait expires.
+  // Reads (and clears) the error code the kernels record: a bounded wait that
+  // expired, or the end-of-run sentinel's non-finite value.
   void check_error() {
     if (!d_err.n) return;
     int e = 0;
     CK(cudaMemcpy(&e, d_err.p, sizeof(int), cudaMemcpyDeviceToHost));
     if (e) {
       CK(cudaMemset(d_err.p, 0, sizeof(int)));
+      if (e == kErrNonFinite)
+        throw ArgError{FDTD_ERR_NONFINITE, "the run diverged: a probe record or a field value is not finite"};
       throw ArgError{FDTD_ERR_DEVICE, "step kernel gave up waiting for a TMA plane load (code " +
                                           std::to_string(e) + ")"};
     }
@@ -1171,6 +1275,8 @@ void new_engine(fdtd_sim* s) {
   s->engine->cfg = s->cfg;
   s->engine->ext_stream = s->ext_stream;
   s->engine->use_graph = s->use_graph;
+  s->engine->wait_limit = s->dbg_wait_limit;
+  s->engine->withhold = s->dbg_withhold;
   s->engine->build_tiles();
 }
 
@@ -1501,7 +1607,8 @@ int fdtd_get_material_table(fdtd_sim* s, uint16_t* ids, int64_t n_ids, uint32_t*
 int fdtd_set_kernel(fdtd_sim* s, int variant, int tile_y, int stages, int zchunk) {
   if (!s) return FDTD_ERR_ARG;
   return guarded(&s->err, [&] {
-    if (variant < 0 || variant > 1) throw ArgError{FDTD_ERR_ARG, "variant must be 0 (plain) or 1 (stream)"};
+    if (variant < 0 || variant > 2)
+      throw ArgError{FDTD_ERR_ARG, "variant must be 0 (plain), 1 (stream) or 2 (march)"};
     if (!kernel_exists(variant, tile_y, stages))
       throw ArgError{FDTD_ERR_ARG, "No kernel instantiated for this variant / tile height / stage count."};
     KernelConfig c;
@@ -1519,6 +1626,18 @@ int fdtd_set_graph(fdtd_sim* s, int enabled) {
   s->use_graph = enabled != 0;
   if (s->engine) {
     s->engine->use_graph = s->use_graph;
+    s->engine->reset_graph();
+  }
+  return FDTD_OK;
+}
+
+int fdtd_set_debug(fdtd_sim* s, unsigned wait_limit, int withhold_plane) {
+  if (!s) return FDTD_ERR_ARG;
+  s->dbg_wait_limit = wait_limit ? wait_limit : kStreamWaitLimit;
+  s->dbg_withhold = withhold_plane < 0 ? -1 : withhold_plane;
+  if (s->engine) {
+    s->engine->wait_limit = s->dbg_wait_limit;
+    s->engine->withhold = s->dbg_withhold;
     s->engine->reset_graph();
   }
   return FDTD_OK;
@@ -1707,7 +1826,8 @@ int fdtd_batch_create(fdtd_sim* const* sims, int n_sims, fdtd_batch** out) {
 int fdtd_batch_set_kernel(fdtd_batch* b, int variant, int tile_y, int stages, int zchunk) {
   if (!b) return FDTD_ERR_ARG;
   return guarded(&b->err, [&] {
-    if (variant < 0 || variant > 1) throw ArgError{FDTD_ERR_ARG, "variant must be 0 (plain) or 1 (stream)"};
+    if (variant < 0 || variant > 2)
+      throw ArgError{FDTD_ERR_ARG, "variant must be 0 (plain), 1 (stream) or 2 (march)"};
     if (!kernel_exists(variant, tile_y, stages))
       throw ArgError{FDTD_ERR_ARG, "No kernel instantiated for this variant / tile height / stage count."};
     b->engine.cfg.variant = variant;

@@ -324,6 +324,19 @@ fdtd_step_kernel(const SimDev* __restrict__ sims, const int4* __restrict__ tiles
   }
 }
 
+// Error codes the kernels record in the engine's error word.
+constexpr int kErrWaitExpired = 1;  // a bounded pipeline wait gave up
+constexpr int kErrNonFinite = 2;    // a probe record or a final field value is NaN or infinite
+
+// Run sentinel: records kErrNonFinite when any of n floats is NaN or
+// infinite (a diverged run), checked once after the last step.
+__global__ void nonfinite_check_kernel(const float* __restrict__ v, int64_t n, int* __restrict__ err) {
+  bool bad = false;
+  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x)
+    bad |= !isfinite(__ldg(v + i));
+  if (__syncthreads_or(bad) && threadIdx.x == 0) atomicCAS(err, 0, kErrNonFinite);
+}
+
 // Ids arrive in the reference order [x][y][z]; the kernels read [z][y][pitch].
 __global__ void transpose_ids_kernel(const uint16_t* __restrict__ in, uint16_t* __restrict__ out, int nx, int ny,
                                      int nz, int pitch) {

@@ -49,7 +49,6 @@ namespace rfn {
 
 constexpr int kStreamOwnX = 31;           // owned columns per tile (lane 0 is the halo column)
 constexpr uint32_t kStreamWaitLimit = 1u << 20;  // sleeping polls (each <= 2 us) per wait
-constexpr int kStreamErrTimeout = 1;
 constexpr int kStreamBar = 1;             // named barrier of the consumer warps
 
 constexpr int kStreamWin = 16;            // columns of a narrow split window
@@ -244,7 +243,7 @@ fdtd_step_stream_kernel(const SimDev* __restrict__ sims, const StreamTile* __res
       ++k;
     }
     if (failed) {
-      atomicExch(err, kStreamErrTimeout);
+      atomicExch(err, kErrWaitExpired);
       // drain the loads still in flight (bounded)
       for (uint32_t r = q > uint32_t(S) ? q - S : 0; r < q; ++r)
         mbar_wait_bounded(&full[r % S], (r / S) & 1u, kStreamWaitLimit);
@@ -262,7 +261,7 @@ fdtd_step_stream_kernel(const SimDev* __restrict__ sims, const StreamTile* __res
   for (int k = 0;; ++k) {
     bool ok = mbar_wait_bounded(&full[sq], pq, kStreamWaitLimit);
     if (named_bar_or(kStreamBar, NC, !ok)) {
-      if (tid == 0) atomicExch(err, kStreamErrTimeout);
+      if (tid == 0) atomicExch(err, kErrWaitExpired);
       return;
     }
     const int ti = s_tq[k & 3];
@@ -389,7 +388,7 @@ fdtd_step_stream_kernel(const SimDev* __restrict__ sims, const StreamTile* __res
         const float ez_xm = __shfl_up_sync(0xffffffffu, ez, 1);
         // E^{n+1}(z) of the block complete; a consumer whose wait expired votes here
         if (named_bar_or(kStreamBar, NC, !ok)) {
-          if (tid == 0) atomicExch(err, kStreamErrTimeout);
+          if (tid == 0) atomicExch(err, kErrWaitExpired);
           return false;
         }
 

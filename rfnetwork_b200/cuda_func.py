@@ -15,13 +15,17 @@ bounds; ``is_source`` is honoured as a flag (the reference tests only that the
 key exists, rfnetwork/core/src/solver.cpp:528, which makes no difference for
 the zero-valued non-source probes that ``solve()`` builds); each phasor
 monitor uses its own ``dtft_phase`` table (the reference GPU path reuses the
-last monitor's, solver.cu:842-878).
+last monitor's, solver.cu:842-878). A run that diverges writes its (NaN or
+infinite) results in place as the reference does, and also emits a
+``RuntimeWarning`` (the engine's end-of-run sentinel, FDTD_ERR_NONFINITE).
 """
 from __future__ import annotations
 
+import warnings
+
 import numpy as np
 
-from ._lib import Simulation
+from ._lib import FdtdError, Simulation
 from .solver_constants import COEFF_NAMES
 
 _last_info = {}
@@ -106,7 +110,12 @@ def _run(coefficients, probes, monitors, Nx, Ny, Nz, Nt, terms=None, omega=None)
                 sim.add_monitor(int(m["field"]), int(m["axis"]), int(m["position"]), int(m["n_step"]))
         if terms is not None:
             sim.set_dft(terms, omega)
-        sim.run(Nt)
+        try:
+            sim.run(Nt)
+        except FdtdError as e:
+            if e.code != 6:  # FDTD_ERR_NONFINITE: the results are complete, only not finite
+                raise
+            warnings.warn(f"FDTD run diverged: {e}", RuntimeWarning, stacklevel=3)
         if probes:
             rec = sim.probe_values()
             for p, r in zip(probes, rec):

@@ -47,12 +47,13 @@ def test_ragged_grids_stream_equals_plain(engine_lib, shape):
     ref = plain.probe_values()
     plain.close()
     assert np.isfinite(ref).all() and np.abs(ref).max() > 0
-    for ty, stages, zchunk in ((8, 4, 0), (4, 5, 1), (6, 3, 2)):
-        sim = _random_sim(shape, 1, nt, 1, tile_y=ty, stages=stages, zchunk=zchunk)
+    for variant, ty, stages, zchunk in ((1, 8, 4, 0), (1, 4, 5, 1), (1, 6, 3, 2), (2, 16, 4, 0), (2, 32, 8, 1),
+                                        (2, 16, 8, 2), (2, 32, 4, 3)):
+        sim = _random_sim(shape, 1, nt, variant, tile_y=ty, stages=stages, zchunk=zchunk)
         sim.run(nt)
         got = sim.probe_values()
         sim.close()
-        assert np.array_equal(got, ref), (shape, ty, stages, zchunk)
+        assert np.array_equal(got, ref), (shape, variant, ty, stages, zchunk)
 
 
 def test_run_without_probes_and_one_step(engine_lib):
@@ -69,7 +70,8 @@ def test_run_without_probes_and_one_step(engine_lib):
     b.close()
 
 
-def test_batch_of_tiny_grids_equals_single_runs(engine_lib):
+@pytest.mark.parametrize("kernel", [(1, 8, 4, 0), (2, 16, 4, 0)])
+def test_batch_of_tiny_grids_equals_single_runs(engine_lib, kernel):
     """A batch whose members are smaller than one tile or leave ragged tiles
     gives each member the bits of its own run."""
     shapes = [(2, 2, 2), (3, 5, 2), (33, 9, 5), (40, 17, 3), (31, 8, 27)]
@@ -82,7 +84,7 @@ def test_batch_of_tiny_grids_equals_single_runs(engine_lib):
         sim.close()
     sims = [_random_sim(shape, 10 + k, nt, 1) for k, shape in enumerate(shapes)]
     batch = _lib.Batch(sims)
-    batch.set_kernel(1, 8, 4, 0)
+    batch.set_kernel(*kernel)
     batch.run(nt)
     for sim, ref in zip(sims, singles):
         assert np.array_equal(sim.probe_values(), ref)
