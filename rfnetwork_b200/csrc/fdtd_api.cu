@@ -29,6 +29,7 @@
 #include "fdtd_nf2ff.cuh"
 #include "fdtd_step_stream.cuh"
 #include "fdtd_step_march.cuh"
+#include "fdtd_adjoint_march.cuh"
 #include <cudaTypedefs.h>
 
 using namespace rfn;
@@ -343,6 +344,17 @@ uint32_t march_slots(const MarchVariant& v, int* n_main, int* n_split) {
     return m * v.main_bytes + sp * v.split_bytes;
   }
   throw ArgError{FDTD_ERR_LIMIT, "Marching kernel's plane slots do not fit in shared memory."};
+}
+
+// The marching reverse step: tile height and rows per warp of the instantiation used.
+constexpr int kAdjMarchXW = 4, kAdjMarchTY = 4;
+using AdjGeom = AdjMarchGeom<kAdjMarchXW, kAdjMarchTY>;
+
+// Plane and split slots of a marching reverse-step block, as march_slots.
+uint32_t adj_march_slots(int* n_main, int* n_split) {
+  MarchVariant v{AdjGeom::ROWS, kAdjMarchTY, AdjGeom::THREADS, AdjGeom::MAIN, AdjGeom::SPLIT,
+                 reinterpret_cast<MarchKernelFn>(&adj_march_kernel<kAdjMarchXW, kAdjMarchTY>)};
+  return march_slots(v, n_main, n_split);
 }
 
 // Whether a (variant, tile height, stages) triple names an instantiated kernel.
@@ -765,6 +777,62 @@ struct Engine {
   DevBuf<AdjSim> adj_d_as;
   DevBuf<int4> adj_d_t;
   DevBuf<CapSim> adj_d_c;
+  // marching reverse step: tensor maps per request, tiles, tile counter
+  DevBuf<AdjMaps> adj_d_maps;
+  DevBuf<StreamTile> adj_d_mtiles;
+  DevBuf<unsigned> adj_d_counter;
+
+  // Tiles of the marching reverse step: 30 x ROWS columns in z chunks, each
+  // with the mask of its planes z0-1 .. z1 that hold split cells in its
+  // boxes (columns x0-1 .. x0+30, rows y0-1 .. y0+ROWS).
+  std::vector<StreamTile> adj_march_tiles(const std::vector<fdtd_sim*>& ss, int64_t slots) {
+    constexpr int R = AdjGeom::ROWS, TX = kAdjMarchOwnX;
+    int64_t cols = 0;
+    for (auto* s : ss) cols += int64_t((s->nx + TX - 1) / TX) * ((s->ny + R - 1) / R);
+    std::vector<StreamTile> tiles;
+    for (size_t i = 0; i < ss.size(); ++i) {
+      fdtd_sim* s = ss[i];
+      const int64_t chunks = std::max<int64_t>(1, (slots * 4 + cols - 1) / std::max<int64_t>(cols, 1));
+      const int zc = std::max(1, std::min(62, int((s->nz + chunks - 1) / chunks)));
+      const GradedIndex split_idx(s->grid, kFlagESplit | kFlagHSplit);
+      for (int z0 = 0; z0 < s->nz; z0 += zc)
+        for (int y0 = 0; y0 < s->ny; y0 += R)
+          for (int x0 = 0; x0 < s->nx; x0 += TX) {
+            const int z1 = std::min(s->nz, z0 + zc);
+            uint64_t mask = 0;
+            for (int j = 0; j <= z1 - z0 + 1; ++j) {
+              const int z = z0 - 1 + j;
+              if (z < 0 || z >= s->nz) continue;
+              if (split_idx.count(x0 - 1, x0 + TX + 1, y0 - 1, y0 + R + 1, z, z + 1) > 0) mask |= uint64_t(1) << j;
+            }
+            StreamTile t{};
+            t.sim = int(i);
+            t.x0 = x0;
+            t.y0 = y0;
+            t.z0 = z0;
+            t.z1 = z1;
+            t.split_lo = uint32_t(mask);
+            t.split_hi = uint32_t(mask >> 32);
+            tiles.push_back(t);
+          }
+    }
+    return tiles;
+  }
+
+  // 4D tensor map (x, y, z, component) over nc components `comp_stride`
+  // elements apart, box (box_x, box_y, 1, box_c).
+  static void encode_map4(CUtensorMap* m, const void* base, CUtensorMapDataType type, int elem, const fdtd_sim* s,
+                          int nc, size_t comp_stride, int box_x, int box_y, int box_c) {
+    const cuuint64_t row = cuuint64_t(s->pitch);
+    const cuuint64_t dims[4] = {row, cuuint64_t(s->ny), cuuint64_t(s->nz), cuuint64_t(nc)};
+    const cuuint64_t strides[3] = {row * elem, row * s->ny * elem, cuuint64_t(comp_stride) * elem};
+    const cuuint32_t box[4] = {cuuint32_t(box_x), cuuint32_t(box_y), 1, cuuint32_t(box_c)};
+    const cuuint32_t estr[4] = {1, 1, 1, 1};
+    CUresult r = get_encode_fn()(m, type, 4, const_cast<void*>(base), dims, strides, box, estr,
+                                 CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                                 CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) throw ArgError{FDTD_ERR_CUDA, "cuTensorMapEncodeTiled failed: " + std::to_string(int(r))};
+  }
 
   static int adj_tiles_per_sm() {
     const char* v = std::getenv("RFN_ADJ_TILES_PER_SM");
@@ -865,6 +933,66 @@ struct Engine {
       }
     }
     const std::vector<int4> tiles = plain_tiles(n_sm, 0, nullptr, kAdjTileX, kAdjTileY, adj_tiles_per_sm());
+    // the marching reverse step (default) or the plain-load one (RFN_ADJ_KERNEL=plain)
+    const char* ak = std::getenv("RFN_ADJ_KERNEL");
+    const bool march = !(ak && std::string(ak) == "plain");
+    int am_main = 0, am_split = 0, am_grid = 0, am_tiles = 0;
+    uint32_t am_ring = 0;
+    if (march) {
+      auto fn = &adj_march_kernel<kAdjMarchXW, kAdjMarchTY>;
+      am_ring = adj_march_slots(&am_main, &am_split);
+      CK(cudaFuncSetAttribute(reinterpret_cast<const void*>(fn), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              int(am_ring)));
+      int per_sm = 0;
+      CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, reinterpret_cast<const void*>(fn),
+                                                       AdjGeom::THREADS, am_ring));
+      if (per_sm < 1) throw ArgError{FDTD_ERR_LIMIT, "Marching reverse step does not fit on an SM."};
+      std::vector<fdtd_sim*> ss;
+      for (const auto& r : req) ss.push_back(r.s);
+      const int64_t slots = int64_t(per_sm) * n_sm;
+      const std::vector<StreamTile> mt = adj_march_tiles(ss, slots);
+      am_tiles = int(mt.size());
+      am_grid = int(std::min<int64_t>(am_tiles, slots));
+      std::vector<AdjMaps> maps(req.size());
+      for (size_t i = 0; i < req.size(); ++i) {
+        fdtd_sim* s = req[i].s;
+        AdjBufs* B = adj_bufs[i].get();
+        const size_t N = s->cells_padded;
+        const auto F = CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
+        std::memset(&maps[i], 0, sizeof(AdjMaps));
+        encode_map4(&maps[i].lamE, B->lam.p, F, 4, s, 12, N, AdjGeom::W, AdjGeom::ER, 3);
+        encode_map4(&maps[i].lamH, B->lam.p, F, 4, s, 12, N, AdjGeom::W, AdjGeom::HR, 3);
+        const bool halves = s->splits.n != 0;
+        encode_map4(&maps[i].lamEs, halves ? B->lams.p : B->lam.p, F, 4, s, halves ? 24 : 12, N, AdjGeom::W,
+                    AdjGeom::ER, 6);
+        encode_map4(&maps[i].lamHs, halves ? B->lams.p : B->lam.p, F, 4, s, halves ? 24 : 12, N, AdjGeom::W,
+                    AdjGeom::HR, 6);
+        encode_map(&maps[i].ids, s->mat.p, CU_TENSOR_MAP_DATA_TYPE_UINT16, 2, s, 3, AdjGeom::IW, AdjGeom::IR, 1,
+                   0, 0);
+      }
+      adj_d_maps.reserve(maps.size());
+      CK(cudaMemcpy(adj_d_maps.p, maps.data(), maps.size() * sizeof(AdjMaps), cudaMemcpyHostToDevice));
+      for (size_t i = 0; i < as.size(); ++i) as[i].maps = adj_d_maps.p + i;
+      adj_d_mtiles.reserve(mt.size());
+      CK(cudaMemcpy(adj_d_mtiles.p, mt.data(), mt.size() * sizeof(StreamTile), cudaMemcpyHostToDevice));
+      adj_d_counter.reserve(1);
+      CK(cudaMemsetAsync(adj_d_counter.p, 0, sizeof(unsigned), st));
+    }
+    unsigned am_seq = 0;
+    auto reverse_step = [&](int n, int hist_n0) {
+      if (march) {
+        const unsigned base = am_seq++ * unsigned(am_tiles + am_grid);
+        adj_march_kernel<kAdjMarchXW, kAdjMarchTY><<<am_grid, AdjGeom::THREADS, am_ring, st>>>(
+            adj_d_as.p, adj_d_mtiles.p, am_tiles, n, hist_n0, adj_d_counter.p, base, d_err.p, am_main, am_split,
+            wait_limit);
+      } else {
+        const char* mb = std::getenv("RFN_ADJ_MINB");
+        auto adj_fn = (mb && std::atoi(mb) == 3) ? &adj_step_kernel<kAdjTileY, 3> : &adj_step_kernel<kAdjTileY, 2>;
+        adj_fn<<<int(tiles.size()), dim3(32, kAdjTileY + 2), 0, st>>>(adj_d_as.p, adj_d_t.p, n, hist_n0);
+      }
+      CK(cudaGetLastError());
+      ++adj_launches;
+    };
     DevBuf<AdjSim>& d_as = adj_d_as;
     DevBuf<int4>& d_t = adj_d_t;
     DevBuf<CapSim>& d_c = adj_d_c;
@@ -877,10 +1005,6 @@ struct Engine {
       CK(cudaMemcpy(d_c.p, caps.data(), caps.size() * sizeof(CapSim), cudaMemcpyHostToDevice));
     }
     const int cap_grid = int(std::min<int64_t>(1024, std::max<int64_t>(1, (nb_max + 255) / 256)));
-    const dim3 blk(32, kAdjTileY + 2);
-    // register cap: two resident blocks per SM (default) or three
-    const char* mb = std::getenv("RFN_ADJ_MINB");
-    auto adj_fn = (mb && std::atoi(mb) == 3) ? &adj_step_kernel<kAdjTileY, 3> : &adj_step_kernel<kAdjTileY, 2>;
     if (p_max > 0) {
       adj_inject_kernel<<<dim3((p_max + 127) / 128, unsigned(as.size())), 128, 0, st>>>(d_as.p, nt - 1,
                                                                                         (nt - 1) & 1);
@@ -889,11 +1013,7 @@ struct Engine {
     adj_launches = 0;
     CK(cudaEventRecord(ev0, st));
     if (mode == 2) {
-      for (int n = nt - 1; n >= 0; --n) {
-        adj_fn<<<int(tiles.size()), blk, 0, st>>>(d_as.p, d_t.p, n, 0);
-        CK(cudaGetLastError());
-        ++adj_launches;
-      }
+      for (int n = nt - 1; n >= 0; --n) reverse_step(n, 0);
     } else {
       const int nseg = (nt + K - 1) / K;
       for (int k = nseg - 1; k >= 0; --k) {
@@ -924,11 +1044,7 @@ struct Engine {
           launch_step(st, n);
           CK(cudaStreamWaitEvent(st, cap_join, 0));
         }
-        for (int n = n1 - 1; n >= n0; --n) {
-          adj_fn<<<int(tiles.size()), blk, 0, st>>>(d_as.p, d_t.p, n, n0);
-          CK(cudaGetLastError());
-          ++adj_launches;
-        }
+        for (int n = n1 - 1; n >= n0; --n) reverse_step(n, n0);
       }
     }
     CK(cudaEventRecord(ev1, st));

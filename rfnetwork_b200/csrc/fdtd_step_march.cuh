@@ -321,6 +321,10 @@ fdtd_step_march_kernel(const SimDev* __restrict__ sims, const StreamTile* __rest
         }
 
         // ---------------------------------------------------- owned rows
+        // H^n of the first owned row (the row above the halo row)
+        hx0 = sH[hb0 + HW];
+        hy0 = sH[HC + hb0 + HW];
+        hz0 = sH[2 * HC + hb0 + HW];
 #pragma unroll
         for (int j = 1; j <= TY; ++j) {
           const int br = br0 + j;                  // box row (grid row y0-1+br)

@@ -27,7 +27,9 @@ FDTD_ERR_DEVICE, FDTD_ERR_NONFINITE = 5, 6
 def _model_sim(s):
     co, pr, mo, mem, Nx, Ny, Nz, Nt = s.pack_inputs(gpu=True)
     sim = _lib.Simulation(Nx, Ny, Nz)
-    sim.set_kernel(2, 16, 4, 0)
+    # 12-plane z chunks: every block streams at least 14 planes, so each one
+    # reaches the withheld plane number
+    sim.set_kernel(2, 16, 4, 12)
     sim.set_coefficients(co)
     for p in pr:
         src = bool(p["is_source"])
