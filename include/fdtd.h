@@ -129,16 +129,13 @@ int fdtd_synchronize(fdtd_sim* s);
 
 /* Step-kernel selection: variant 0 = plain loads (1 cell per thread, 31 x 7
  * tiles), 1 = TMA streaming, one thread per cell (31 x tile_y tiles, tile_y in
- * {4, 6, 8, 12}; stages = shared-memory plane buffers), 2 = TMA row marching,
- * each warp walking `stages` rows of a 31 x tile_y tile ((tile_y, stages) in
- * {(16, 4), (32, 4), (32, 8), (16, 8)}). zchunk = z planes per tile (0:
- * derived from the grid). tile_y = 0 autotunes: the first run times a few
- * candidate shapes on the simulation itself for a few steps and keeps the
- * fastest, remembered per set of grid sizes for the life of the process --
- * streaming and marching shapes with variant 1, marching shapes only with
- * variant 2. The default comes from RFN_FDTD_KERNEL (plain / stream / march)
- * / RFN_FDTD_TY / RFN_FDTD_STAGES / RFN_FDTD_ZCHUNK or is (1, 0, 4, 0):
- * autotuned.
+ * {4, 6, 8, 12}; stages = shared-memory plane slots, 3..8). zchunk = z planes
+ * per tile (0: derived from the grid). tile_y = 0 with variant 1 autotunes:
+ * the first run times a few candidate (tile_y, stages, zchunk) shapes on the
+ * simulation itself for a few steps and keeps the fastest, remembered per set
+ * of grid sizes for the life of the process. The default comes from
+ * RFN_FDTD_KERNEL (plain / stream) / RFN_FDTD_TY / RFN_FDTD_STAGES /
+ * RFN_FDTD_ZCHUNK or is (1, 0, 6, 0): autotuned streaming.
  * All variants give bit-identical results. The reference has one fixed 8x8x8
  * launch shape (solver.cu:549-557). */
 int fdtd_set_kernel(fdtd_sim* s, int variant, int tile_y, int stages, int zchunk);
@@ -151,7 +148,7 @@ int fdtd_set_stream(fdtd_sim* s, void* stream);
  * reference's solver_run_cu does (rfnetwork/core/src/solver.cu:1005-1120). */
 int fdtd_set_graph(fdtd_sim* s, int enabled);
 
-/* Failure-path testing of the row-marching step kernel (variant 2), not for
+/* Failure-path testing of the TMA streaming step kernel (variant 1), not for
  * production runs. wait_limit: sleeping polls (each at most ~2 us) after
  * which a shared-memory pipeline wait gives up (0 restores the default of
  * 2^20, about 2 s); withhold_plane >= 0: every block's producer skips the

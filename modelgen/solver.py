@@ -699,7 +699,7 @@ class FDTD_Solver:
         """Far-field E (theta and phi polarisations) normalised by exp(-j beta r) / r,
         [2, frequency, theta, phi] complex64, theta and phi in degrees
         (rfnetwork/solver.py:2870-3021); the transform runs on the GPU engine."""
-        from . import _lib
+        from rfnetwork_b200 import _lib
 
         theta, phi = np.atleast_1d(theta), np.atleast_1d(phi)
         J_xyz, M_xyz, r_grid, ds_grid, surf_pos = self.farfield_currents()

@@ -248,14 +248,14 @@ class Simulation:
         self._check(self.lib.fdtd_set_graph(self.h, int(bool(enabled))))
 
     def set_debug(self, wait_limit: int = 0, withhold_plane: int = -1):
-        """Failure-path testing of the marching kernel: pipeline waits give up
+        """Failure-path testing of the streaming kernel: pipeline waits give up
         after ``wait_limit`` polls (0: the default, about 2 s) and, with
         ``withhold_plane`` >= 0, that plane's loads are never issued."""
         self._check(self.lib.fdtd_set_debug(self.h, int(wait_limit), int(withhold_plane)))
 
     def run(self, nt: int):
+        self.nt = int(nt)  # the records of a failed run stay readable
         self._check(self.lib.fdtd_run(self.h, int(nt)))
-        self.nt = int(nt)
 
     def run_checkpointed(self, nt: int, every: int):
         """Run like ``run`` and keep a field snapshot every ``every`` steps for ``adjoint``."""

@@ -38,7 +38,6 @@
 namespace rfn {
 
 struct AdjSim {
-  const void* maps;          // tensor maps of the adjoint buffers (marching reverse step)
   int nx, ny, nz, pitch, plane, nt;
   const uint16_t* mat;       // material index [z][y][pitch]
   const float4* rows;        // 8 float4 per table row

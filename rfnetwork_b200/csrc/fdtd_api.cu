@@ -28,8 +28,6 @@
 #include "fdtd_adjoint.cuh"
 #include "fdtd_nf2ff.cuh"
 #include "fdtd_step_stream.cuh"
-#include "fdtd_step_march.cuh"
-#include "fdtd_adjoint_march.cuh"
 #include <cudaTypedefs.h>
 
 using namespace rfn;
@@ -133,28 +131,27 @@ int threads_for_host() {
 
 }  // namespace
 
-// Kernel selection of an engine: the plain-load kernel (one cell per thread),
-// the TMA-pipelined streaming kernel (tile height, stage count) or the
-// row-marching kernel (tile height, rows per warp), and the z chunk.
+// Kernel selection of an engine: the plain-load kernel (one cell per thread)
+// or the TMA-pipelined streaming kernel (tile height, plane slots), and the z chunk.
 struct KernelConfig {
-  int variant = 1;  // 0 plain loads, 1 TMA streaming, 2 TMA row marching
-  int ty = 0;       // tile height; 0 (with variant 1 or 2): autotuned (variant, ty, stages, zchunk)
-  int stages = 4;   // streaming: shared-memory stages; marching: rows per warp
+  int variant = 1;  // 0 plain loads, 1 TMA streaming
+  int ty = 0;       // tile height; 0 (with variant 1): autotuned (ty, stages, zchunk)
+  int stages = 6;   // streaming: shared-memory plane slots
   int zchunk = 0;   // 0: pick from the grid size
 };
 
 // Step-kernel shapes the autotuner times, (variant, tile height, stages or
 // rows per warp, z chunk), and its choices per set of grid sizes (process-wide).
-constexpr int kTuneCandidates[][4] = {{2, 16, 4, 0}, {2, 32, 4, 0}, {2, 32, 8, 0}, {2, 16, 8, 0},
-                                      {2, 16, 4, 8}, {1, 8, 4, 0},  {1, 8, 4, 32}, {1, 8, 3, 0},
-                                      {1, 4, 4, 0},  {1, 4, 4, 16}, {1, 8, 4, 4},  {1, 4, 4, 4}};
+constexpr int kTuneCandidates[][4] = {{1, 8, 6, 0},  {1, 8, 8, 0}, {1, 8, 4, 0},  {1, 8, 6, 32}, {1, 12, 4, 0},
+                                      {1, 6, 6, 0},  {1, 4, 6, 0}, {1, 4, 6, 16}, {1, 8, 6, 4},  {1, 4, 6, 4},
+                                      };
 std::mutex g_tune_mutex;
 std::map<std::vector<int>, std::array<int, 4>> g_tune_cache;
 
 KernelConfig default_config() {
   KernelConfig c;
   if (const char* v = std::getenv("RFN_FDTD_KERNEL"))
-    c.variant = std::string(v) == "plain" ? 0 : std::string(v) == "march" ? 2 : 1;
+    c.variant = std::string(v) == "plain" ? 0 : 1;
   if (const char* v = std::getenv("RFN_FDTD_TY")) c.ty = std::atoi(v);
   if (const char* v = std::getenv("RFN_FDTD_STAGES")) c.stages = std::atoi(v);
   if (const char* v = std::getenv("RFN_FDTD_ZCHUNK")) c.zchunk = std::atoi(v);
@@ -267,101 +264,57 @@ void d2h(fdtd_sim* s, void* dst, const void* src, size_t bytes) {
   s->d2h_bytes += int64_t(bytes);
 }
 
-using StreamKernelFn = void (*)(const SimDev*, const StreamTile*, int, int, unsigned*, unsigned, int*);
+using StreamKernelFn = void (*)(const SimDev*, const StreamTile*, int, int, unsigned*, unsigned, int*, int, int,
+                                uint32_t, int);
 
-// One instantiation of the streaming step kernel.
+// One instantiation of the streaming step kernel (tile height TY) and the
+// bytes of its exchange buffers, plane slots and split slots.
 struct StreamVariant {
-  int ty, stages;
-  int smem, threads;
+  int ty, threads, min_blocks;
+  uint32_t xch_bytes, main_bytes, split_bytes;
   StreamKernelFn fn;
 };
 
-template <int TY, int S>
+template <int TY>
 StreamVariant stream_variant() {
-  return StreamVariant{TY, S, stream_smem_bytes<TY, S>(), StreamGeom<TY>::THREADS, &fdtd_step_stream_kernel<TY, S>};
+  using G = StreamGeom<TY>;
+  return StreamVariant{TY, G::THREADS, G::MIN_BLOCKS, uint32_t(2 * G::XCH), G::MAIN, G::SPLIT,
+                       &fdtd_step_stream_kernel<TY>};
 }
 
 const std::vector<StreamVariant>& stream_variants() {
-  static const std::vector<StreamVariant> v = {
-      stream_variant<4, 4>(), stream_variant<4, 5>(), stream_variant<6, 3>(), stream_variant<6, 4>(),
-      stream_variant<8, 3>(), stream_variant<8, 4>(), stream_variant<12, 3>()};
+  static const std::vector<StreamVariant> v = {stream_variant<4>(), stream_variant<6>(), stream_variant<8>(),
+                                               stream_variant<12>()};
   return v;
 }
 
+// The streaming kernel with tile height ty and `stages` plane slots (3..8).
 const StreamVariant* find_stream_variant(int ty, int stages) {
+  if (stages < 3 || stages > kSlotsMax) return nullptr;
   for (auto& v : stream_variants())
-    if (v.ty == ty && v.stages == stages) return &v;
+    if (v.ty == ty) return &v;
   return nullptr;
 }
 
-using MarchKernelFn = void (*)(const SimDev*, const StreamTile*, int, int, unsigned*, unsigned, int*, int, int,
-                               uint32_t, int);
-
-// One instantiation of the row-marching step kernel: tile height XW*TY,
-// TY rows per warp, and the bytes of its plane and split slots.
-struct MarchVariant {
-  int rows, ty, threads;
-  uint32_t main_bytes, split_bytes;
-  MarchKernelFn fn;
-};
-
-template <int XW, int TY>
-MarchVariant march_variant() {
-  using G = MarchGeom<XW, TY>;
-  return MarchVariant{G::ROWS, TY, G::THREADS, G::MAIN, G::SPLIT, &fdtd_step_march_kernel<XW, TY>};
-}
-
-const std::vector<MarchVariant>& march_variants() {
-  static const std::vector<MarchVariant> v = {march_variant<4, 4>(), march_variant<8, 4>(), march_variant<4, 8>(),
-                                              march_variant<2, 8>()};
-  return v;
-}
-
-const MarchVariant* find_march_variant(int rows, int ty) {
-  for (auto& v : march_variants())
-    if (v.rows == rows && v.ty == ty) return &v;
-  return nullptr;
-}
-
-// Plane and split slots of a marching block: as many blocks per SM as its
-// registers allow (at most two), each block's shared memory split into
-// plane slots (at least three: the plane, its look-ahead and one load in
-// flight) and split slots (at least two). Returns the dynamic shared bytes.
-uint32_t march_slots(const MarchVariant& v, int* n_main, int* n_split) {
+// Dynamic shared bytes of a streaming block with (at most) `want` plane
+// slots and two or three split slots, sized for the kernel's resident blocks
+// per SM; the slot counts it fits go to n_main / n_split.
+uint32_t stream_slots(const StreamVariant& v, int want, int* n_main, int* n_split) {
   constexpr uint32_t kSmemPerSm = 233472, kPerBlockReserve = 1024 + 512, kMaxPerBlock = 232448 - 512;
-  cudaFuncAttributes fa{};
-  CK(cudaFuncGetAttributes(&fa, reinterpret_cast<const void*>(v.fn)));
-  const int regs_per_block = ((fa.numRegs * 32 + 255) / 256 * 256) * (v.threads / 32);
-  int bps = std::max(1, std::min(2, 65536 / std::max(regs_per_block, 1)));
-  for (; bps >= 1; --bps) {
-    const uint32_t budget = std::min(kSmemPerSm / bps - kPerBlockReserve, kMaxPerBlock);
-    if (budget < 3 * v.main_bytes + 2 * v.split_bytes) continue;
-    uint32_t m = std::min<uint32_t>(6, (budget - 2 * v.split_bytes) / v.main_bytes);
-    const uint32_t sp = std::min<uint32_t>(kMarchSplitSlots, (budget - m * v.main_bytes) / v.split_bytes);
-    m = std::min<uint32_t>(kMarchSlots, (budget - sp * v.split_bytes) / v.main_bytes);
-    *n_main = int(m);
-    *n_split = int(sp);
-    return m * v.main_bytes + sp * v.split_bytes;
-  }
-  throw ArgError{FDTD_ERR_LIMIT, "Marching kernel's plane slots do not fit in shared memory."};
-}
-
-// The marching reverse step: tile height and rows per warp of the instantiation used.
-constexpr int kAdjMarchXW = 4, kAdjMarchTY = 4;
-using AdjGeom = AdjMarchGeom<kAdjMarchXW, kAdjMarchTY>;
-
-// Plane and split slots of a marching reverse-step block, as march_slots.
-uint32_t adj_march_slots(int* n_main, int* n_split) {
-  MarchVariant v{AdjGeom::ROWS, kAdjMarchTY, AdjGeom::THREADS, AdjGeom::MAIN, AdjGeom::SPLIT,
-                 reinterpret_cast<MarchKernelFn>(&adj_march_kernel<kAdjMarchXW, kAdjMarchTY>)};
-  return march_slots(v, n_main, n_split);
+  const uint32_t budget = std::min(kSmemPerSm / v.min_blocks - kPerBlockReserve, kMaxPerBlock) - v.xch_bytes;
+  if (budget < 3 * v.main_bytes + 2 * v.split_bytes)
+    throw ArgError{FDTD_ERR_LIMIT, "Streaming kernel's plane slots do not fit in shared memory."};
+  const uint32_t m = std::min<uint32_t>(uint32_t(std::min(want, kSlotsMax)), (budget - 2 * v.split_bytes) / v.main_bytes);
+  const uint32_t sp = std::min<uint32_t>(3, (budget - m * v.main_bytes) / v.split_bytes);
+  *n_main = int(std::max<uint32_t>(m, 3));
+  *n_split = int(sp);
+  return v.xch_bytes + uint32_t(*n_main) * v.main_bytes + sp * v.split_bytes;
 }
 
 // Whether a (variant, tile height, stages) triple names an instantiated kernel.
 bool kernel_exists(int variant, int ty, int stages) {
   if (variant == 0) return true;
   if (variant == 1) return ty == 0 || find_stream_variant(ty, stages) != nullptr;
-  if (variant == 2) return ty == 0 || find_march_variant(ty, stages) != nullptr;
   return false;
 }
 
@@ -411,11 +364,10 @@ void encode_stream_maps(StreamMaps& m, const fdtd_sim* s, int ty) {
   encode_map(&m.ids, s->mat.p, CU_TENSOR_MAP_DATA_TYPE_UINT16, 2, s, 3, 40, ty + 1, 1, 0, 0);
 }
 
-// Everything one launch of the streaming or the marching kernel needs.
+// Everything one launch of the streaming kernel needs.
 struct StreamClass {
   const StreamVariant* v = nullptr;
-  const MarchVariant* mv = nullptr;  // the marching kernel (v is then null)
-  uint32_t ring = 0;                 // its dynamic shared bytes: plane slots, then split slots
+  uint32_t ring = 0;                 // dynamic shared bytes: exchange buffers, plane slots, split slots
   int n_main = 0, n_split = 0;
   std::vector<StreamTile> host_tiles;
   std::vector<StreamMaps> host_maps;
@@ -426,7 +378,6 @@ struct StreamClass {
   int n_tiles = 0, grid = 0;
   void reset() {
     v = nullptr;
-    mv = nullptr;
     ring = 0;
     host_tiles.clear();
     host_maps.clear();
@@ -457,8 +408,8 @@ struct Engine {
   cudaEvent_t cap_fork = nullptr, cap_join = nullptr;
   int64_t step_launches = 0, dft_launches = 0, adj_launches = 0;
   double adj_ms = 0;
-  uint32_t wait_limit = kStreamWaitLimit;  // polls per mbarrier wait of the marching kernel
-  int withhold = -1;                       // test hook: plane the marching kernel's producers never issue
+  uint32_t wait_limit = kStreamWaitLimit;  // polls per mbarrier wait of the streaming kernel
+  int withhold = -1;                       // test hook: plane the TMA kernels' producers never issue
   bool use_graph = true;  // replay the time loop as a captured CUDA graph
   double last_ms = 0;
   bool timing_pending = false;
@@ -498,7 +449,7 @@ struct Engine {
       d_err.alloc(1);
       CK(cudaMemset(d_err.p, 0, sizeof(int)));
     }
-    if (cfg.variant == 1 || cfg.variant == 2) {
+    if (cfg.variant == 1) {
       if (cfg.ty == 0)
         autotune(n_sm);
       else
@@ -542,16 +493,13 @@ struct Engine {
     return tiles;
   }
 
-  // Picks the step kernel's (variant, tile height, stages or rows per warp,
-  // z chunk) for this set of grids: each candidate runs a few time steps on
-  // the simulations themselves (their fields are cleared again by the next
-  // run), the fastest is kept and remembered for the same grid sizes. With
-  // variant 2 requested only the marching shapes are timed.
+  // Picks the streaming kernel's (tile height, plane slots, z chunk) for this
+  // set of grids: each candidate runs a few time steps on the simulations
+  // themselves (their fields are cleared again by the next run), the fastest
+  // is kept and remembered for the same grid sizes.
   void autotune(int n_sm) {
     std::vector<int> key;
     int nt_min = 1 << 30;
-    const bool march_only = cfg.variant == 2;
-    key.push_back(march_only ? 2 : 1);
     for (auto* s : sims) {
       key.insert(key.end(), {s->nx, s->ny, s->nz});
       nt_min = std::min(nt_min, s->prepared_nt);
@@ -579,7 +527,6 @@ struct Engine {
       cudaStream_t st = stream();
       float best_ms = 1e30f;
       for (const auto& cand : kTuneCandidates) {
-        if (march_only && cand[0] != 2) continue;
         apply({cand[0], cand[1], cand[2], cand[3]});
         build_stream_tiles(n_sm);
         CK(cudaMemsetAsync(scls.d_counter.p, 0, sizeof(unsigned), st));
@@ -605,28 +552,20 @@ struct Engine {
     build_stream_tiles(n_sm);
   }
 
-  // Streaming and marching kernels: 31 x TY column tiles cut in z chunks of
-  // at most 62 planes, each with the mask of its planes that hold split-field
-  // cells (TY: the tile height).
+  // Streaming kernel: 31 x TY column tiles cut in z chunks of at most 62
+  // planes, each with the mask of its planes that hold split-field cells.
   void build_stream_tiles(int n_sm) {
     StreamClass& c = scls;
     c.reset();
     const void* fn = nullptr;
     int threads = 0, smem = 0, ty = 0;
-    if (cfg.variant == 2) {
-      c.mv = find_march_variant(cfg.ty, cfg.stages);
-      if (!c.mv) throw ArgError{FDTD_ERR_ARG, "No marching kernel instantiated for this tile height / rows per warp."};
-      c.ring = march_slots(*c.mv, &c.n_main, &c.n_split);
-      fn = reinterpret_cast<const void*>(c.mv->fn);
-      threads = c.mv->threads;
-      smem = int(c.ring);
-      ty = c.mv->rows;
-    } else {
+    {
       c.v = find_stream_variant(cfg.ty, cfg.stages);
       if (!c.v) throw ArgError{FDTD_ERR_ARG, "No streaming kernel instantiated for this tile height / stage count."};
       fn = reinterpret_cast<const void*>(c.v->fn);
       threads = c.v->threads;
-      smem = c.v->smem;
+      c.ring = stream_slots(*c.v, cfg.stages, &c.n_main, &c.n_split);
+      smem = int(c.ring);
       ty = c.v->ty;
     }
     CK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
@@ -704,8 +643,22 @@ struct Engine {
     auto cost = [](const StreamTile& t) {
       return (t.z1 - t.z0 + 1) + 2 * (__builtin_popcount(t.split_lo) + __builtin_popcount(t.split_hi));
     };
-    std::stable_sort(c.host_tiles.begin(), c.host_tiles.end(),
-                     [&](const StreamTile& a, const StreamTile& b) { return cost(a) > cost(b); });
+    const char* ord = std::getenv("RFN_TILE_ORDER");
+    if (ord && std::string(ord) == "chunk") {
+      // whole z chunks in turn, costliest chunk first, tiles of a chunk in
+      // (y, x) order: the blocks working at the same time are x / y
+      // neighbours of one chunk, so their halo rows are read from L2
+      std::map<std::pair<int, int>, int64_t> chunk_cost;
+      for (const auto& t : c.host_tiles) chunk_cost[{t.sim, t.z0}] += cost(t);
+      std::stable_sort(c.host_tiles.begin(), c.host_tiles.end(), [&](const StreamTile& a, const StreamTile& b) {
+        const int64_t ca = chunk_cost[{a.sim, a.z0}], cb = chunk_cost[{b.sim, b.z0}];
+        if (ca != cb) return ca > cb;
+        return std::make_pair(a.sim, a.z0) < std::make_pair(b.sim, b.z0);
+      });
+    } else {
+      std::stable_sort(c.host_tiles.begin(), c.host_tiles.end(),
+                       [&](const StreamTile& a, const StreamTile& b) { return cost(a) > cost(b); });
+    }
     c.n_tiles = int(c.host_tiles.size());
     c.d_maps.alloc(c.host_maps.size());
     CK(cudaMemcpy(c.d_maps.p, c.host_maps.data(), c.host_maps.size() * sizeof(StreamMaps), cudaMemcpyHostToDevice));
@@ -725,15 +678,11 @@ struct Engine {
   }
 
   void launch_step(cudaStream_t st, int n) {
-    if (cfg.variant == 1 || cfg.variant == 2) {
+    if (cfg.variant == 1) {
       StreamClass& c = scls;
       const unsigned base = unsigned(n) * unsigned(c.n_tiles + c.grid);
-      if (c.mv)
-        c.mv->fn<<<c.grid, c.mv->threads, c.ring, st>>>(c.d_sims.p, c.d_tiles.p, c.n_tiles, n, c.d_counter.p, base,
-                                                         d_err.p, c.n_main, c.n_split, wait_limit, withhold);
-      else
-        c.v->fn<<<c.grid, c.v->threads, c.v->smem, st>>>(c.d_sims.p, c.d_tiles.p, c.n_tiles, n, c.d_counter.p, base,
-                                                          d_err.p);
+      c.v->fn<<<c.grid, c.v->threads, c.ring, st>>>(c.d_sims.p, c.d_tiles.p, c.n_tiles, n, c.d_counter.p, base,
+                                                       d_err.p, c.n_main, c.n_split, wait_limit, withhold);
       CK(cudaGetLastError());
     } else {
       fdtd_step_kernel<kTileY><<<n_tiles, dim3(32, kBlockY), 0, st>>>(d_sims.p, d_tiles.p, n);
@@ -777,63 +726,6 @@ struct Engine {
   DevBuf<AdjSim> adj_d_as;
   DevBuf<int4> adj_d_t;
   DevBuf<CapSim> adj_d_c;
-  // marching reverse step: tensor maps per request, tiles, tile counter
-  DevBuf<AdjMaps> adj_d_maps;
-  DevBuf<StreamTile> adj_d_mtiles;
-  DevBuf<unsigned> adj_d_counter;
-
-  // Tiles of the marching reverse step: 30 x ROWS columns in z chunks, each
-  // with the mask of its planes z0-1 .. z1 that hold split cells in its
-  // boxes (columns x0-1 .. x0+30, rows y0-1 .. y0+ROWS).
-  std::vector<StreamTile> adj_march_tiles(const std::vector<fdtd_sim*>& ss, int64_t slots) {
-    constexpr int R = AdjGeom::ROWS, TX = kAdjMarchOwnX;
-    int64_t cols = 0;
-    for (auto* s : ss) cols += int64_t((s->nx + TX - 1) / TX) * ((s->ny + R - 1) / R);
-    std::vector<StreamTile> tiles;
-    for (size_t i = 0; i < ss.size(); ++i) {
-      fdtd_sim* s = ss[i];
-      const int64_t chunks = std::max<int64_t>(1, (slots * 4 + cols - 1) / std::max<int64_t>(cols, 1));
-      const int zc = std::max(1, std::min(62, int((s->nz + chunks - 1) / chunks)));
-      const GradedIndex split_idx(s->grid, kFlagESplit | kFlagHSplit);
-      for (int z0 = 0; z0 < s->nz; z0 += zc)
-        for (int y0 = 0; y0 < s->ny; y0 += R)
-          for (int x0 = 0; x0 < s->nx; x0 += TX) {
-            const int z1 = std::min(s->nz, z0 + zc);
-            uint64_t mask = 0;
-            for (int j = 0; j <= z1 - z0 + 1; ++j) {
-              const int z = z0 - 1 + j;
-              if (z < 0 || z >= s->nz) continue;
-              if (split_idx.count(x0 - 1, x0 + TX + 1, y0 - 1, y0 + R + 1, z, z + 1) > 0) mask |= uint64_t(1) << j;
-            }
-            StreamTile t{};
-            t.sim = int(i);
-            t.x0 = x0;
-            t.y0 = y0;
-            t.z0 = z0;
-            t.z1 = z1;
-            t.split_lo = uint32_t(mask);
-            t.split_hi = uint32_t(mask >> 32);
-            tiles.push_back(t);
-          }
-    }
-    return tiles;
-  }
-
-  // 4D tensor map (x, y, z, component) over nc components `comp_stride`
-  // elements apart, box (box_x, box_y, 1, box_c).
-  static void encode_map4(CUtensorMap* m, const void* base, CUtensorMapDataType type, int elem, const fdtd_sim* s,
-                          int nc, size_t comp_stride, int box_x, int box_y, int box_c) {
-    const cuuint64_t row = cuuint64_t(s->pitch);
-    const cuuint64_t dims[4] = {row, cuuint64_t(s->ny), cuuint64_t(s->nz), cuuint64_t(nc)};
-    const cuuint64_t strides[3] = {row * elem, row * s->ny * elem, cuuint64_t(comp_stride) * elem};
-    const cuuint32_t box[4] = {cuuint32_t(box_x), cuuint32_t(box_y), 1, cuuint32_t(box_c)};
-    const cuuint32_t estr[4] = {1, 1, 1, 1};
-    CUresult r = get_encode_fn()(m, type, 4, const_cast<void*>(base), dims, strides, box, estr,
-                                 CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
-                                 CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-    if (r != CUDA_SUCCESS) throw ArgError{FDTD_ERR_CUDA, "cuTensorMapEncodeTiled failed: " + std::to_string(int(r))};
-  }
-
   static int adj_tiles_per_sm() {
     const char* v = std::getenv("RFN_ADJ_TILES_PER_SM");
     return v ? std::max(1, std::atoi(v)) : 4;
@@ -933,63 +825,11 @@ struct Engine {
       }
     }
     const std::vector<int4> tiles = plain_tiles(n_sm, 0, nullptr, kAdjTileX, kAdjTileY, adj_tiles_per_sm());
-    // the marching reverse step (default) or the plain-load one (RFN_ADJ_KERNEL=plain)
-    const char* ak = std::getenv("RFN_ADJ_KERNEL");
-    const bool march = !(ak && std::string(ak) == "plain");
-    int am_main = 0, am_split = 0, am_grid = 0, am_tiles = 0;
-    uint32_t am_ring = 0;
-    if (march) {
-      auto fn = &adj_march_kernel<kAdjMarchXW, kAdjMarchTY>;
-      am_ring = adj_march_slots(&am_main, &am_split);
-      CK(cudaFuncSetAttribute(reinterpret_cast<const void*>(fn), cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              int(am_ring)));
-      int per_sm = 0;
-      CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, reinterpret_cast<const void*>(fn),
-                                                       AdjGeom::THREADS, am_ring));
-      if (per_sm < 1) throw ArgError{FDTD_ERR_LIMIT, "Marching reverse step does not fit on an SM."};
-      std::vector<fdtd_sim*> ss;
-      for (const auto& r : req) ss.push_back(r.s);
-      const int64_t slots = int64_t(per_sm) * n_sm;
-      const std::vector<StreamTile> mt = adj_march_tiles(ss, slots);
-      am_tiles = int(mt.size());
-      am_grid = int(std::min<int64_t>(am_tiles, slots));
-      std::vector<AdjMaps> maps(req.size());
-      for (size_t i = 0; i < req.size(); ++i) {
-        fdtd_sim* s = req[i].s;
-        AdjBufs* B = adj_bufs[i].get();
-        const size_t N = s->cells_padded;
-        const auto F = CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
-        std::memset(&maps[i], 0, sizeof(AdjMaps));
-        encode_map4(&maps[i].lamE, B->lam.p, F, 4, s, 12, N, AdjGeom::W, AdjGeom::ER, 3);
-        encode_map4(&maps[i].lamH, B->lam.p, F, 4, s, 12, N, AdjGeom::W, AdjGeom::HR, 3);
-        const bool halves = s->splits.n != 0;
-        encode_map4(&maps[i].lamEs, halves ? B->lams.p : B->lam.p, F, 4, s, halves ? 24 : 12, N, AdjGeom::W,
-                    AdjGeom::ER, 6);
-        encode_map4(&maps[i].lamHs, halves ? B->lams.p : B->lam.p, F, 4, s, halves ? 24 : 12, N, AdjGeom::W,
-                    AdjGeom::HR, 6);
-        encode_map(&maps[i].ids, s->mat.p, CU_TENSOR_MAP_DATA_TYPE_UINT16, 2, s, 3, AdjGeom::IW, AdjGeom::IR, 1,
-                   0, 0);
-      }
-      adj_d_maps.reserve(maps.size());
-      CK(cudaMemcpy(adj_d_maps.p, maps.data(), maps.size() * sizeof(AdjMaps), cudaMemcpyHostToDevice));
-      for (size_t i = 0; i < as.size(); ++i) as[i].maps = adj_d_maps.p + i;
-      adj_d_mtiles.reserve(mt.size());
-      CK(cudaMemcpy(adj_d_mtiles.p, mt.data(), mt.size() * sizeof(StreamTile), cudaMemcpyHostToDevice));
-      adj_d_counter.reserve(1);
-      CK(cudaMemsetAsync(adj_d_counter.p, 0, sizeof(unsigned), st));
-    }
-    unsigned am_seq = 0;
     auto reverse_step = [&](int n, int hist_n0) {
-      if (march) {
-        const unsigned base = am_seq++ * unsigned(am_tiles + am_grid);
-        adj_march_kernel<kAdjMarchXW, kAdjMarchTY><<<am_grid, AdjGeom::THREADS, am_ring, st>>>(
-            adj_d_as.p, adj_d_mtiles.p, am_tiles, n, hist_n0, adj_d_counter.p, base, d_err.p, am_main, am_split,
-            wait_limit);
-      } else {
-        const char* mb = std::getenv("RFN_ADJ_MINB");
-        auto adj_fn = (mb && std::atoi(mb) == 3) ? &adj_step_kernel<kAdjTileY, 3> : &adj_step_kernel<kAdjTileY, 2>;
-        adj_fn<<<int(tiles.size()), dim3(32, kAdjTileY + 2), 0, st>>>(adj_d_as.p, adj_d_t.p, n, hist_n0);
-      }
+      // register cap: two resident blocks per SM (default) or three
+      const char* mb = std::getenv("RFN_ADJ_MINB");
+      auto adj_fn = (mb && std::atoi(mb) == 3) ? &adj_step_kernel<kAdjTileY, 3> : &adj_step_kernel<kAdjTileY, 2>;
+      adj_fn<<<int(tiles.size()), dim3(32, kAdjTileY + 2), 0, st>>>(adj_d_as.p, adj_d_t.p, n, hist_n0);
       CK(cudaGetLastError());
       ++adj_launches;
     };
@@ -1029,7 +869,7 @@ struct Engine {
             CK(cudaMemcpyAsync(s->splits.p + b * 12 * N, src + 6 * N, 12 * N * sizeof(float),
                                cudaMemcpyDeviceToDevice, st));
         }
-        if (cfg.variant == 1 || cfg.variant == 2) {
+        if (cfg.variant == 1) {
           // the streaming kernel's tile counter as it stood before step n0
           const unsigned c0 = unsigned(n0) * unsigned(scls.n_tiles + scls.grid);
           CK(cudaMemcpyAsync(scls.d_counter.p, &c0, sizeof(unsigned), cudaMemcpyHostToDevice, st));
@@ -1723,8 +1563,8 @@ int fdtd_get_material_table(fdtd_sim* s, uint16_t* ids, int64_t n_ids, uint32_t*
 int fdtd_set_kernel(fdtd_sim* s, int variant, int tile_y, int stages, int zchunk) {
   if (!s) return FDTD_ERR_ARG;
   return guarded(&s->err, [&] {
-    if (variant < 0 || variant > 2)
-      throw ArgError{FDTD_ERR_ARG, "variant must be 0 (plain), 1 (stream) or 2 (march)"};
+    if (variant < 0 || variant > 1)
+      throw ArgError{FDTD_ERR_ARG, "variant must be 0 (plain) or 1 (stream)"};
     if (!kernel_exists(variant, tile_y, stages))
       throw ArgError{FDTD_ERR_ARG, "No kernel instantiated for this variant / tile height / stage count."};
     KernelConfig c;
@@ -1942,8 +1782,8 @@ int fdtd_batch_create(fdtd_sim* const* sims, int n_sims, fdtd_batch** out) {
 int fdtd_batch_set_kernel(fdtd_batch* b, int variant, int tile_y, int stages, int zchunk) {
   if (!b) return FDTD_ERR_ARG;
   return guarded(&b->err, [&] {
-    if (variant < 0 || variant > 2)
-      throw ArgError{FDTD_ERR_ARG, "variant must be 0 (plain), 1 (stream) or 2 (march)"};
+    if (variant < 0 || variant > 1)
+      throw ArgError{FDTD_ERR_ARG, "variant must be 0 (plain) or 1 (stream)"};
     if (!kernel_exists(variant, tile_y, stages))
       throw ArgError{FDTD_ERR_ARG, "No kernel instantiated for this variant / tile height / stage count."};
     b->engine.cfg.variant = variant;

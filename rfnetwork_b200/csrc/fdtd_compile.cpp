@@ -148,6 +148,57 @@ Box3 core_box(const GradedIndex& gi, int halo_x, int align) {
   return b;
 }
 
+bool plan_split_storage(CompiledGrid& g, SplitPlan& plan, std::string& err) {
+  plan = SplitPlan();
+  const int nx = g.nx, ny = g.ny, nz = g.nz;
+  const GradedIndex split(g, kFlagESplit | kFlagHSplit);
+  // a slab grows while its next layer is more than half split
+  auto mostly = [&](int x0, int x1, int y0, int y1, int z0, int z1) {
+    const int64_t n = int64_t(x1 - x0) * (y1 - y0) * (z1 - z0);
+    return n > 0 && 2 * split.count(x0, x1, y0, y1, z0, z1) > n;
+  };
+  int* t = plan.t;
+  while (t[4] < nz && mostly(0, nx, 0, ny, t[4], t[4] + 1)) ++t[4];
+  while (t[4] + t[5] < nz && mostly(0, nx, 0, ny, nz - 1 - t[5], nz - t[5])) ++t[5];
+  const int z0 = t[4], z1 = nz - t[5];
+  if (z1 > z0) {
+    while (t[2] < ny && mostly(0, nx, t[2], t[2] + 1, z0, z1)) ++t[2];
+    while (t[2] + t[3] < ny && mostly(0, nx, ny - 1 - t[3], ny - t[3], z0, z1)) ++t[3];
+    const int y0 = t[2], y1 = ny - t[3];
+    if (y1 > y0) {
+      while (t[0] < nx && mostly(t[0], t[0] + 1, y0, y1, z0, z1)) ++t[0];
+      while (t[0] + t[1] < nx && mostly(nx - 1 - t[1], nx - t[1], y0, y1, z0, z1)) ++t[1];
+    }
+  }
+  const int64_t ncell = int64_t(nx) * ny * nz;
+  const int64_t core = int64_t(std::max(0, nx - t[0] - t[1])) * std::max(0, ny - t[2] - t[3]) *
+                       std::max(0, nz - t[4] - t[5]);
+  plan.slab_cells = ncell - core;
+  // sparse split cells: probe cells keep their (unique) probe-list offset as
+  // slot; the others get fresh slots after the probe entries, on rows of their own
+  int64_t next = int64_t(g.cell_probes.size());
+  for (int x = 0; x < nx; ++x)
+    for (int y = 0; y < ny; ++y)
+      for (int z = 0; z < nz; ++z) {
+        if (split_store_of(t, nx, ny, nz, x, y, z) != kStoreSparse) continue;
+        uint16_t& id = g.ids[(size_t(x) * ny + y) * nz + z];
+        const Row& r = g.rows[id];
+        if (!(r.w[R_FLAGS] & (kFlagESplit | kFlagHSplit))) continue;
+        ++plan.sparse_cells;
+        if ((r.w[R_FLAGS] >> 16) != 0) continue;  // a probe cell: its row is its own
+        if (g.rows.size() >= 65536) {
+          err = "The sparse split cells need more rows than the 16-bit material index addresses.";
+          return false;
+        }
+        Row u = r;
+        u.w[R_PROBE] = uint32_t(next++);
+        id = uint16_t(g.rows.size());
+        g.rows.push_back(u);
+      }
+  plan.n_sparse = next;
+  return true;
+}
+
 float row_coefficient(const Row& r, int c) {
   float f;
   std::memcpy(&f, &r.w[kSlotOf[c]], 4);

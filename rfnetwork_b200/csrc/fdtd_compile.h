@@ -65,6 +65,39 @@ struct CompiledGrid {
   double compile_ms = 0;
 };
 
+// Where the split pairs of a grid live. The PML slabs (runs of planes, rows
+// or columns at a face in which most cells are split) each get a store of
+// their own, in the priority z faces, then y faces, then x faces: a cell
+// belongs to the first slab that contains it. A split cell outside every slab
+// (a soft-source cell, or a split cell of a model without slabs) is "sparse":
+// its pairs sit at the slot its row's word 31 names in a sparse store, and its
+// row is unique to it.
+enum SplitStore : int { kStoreXlo = 0, kStoreXhi, kStoreYlo, kStoreYhi, kStoreZlo, kStoreZhi, kStoreSparse };
+
+struct SplitPlan {
+  int t[6] = {0, 0, 0, 0, 0, 0};  // slab thickness in cells: x-lo, x-hi, y-lo, y-hi, z-lo, z-hi
+  int64_t n_sparse = 0;           // sparse slots (word-31 values 0 .. n_sparse-1)
+  int64_t slab_cells = 0;         // cells inside the slabs
+  int64_t sparse_cells = 0;       // split cells outside them
+};
+
+// Store of cell (x, y, z) under plan t (kStoreSparse: outside every slab).
+inline int split_store_of(const int* t, int nx, int ny, int nz, int x, int y, int z) {
+  if (z < t[4]) return kStoreZlo;
+  if (z >= nz - t[5]) return kStoreZhi;
+  if (y < t[2]) return kStoreYlo;
+  if (y >= ny - t[3]) return kStoreYhi;
+  if (x < t[0]) return kStoreXlo;
+  if (x >= nx - t[1]) return kStoreXhi;
+  return kStoreSparse;
+}
+
+// Finds the slabs of a compiled grid and gives every sparse split cell a
+// unique row whose word 31 is its sparse slot (a probe cell keeps its
+// probe-list offset, already unique). Returns false with `err` when the
+// table would exceed 65536 rows.
+bool plan_split_storage(CompiledGrid& g, SplitPlan& plan, std::string& err);
+
 // Builds the table. coef[i] points to kCoefNames[i]'s (nx, ny, nz) array.
 // Returns false with `err` set on invalid input or when more than 65535
 // distinct rows are needed.

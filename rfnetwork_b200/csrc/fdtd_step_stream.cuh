@@ -84,9 +84,9 @@ struct StreamGeom {
   static constexpr int A(int b) { return (b + 127) / 128 * 128; }
   static constexpr int OFF_E = A(HB);
   static constexpr int OFF_I = OFF_E + A(EB);
-  static constexpr int OFF_ES = OFF_I + A(IB);
-  static constexpr int OFF_HS = OFF_ES + A(SEB);
-  static constexpr int STAGE = OFF_HS + A(SHB);
+  static constexpr uint32_t MAIN = OFF_I + A(IB);  // plane slot: H, E, index
+  static constexpr uint32_t SPLIT_HS = A(SEB);     // H pairs inside a split slot
+  static constexpr uint32_t SPLIT = A(SEB) + A(SHB); // split slot: E pairs, then H pairs
   static constexpr uint32_t MAIN_BYTES = HB + EB + IB;
   static constexpr uint32_t SPLIT_BYTES = SEB + SHB;
   static constexpr int SECN = ER * kStreamWin;     // float2 pairs per E split pair, narrow window
@@ -100,11 +100,18 @@ struct StreamGeom {
   static constexpr int MIN_BLOCKS = TY <= 4 ? 4 : TY <= 6 ? 3 : 2;
 };
 
-template <int TY, int S>
-constexpr int stream_smem_bytes() {
-  using G = StreamGeom<TY>;
-  return S * G::STAGE + 2 * G::XCH + 16 * S;
-}
+// Plane slots and split slots of the streaming and marching kernels (at most).
+constexpr int kSlotsMax = 8;
+constexpr int kSplitSlotsMax = 4;
+
+// A plane's place in the ring of P plane slots: slot index and the parity of
+// the slot's current use, advanced without a division.
+struct SlotPos {
+  uint32_t slot, par;
+  __device__ __forceinline__ SlotPos next(uint32_t P) const {
+    return slot + 1 == P ? SlotPos{0u, par ^ 1u} : SlotPos{slot + 1, par};
+  }
+};
 
 __device__ __forceinline__ StreamTile load_stream_tile(const StreamTile* tiles, int i) {
   const int4* p = reinterpret_cast<const int4*>(tiles + i);
@@ -139,25 +146,30 @@ __device__ __forceinline__ void stream_inject(const SimDev& Sd, const float4& r7
   }
 }
 
-template <int TY, int S>
+template <int TY>
 __global__ void __launch_bounds__(StreamGeom<TY>::THREADS, StreamGeom<TY>::MIN_BLOCKS)
 fdtd_step_stream_kernel(const SimDev* __restrict__ sims, const StreamTile* __restrict__ tiles, int n_tiles, int n,
-                        unsigned* __restrict__ counter, unsigned base, int* __restrict__ err) {
+                        unsigned* __restrict__ counter, unsigned base, int* __restrict__ err, int n_main,
+                        int n_split, uint32_t wait_limit, int withhold) {
   using G = StreamGeom<TY>;
-  // a tile streams at least 3 planes, so S <= 7 keeps the producer within
-  // three tiles of the consumers (the s_tq ring holds 4)
-  static_assert(S >= 3 && S <= 7, "stage count out of range");
+  // dynamic shared memory: the E exchange buffers, n_main plane slots (H, E,
+  // index), n_split split slots (E and H pairs). A warp holds two plane slots
+  // (the plane and its look-ahead) and one split slot at a time; a plane's
+  // split slot is free again once that plane is released.
   extern __shared__ __align__(128) unsigned char smem[];
-  float* xch = reinterpret_cast<float*>(smem + S * G::STAGE);  // [2][ex, ez][ER][32]
-  uint64_t* full = reinterpret_cast<uint64_t*>(smem + S * G::STAGE + 2 * G::XCH);
-  uint64_t* empty = full + S;
+  float* xch = reinterpret_cast<float*>(smem);  // [2][ex, ez][ER][32]
+  unsigned char* ring = smem + 2 * G::XCH;
+  __shared__ __align__(8) uint64_t full[kSlotsMax], empty[kSlotsMax];
+  __shared__ uint32_t s_soff[kSlotsMax];       // byte offset of each plane's split slot
+  __shared__ uint32_t s_suser[kSplitSlotsMax]; // last plane that used each split slot (producer only)
   __shared__ int s_tq[4];
   const int tid = threadIdx.x;
   const int cur = n & 1, nxt = cur ^ 1;
   constexpr int NC = G::CONSUMERS;
+  const int P = n_main;
 
   if (tid == 0) {
-    for (int s = 0; s < S; ++s) {
+    for (int s = 0; s < P; ++s) {
       mbar_init(&full[s], 1);
       mbar_init(&empty[s], G::NCW);
     }
@@ -168,12 +180,22 @@ fdtd_step_stream_kernel(const SimDev* __restrict__ sims, const StreamTile* __res
   // =================================================================== producer
   if (tid >= NC) {
     if (tid != NC) return;
-    uint32_t q = 0;        // sequence number of the next plane
-    int sq = 0;            // its stage
-    uint32_t pq = 0;       // parity of its stage's current use
+    uint32_t q = 0;    // planes issued
+    uint32_t rel = 0;  // planes below rel are known to be released by every consumer warp
+    uint32_t ns = 0;   // split slots taken
+    SlotPos qp{0u, 0u}, rp{0u, 0u};  // ring positions of planes q and rel
     int k = 0;
     const StreamMaps* cur_maps = nullptr;
     bool failed = false;
+    // waits until plane u has been released (planes are released in order)
+    auto release_upto = [&](uint32_t u) -> bool {
+      while (rel <= u) {
+        if (!mbar_wait_bounded(&empty[rp.slot], rp.par, wait_limit)) return false;
+        ++rel;
+        rp = rp.next(P);
+      }
+      return true;
+    };
     for (;;) {
       const unsigned v = atomicAdd(counter, 1u) - base;
       const int t = v < unsigned(n_tiles) ? int(v) : -1;
@@ -200,44 +222,62 @@ fdtd_step_stream_kernel(const SimDev* __restrict__ sims, const StreamTile* __res
       }
       const int xs = (td.x0 - 1) & ~3, xi = (td.x0 - 1) & ~7;
       for (int j = 0; j < nload; ++j) {
-        // the stage's previous use (parity pq ^ 1) must have been released
-        if (q >= uint32_t(S) && !mbar_wait_bounded(&empty[sq], pq ^ 1u, kStreamWaitLimit)) {
+        const bool last = t >= 0 && j == nload - 1;
+        const bool split = t >= 0 && !last && ((mask >> j) & 1u);
+        const bool win = (narrow >> j) & 1u;
+        // the plane slot's previous plane, and the split slot's last user, must be released
+        if (q >= uint32_t(P) && !release_upto(q - P)) {
           failed = true;
           break;
         }
+        const int slot = int(qp.slot);
+        uint32_t soff = 0;
+        if (split) {
+          const uint32_t ss = ns % uint32_t(n_split);
+          if (ns >= uint32_t(n_split) && !release_upto(s_suser[ss])) {
+            failed = true;
+            break;
+          }
+          s_suser[ss] = q;
+          ++ns;
+          soff = uint32_t(P) * G::MAIN + ss * G::SPLIT;
+        }
+        s_soff[slot] = soff;
         if (j == 0) s_tq[k & 3] = t;
         if (t < 0) {  // end of the stream: complete the phase without data
-          mbar_arrive(&full[sq]);
+          mbar_arrive(&full[slot]);
           ++q;
+          qp = qp.next(P);
           break;
         }
-        unsigned char* b = smem + sq * G::STAGE;
+        if (int(q) == withhold) {  // test hook: this plane is never issued, so the waits for it expire
+          ++q;
+          qp = qp.next(P);
+          continue;
+        }
+        unsigned char* b = ring + uint32_t(slot) * G::MAIN;
+        unsigned char* sb = ring + soff;
+        uint64_t* fb = &full[slot];
         const int zp = td.z0 - 1 + j;
-        const bool last = j == nload - 1;
-        const bool split = !last && ((mask >> j) & 1u);
-        const bool win = (narrow >> j) & 1u;
         fence_proxy_async();
-        mbar_arrive_expect_tx(&full[sq], last    ? uint32_t(G::HB)
-                                         : !split ? G::MAIN_BYTES
-                                                  : G::MAIN_BYTES + (win ? G::SPLIT_BYTES_N : G::SPLIT_BYTES));
-        tma_load_5d(b, &maps->H, xs, td.y0 - 1, zp, 0, cur, &full[sq]);
+        mbar_arrive_expect_tx(fb, last    ? uint32_t(G::HB)
+                                  : !split ? G::MAIN_BYTES
+                                           : G::MAIN_BYTES + (win ? G::SPLIT_BYTES_N : G::SPLIT_BYTES));
+        tma_load_5d(b, &maps->H, xs, td.y0 - 1, zp, 0, cur, fb);
         if (!last) {
-          tma_load_5d(b + G::OFF_E, &maps->E, xs, td.y0 - 1, zp, 0, cur, &full[sq]);
-          tma_load_3d(b + G::OFF_I, &maps->ids, xi, td.y0 - 1, zp, &full[sq]);
+          tma_load_5d(b + G::OFF_E, &maps->E, xs, td.y0 - 1, zp, 0, cur, fb);
+          tma_load_3d(b + G::OFF_I, &maps->ids, xi, td.y0 - 1, zp, fb);
           // split pairs are interleaved along x: float column 2x holds cell x
           if (split && win) {
-            tma_load_5d(b + G::OFF_ES, &maps->Es16, 2 * td.wx0, td.y0 - 1, zp, 0, cur, &full[sq]);
-            tma_load_5d(b + G::OFF_HS, &maps->Hs16, 2 * td.wx0, td.y0, zp, 0, cur, &full[sq]);
+            tma_load_5d(sb, &maps->Es16, 2 * td.wx0, td.y0 - 1, zp, 0, cur, fb);
+            tma_load_5d(sb + G::SPLIT_HS, &maps->Hs16, 2 * td.wx0, td.y0, zp, 0, cur, fb);
           } else if (split) {
-            tma_load_5d(b + G::OFF_ES, &maps->Es, 2 * xs, td.y0 - 1, zp, 0, cur, &full[sq]);
-            tma_load_5d(b + G::OFF_HS, &maps->Hs, 2 * xs, td.y0, zp, 0, cur, &full[sq]);
+            tma_load_5d(sb, &maps->Es, 2 * xs, td.y0 - 1, zp, 0, cur, fb);
+            tma_load_5d(sb + G::SPLIT_HS, &maps->Hs, 2 * xs, td.y0, zp, 0, cur, fb);
           }
         }
         ++q;
-        if (++sq == S) {
-          sq = 0;
-          pq ^= 1u;
-        }
+        qp = qp.next(P);
       }
       if (failed || t < 0) break;
       ++k;
@@ -245,8 +285,7 @@ fdtd_step_stream_kernel(const SimDev* __restrict__ sims, const StreamTile* __res
     if (failed) {
       atomicExch(err, kErrWaitExpired);
       // drain the loads still in flight (bounded)
-      for (uint32_t r = q > uint32_t(S) ? q - S : 0; r < q; ++r)
-        mbar_wait_bounded(&full[r % S], (r / S) & 1u, kStreamWaitLimit);
+      for (uint32_t r = rel; r < q; ++r, rp = rp.next(P)) mbar_wait_bounded(&full[rp.slot], rp.par, wait_limit);
     }
     return;
   }
@@ -256,10 +295,9 @@ fdtd_step_stream_kernel(const SimDev* __restrict__ sims, const StreamTile* __res
   const float4* __restrict__ rows = nullptr;
   int row_id = -1;
   float4 ra = {}, rb = {}, rd = {}, rp = {}, rq = {}, ru = {}, rv = {}, r7 = {};
-  int sq = 0;        // stage of the plane being computed
-  uint32_t pq = 0;   // parity of that stage's current use
+  SlotPos cp{0u, 0u};  // ring position of the plane being computed
   for (int k = 0;; ++k) {
-    bool ok = mbar_wait_bounded(&full[sq], pq, kStreamWaitLimit);
+    bool ok = mbar_wait_bounded(&full[cp.slot], cp.par, wait_limit);
     if (named_bar_or(kStreamBar, NC, !ok)) {
       if (tid == 0) atomicExch(err, kErrWaitExpired);
       return;
@@ -298,21 +336,17 @@ fdtd_step_stream_kernel(const SimDev* __restrict__ sims, const StreamTile* __res
       constexpr bool FAST = decltype(fast_tag)::value;
       float ex_p = 0.f, ey_p = 0.f;  // E^{n+1} of this cell one plane below
       for (int i = 0; i < npl; ++i) {
-        int sn = sq + 1;
-        uint32_t pn = pq;
-        if (sn == S) {
-          sn = 0;
-          pn ^= 1u;
-        }
+        const SlotPos np = cp.next(P);
         // plane z was waited for as the look-ahead of the previous iteration
-        ok = ok && mbar_wait_bounded(&full[sn], pn, kStreamWaitLimit);
-        const unsigned char* st = smem + sq * G::STAGE;
+        ok = ok && mbar_wait_bounded(&full[np.slot], np.par, wait_limit);
+        const unsigned char* st = ring + cp.slot * G::MAIN;
         const float* sH = reinterpret_cast<const float*>(st);
         const float* sE = reinterpret_cast<const float*>(st + G::OFF_E);
         const uint16_t* sI = reinterpret_cast<const uint16_t*>(st + G::OFF_I);
-        const float* sEs = reinterpret_cast<const float*>(st + G::OFF_ES);
-        const float* sHs = reinterpret_cast<const float*>(st + G::OFF_HS);
-        const float* nH = reinterpret_cast<const float*>(smem + sn * G::STAGE);
+        const unsigned char* ss = ring + s_soff[cp.slot];
+        const float* sEs = reinterpret_cast<const float*>(ss);
+        const float* sHs = reinterpret_cast<const float*>(ss + G::SPLIT_HS);
+        const float* nH = reinterpret_cast<const float*>(ring + np.slot * G::MAIN);
         float* xb = xch + (i & 1) * (G::XCH / 4);
         constexpr int HC = G::HC, EC = G::EC;
         const bool store = own_xy && i > 0;
@@ -328,7 +362,7 @@ fdtd_step_stream_kernel(const SimDev* __restrict__ sims, const StreamTile* __res
         const int id = ok ? int(sI[ib]) : 0;  // a stage that never arrived may hold any bits
         if (i + 1 < npl) {
           // the next plane's row into L1 while this plane computes
-          const int idn = reinterpret_cast<const uint16_t*>(smem + sn * G::STAGE + G::OFF_I)[ib];
+          const int idn = reinterpret_cast<const uint16_t*>(ring + np.slot * G::MAIN + G::OFF_I)[ib];
           if (ok && idn != id) prefetch_l1(rows + 8 * idn);
         }
         if (id != row_id) {
@@ -463,9 +497,8 @@ fdtd_step_stream_kernel(const SimDev* __restrict__ sims, const StreamTile* __res
         ey_p = ey;
         // plane z is no longer read by this warp
         __syncwarp();
-        if (lane == 0) mbar_arrive(&empty[sq]);
-        sq = sn;
-        pq = pn;
+        if (lane == 0) mbar_arrive(&empty[cp.slot]);
+        cp = np;
         idx += plane;
       }
       return true;
@@ -473,11 +506,8 @@ fdtd_step_stream_kernel(const SimDev* __restrict__ sims, const StreamTile* __res
     if (!(td.plain ? planes(std::true_type{}) : planes(std::false_type{}))) return;
     // the look-ahead plane z1 was read only by the last iteration
     __syncwarp();
-    if (lane == 0) mbar_arrive(&empty[sq]);
-    if (++sq == S) {
-      sq = 0;
-      pq ^= 1u;
-    }
+    if (lane == 0) mbar_arrive(&empty[cp.slot]);
+    cp = cp.next(P);
   }
 }
 

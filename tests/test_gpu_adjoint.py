@@ -156,19 +156,3 @@ def test_gpu_box_patch_runs_equal_full_arrays(engine_lib):
         ref.close()
     sim.close()
 
-
-@pytest.mark.parametrize("every", [0, 64])
-def test_marching_reverse_step_matches_plain_reverse_step(engine_lib, monkeypatch, every):
-    """The TMA-staged marching reverse step (the default) and the plain-load
-    reverse step evaluate the same adjoint recursion: gradients agree to FP32
-    rounding, on a model with PML, port source cells and an H-probe objective."""
-    s = configs.microstrip(n=(40, 34, 26), n_pml=4, nt=300)
-    grads = []
-    for kernel in ("plain", "march"):
-        monkeypatch.setenv("RFN_ADJ_KERNEL", kernel)
-        sim, pr, nt, _ = _sim(s, 1, every, TERMS, box=(12, 20, 12, 18, 9, 11))
-        X = sim.dft()
-        grads.append(sim.adjoint(2 * X, (12, 20, 12, 18, 9, 11)))
-        sim.close()
-    assert np.abs(grads[0]).max() > 0
-    assert rel_l2(grads[1], grads[0]) <= 1e-5

@@ -47,8 +47,7 @@ def test_ragged_grids_stream_equals_plain(engine_lib, shape):
     ref = plain.probe_values()
     plain.close()
     assert np.isfinite(ref).all() and np.abs(ref).max() > 0
-    for variant, ty, stages, zchunk in ((1, 8, 4, 0), (1, 4, 5, 1), (1, 6, 3, 2), (2, 16, 4, 0), (2, 32, 8, 1),
-                                        (2, 16, 8, 2), (2, 32, 4, 3)):
+    for variant, ty, stages, zchunk in ((1, 8, 4, 0), (1, 4, 5, 1), (1, 6, 3, 2), (1, 8, 8, 3), (1, 12, 3, 1)):
         sim = _random_sim(shape, 1, nt, variant, tile_y=ty, stages=stages, zchunk=zchunk)
         sim.run(nt)
         got = sim.probe_values()
@@ -70,7 +69,7 @@ def test_run_without_probes_and_one_step(engine_lib):
     b.close()
 
 
-@pytest.mark.parametrize("kernel", [(1, 8, 4, 0), (2, 16, 4, 0)])
+@pytest.mark.parametrize("kernel", [(1, 8, 4, 0), (1, 4, 6, 2)])
 def test_batch_of_tiny_grids_equals_single_runs(engine_lib, kernel):
     """A batch whose members are smaller than one tile or leave ragged tiles
     gives each member the bits of its own run."""

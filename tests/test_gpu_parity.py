@@ -188,21 +188,7 @@ def test_stream_kernel_bitwise_equals_plain(engine_lib, ty, stages, zchunk):
         assert np.array_equal(a, b)
 
 
-@pytest.mark.parametrize("ty,rows_per_warp,zchunk", [(16, 4, 0), (32, 4, 5), (32, 8, 0), (16, 8, 62), (16, 4, 1)])
-def test_march_kernel_bitwise_equals_plain(engine_lib, ty, rows_per_warp, zchunk):
-    """The row-marching kernel (variant 2) evaluates the same expressions as
-    the plain one: same models as the streaming-kernel test."""
-    models = (configs.microstrip(n=(72, 40, 30), n_pml=5, nt=150),
-              configs.boxes(n=(70, 45, 38), n_pml=6, n_boxes=6, nt=120, n_ports=2, n_probes=4))
-    for s in models:
-        a, sa = _engine_probe_matrix(s, 0)
-        b, sb = _engine_probe_matrix(s, 2, tile_y=ty, stages=rows_per_warp, zchunk=zchunk)
-        assert sa["variant"] == 0 and sb["variant"] == 2
-        assert np.abs(a).max() > 0
-        assert np.array_equal(a, b)
-
-
-@pytest.mark.parametrize("variant", [0, 1, 2])
+@pytest.mark.parametrize("variant", [0, 1])
 def test_host_launched_steps_equal_graph_replay(engine_lib, variant):
     """fdtd_set_graph(0): the same launches issued step by step from the host."""
     s = configs.microstrip(n=(40, 30, 24), n_pml=4, nt=200)
