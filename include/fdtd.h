@@ -65,6 +65,10 @@ typedef struct fdtd_stats {
   int64_t d2h_bytes;     /* device-to-host bytes read back from it so far */
   int64_t adjoint_launches; /* reverse-step kernel launches of the last fdtd_adjoint */
   double adjoint_ms;     /* device time of the last fdtd_adjoint (CUDA events) */
+  int split_slab[6];     /* PML slab thickness holding split pairs: x-lo, x-hi, y-lo, y-hi, z-lo, z-hi */
+  int64_t slab_cells;    /* cells inside those slabs */
+  int64_t sparse_split_cells; /* split cells outside them (soft-source cells) */
+  int64_t split_bytes;   /* device bytes of the split-pair storage (both time buffers) */
 } fdtd_stats;
 
 /* --------------------------------------------------------------- one grid */

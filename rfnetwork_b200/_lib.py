@@ -44,10 +44,13 @@ class FdtdStats(ctypes.Structure):
         ("variant", ctypes.c_int), ("tile_y", ctypes.c_int), ("stages", ctypes.c_int), ("zchunk", ctypes.c_int),
         ("grid", ctypes.c_int), ("h2d_bytes", ctypes.c_int64), ("d2h_bytes", ctypes.c_int64),
         ("adjoint_launches", ctypes.c_int64), ("adjoint_ms", ctypes.c_double),
+        ("split_slab", ctypes.c_int * 6), ("slab_cells", ctypes.c_int64), ("sparse_split_cells", ctypes.c_int64),
+        ("split_bytes", ctypes.c_int64),
     ]
 
     def as_dict(self):
-        return {k: getattr(self, k) for k, _ in self._fields_}
+        return {k: (list(getattr(self, k)) if k == "split_slab" else getattr(self, k)) for k, _ in self._fields_}
+
 
 
 _lib = None

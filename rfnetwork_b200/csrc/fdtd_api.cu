@@ -181,6 +181,9 @@ struct fdtd_sim {
   int pitch = 0;
   size_t cells_padded = 0;
   CompiledGrid grid;
+  SplitPlan split_plan;         // slab thicknesses and sparse slots of the split cells
+  SplitDev split_geo{};         // store geometry (base pointers set when prepared)
+  size_t split_buf_pairs = 0;   // split pairs per time buffer (all stores)
   DevBuf<float> fields;        // 2 x 6 field arrays
   DevBuf<float> splits;        // 2 x 12 split arrays (only when split cells exist)
   DevBuf<uint16_t> mat;
@@ -355,11 +358,28 @@ void encode_stream_maps(StreamMaps& m, const fdtd_sim* s, int ty) {
   encode_map(&m.E, s->fields.p, F, 4, s, 5, 36, ty + 1, 3, N, 6 * N);
   encode_map(&m.H, s->fields.p + 3 * N, F, 4, s, 5, 40, ty + 2, 3, N, 6 * N);
   if (s->splits.n) {
-    // 3 pair components per field, 2N floats apart, x rows of 2 * pitch floats
-    encode_map(&m.Es, s->splits.p, F, 4, s, 5, 2 * 36, ty + 1, 3, 2 * N, 12 * N, 2);
-    encode_map(&m.Hs, s->splits.p + 6 * N, F, 4, s, 5, 2 * 36, ty, 3, 2 * N, 12 * N, 2);
-    encode_map(&m.Es16, s->splits.p, F, 4, s, 5, 2 * kStreamWin, ty + 1, 3, 2 * N, 12 * N, 2);
-    encode_map(&m.Hs16, s->splits.p + 6 * N, F, 4, s, 5, 2 * kStreamWin, ty, 3, 2 * N, 12 * N, 2);
+    // each slab store: x rows of 2 w floats (pairs interleaved), h rows, its
+    // depth in planes, 6 pair components, 2 time buffers; boxes of 36 pairs
+    // and the E (ty + 1) or H (ty) rows, 3 components
+    const SplitDev& g = s->split_geo;
+    for (int st = 0; st < 6; ++st) {
+      if (!g.comp[st]) continue;
+      const cuuint64_t w2 = cuuint64_t(2 * g.w[st]);
+      const cuuint64_t dims[5] = {w2, cuuint64_t(g.h[st]), cuuint64_t(g.comp[st] / (int64_t(g.w[st]) * g.h[st])), 6,
+                                  2};
+      const cuuint64_t strides[4] = {w2 * 4, w2 * g.h[st] * 4, cuuint64_t(g.comp[st]) * 8,
+                                     cuuint64_t(s->split_buf_pairs) * 8};
+      const cuuint32_t estr[5] = {1, 1, 1, 1, 1};
+      for (int k = 0; k < 2; ++k) {
+        const cuuint32_t box[5] = {72, cuuint32_t(k == 0 ? ty + 1 : ty), 1, 3, 1};
+        CUresult r = get_encode_fn()(k == 0 ? &m.Es[st] : &m.Hs[st], F, 5,
+                                     reinterpret_cast<float2*>(s->splits.p) + g.off[st], dims, strides, box, estr,
+                                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                                     CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+        if (r != CUDA_SUCCESS)
+          throw ArgError{FDTD_ERR_CUDA, "cuTensorMapEncodeTiled failed for a split store: " + std::to_string(int(r))};
+      }
+    }
   }
   encode_map(&m.ids, s->mat.p, CU_TENSOR_MAP_DATA_TYPE_UINT16, 2, s, 3, 40, ty + 1, 1, 0, 0);
 }
@@ -600,39 +620,35 @@ struct Engine {
         for (int y0 = 0; y0 < s->ny; y0 += ty)
           for (int x0 = 0; x0 < s->nx; x0 += kStreamOwnX) {
             const int z1 = std::min(s->nz, z0 + zc);
-            // planes holding split cells in the E region, and the x extent of those cells
-            uint64_t mask = 0, narrow = 0;
-            int wx0 = -1;
-            std::vector<std::pair<int, int>> span(size_t(z1 - z0 + 1), {-1, -1});
+            // planes holding split cells in the E region (columns x0-1 .. x0+30, rows y0-1 .. y0+ty-1)
+            uint64_t mask = 0;
             for (int j = 0; j < z1 - z0 + 1; ++j) {
               const int z = z0 - 1 + j;
-              if (z < 0 || split_idx.count(x0 - 1, x0 + kStreamOwnX, y0 - 1, y0 + ty, z, z + 1) == 0) continue;
-              mask |= uint64_t(1) << j;
-              int lo = 1 << 30, hi = -1;
-              for (int x = std::max(0, x0 - 1); x < std::min(s->nx, x0 + kStreamOwnX); ++x)
-                if (split_idx.count(x, x + 1, y0 - 1, y0 + ty, z, z + 1) > 0) {
-                  lo = std::min(lo, x);
-                  hi = std::max(hi, x);
-                }
-              span[size_t(j)] = {lo, hi};
-              if (wx0 < 0 && hi < (lo & ~3) + kStreamWin) wx0 = lo & ~3;
+              if (z >= 0 && split_idx.count(x0 - 1, x0 + kStreamOwnX, y0 - 1, y0 + ty, z, z + 1) > 0)
+                mask |= uint64_t(1) << j;
             }
-            for (int j = 0; j < z1 - z0 + 1 && wx0 >= 0; ++j)
-              if (((mask >> j) & 1u) && span[size_t(j)].first >= wx0 && span[size_t(j)].second < wx0 + kStreamWin)
-                narrow |= uint64_t(1) << j;
+            // slab stores the tile's rows and columns reach on planes outside the z slabs
+            const int* pt = s->split_plan.t;
+            const int zc0 = pt[4], zc1 = s->nz - pt[5];
+            int ys = -1, xs = -1;
+            if (zc1 > zc0) {
+              if (pt[2] > 0 && y0 - 1 < pt[2]) ys = kStYlo;
+              else if (pt[3] > 0 && y0 + ty - 1 >= s->ny - pt[3]) ys = kStYhi;
+              if (pt[0] > 0 && x0 - 1 < pt[0]) xs = kStXlo;
+              else if (pt[1] > 0 && x0 + kStreamOwnX - 1 >= s->nx - pt[1]) xs = kStXhi;
+            }
             StreamTile t{};
             t.sim = int(i);
             t.x0 = x0;
             t.y0 = y0;
             t.z0 = z0;
             t.z1 = z1;
-            t.wx0 = std::max(wx0, 0);
+            t.ys = ys;
+            t.xs = xs;
             t.plain = mask == 0 &&
                       !probe_tiles.count((int64_t(z0 / zc) * nty + y0 / ty) * ntx + x0 / kStreamOwnX);
             t.split_lo = uint32_t(mask);
             t.split_hi = uint32_t(mask >> 32);
-            t.narrow_lo = uint32_t(narrow);
-            t.narrow_hi = uint32_t(narrow >> 32);
             c.host_tiles.push_back(t);
           }
     }
@@ -862,12 +878,12 @@ struct Engine {
         for (const auto& r : req) {
           fdtd_sim* s = r.s;
           const size_t N = s->cells_padded;
-          const size_t stride = 6 * N + (s->splits.n ? 12 * N : 0);
+          const size_t sb = s->splits.n ? 2 * s->split_buf_pairs : 0;  // split floats per time buffer
+          const size_t stride = 6 * N + sb;
           const float* src = s->ckpt.p + size_t(k) * stride;
           CK(cudaMemcpyAsync(s->fields.p + b * 6 * N, src, 6 * N * sizeof(float), cudaMemcpyDeviceToDevice, st));
-          if (s->splits.n)
-            CK(cudaMemcpyAsync(s->splits.p + b * 12 * N, src + 6 * N, 12 * N * sizeof(float),
-                               cudaMemcpyDeviceToDevice, st));
+          if (sb)
+            CK(cudaMemcpyAsync(s->splits.p + b * sb, src + 6 * N, sb * sizeof(float), cudaMemcpyDeviceToDevice, st));
         }
         if (cfg.variant == 1) {
           // the streaming kernel's tile counter as it stood before step n0
@@ -915,12 +931,12 @@ struct Engine {
       for (auto* s : sims)
         if (s->ckpt_every > 0 && n % s->ckpt_every == 0 && s->ckpt.n) {
           const size_t N = s->cells_padded, b = size_t(n & 1);
-          const size_t stride = 6 * N + (s->splits.n ? 12 * N : 0);
+          const size_t sb = s->splits.n ? 2 * s->split_buf_pairs : 0;  // split floats per time buffer
+          const size_t stride = 6 * N + sb;
           float* dst = s->ckpt.p + size_t(n / s->ckpt_every) * stride;
           CK(cudaMemcpyAsync(dst, s->fields.p + b * 6 * N, 6 * N * sizeof(float), cudaMemcpyDeviceToDevice, st));
-          if (s->splits.n)
-            CK(cudaMemcpyAsync(dst + 6 * N, s->splits.p + b * 12 * N, 12 * N * sizeof(float),
-                               cudaMemcpyDeviceToDevice, st));
+          if (sb)
+            CK(cudaMemcpyAsync(dst + 6 * N, s->splits.p + b * sb, sb * sizeof(float), cudaMemcpyDeviceToDevice, st));
         }
       if (n_caps) {
         // the box history of step n reads buffer n & 1, which step n only
@@ -1035,6 +1051,38 @@ struct Engine {
 
 namespace {
 
+// Geometry of the split stores of a plan (SplitDev without base pointers);
+// returns the pairs one time buffer holds. Slab stores span whole x rows
+// (pitch) except the x faces, whose rows hold at least 16 pairs from an even
+// origin so their TMA boxes start on 16 bytes.
+size_t split_layout(const SplitPlan& plan, int nx, int ny, int nz, int pitch, SplitDev& g) {
+  g = SplitDev{};
+  const int* t = plan.t;
+  for (int k = 0; k < 6; ++k) g.t[k] = t[k];
+  const int zc0 = t[4], zc = std::max(0, nz - t[4] - t[5]);
+  auto set = [&](int st, int ox, int oy, int oz, int w, int h, int d) {
+    g.ox[st] = ox; g.oy[st] = oy; g.oz[st] = oz; g.w[st] = w; g.h[st] = h;
+    g.comp[st] = int64_t(w) * h * d;
+  };
+  set(kStZlo, 0, 0, 0, pitch, ny, t[4]);
+  set(kStZhi, 0, 0, nz - t[5], pitch, ny, t[5]);
+  set(kStYlo, 0, 0, zc0, pitch, t[2], zc);
+  set(kStYhi, 0, ny - t[3], zc0, pitch, t[3], zc);
+  const int wxl = t[0] ? std::max(16, (t[0] + 1) & ~1) : 0;
+  const int oxh = (nx - t[1]) & ~1;
+  const int wxh = t[1] ? std::max(16, (nx - oxh + 1) & ~1) : 0;
+  set(kStXlo, 0, 0, zc0, wxl, ny, zc);
+  set(kStXhi, oxh, 0, zc0, wxh, ny, zc);
+  int64_t off = 0;
+  for (int st = 0; st < 6; ++st) {
+    g.off[st] = off;
+    off += 6 * g.comp[st];
+  }
+  g.off[kStSparse] = off;
+  off += 6 * plan.n_sparse;
+  return size_t(off);
+}
+
 void compile_host(fdtd_sim* s) {
   if (s->compiled) return;
   for (int i = 0; i < kNumCoef; ++i)
@@ -1044,6 +1092,7 @@ void compile_host(fdtd_sim* s) {
   std::string err;
   if (!compile_grid(s->nx, s->ny, s->nz, cp, s->probes, threads_for_host(), s->grid, err))
     throw ArgError{FDTD_ERR_LIMIT, err};
+  if (!plan_split_storage(s->grid, s->split_plan, err)) throw ArgError{FDTD_ERR_LIMIT, err};
   s->compiled = true;
   s->base_rows = int(s->grid.rows.size());
   s->box_rows_from = -1;
@@ -1065,8 +1114,10 @@ void prepare(fdtd_sim* s, int nt) {
       throw ArgError{FDTD_ERR_LIMIT, "Grid too large for 32-bit cell offsets."};
     const size_t N = s->cells_padded;
     s->fields.alloc(12 * N);
+    // split pairs only in the slab stores and the sparse store
+    s->split_buf_pairs = split_layout(s->split_plan, nx, ny, nz, s->pitch, s->split_geo);
     const bool any_split = s->grid.e_split_cells > 0 || s->grid.h_split_cells > 0;
-    s->splits.alloc(any_split ? 24 * N : 0);
+    s->splits.alloc(any_split ? 2 * 2 * s->split_buf_pairs : 0);
     // material index: upload in reference order, transpose on the device
     {
       DevBuf<uint16_t> tmp;
@@ -1143,11 +1194,10 @@ void prepare(fdtd_sim* s, int nt) {
       d.E[b][c] = s->fields.p + (size_t(b) * 6 + c) * N;
       d.H[b][c] = s->fields.p + (size_t(b) * 6 + 3 + c) * N;
     }
-    // split pairs: component c of E at float offset (12 b + 2 c) N, of H at (12 b + 6 + 2 c) N
-    for (int c = 0; c < 3; ++c) {
-      d.Es[b][c] = s->splits.n ? reinterpret_cast<float2*>(s->splits.p + (size_t(b) * 12 + 2 * c) * N) : nullptr;
-      d.Hs[b][c] = s->splits.n ? reinterpret_cast<float2*>(s->splits.p + (size_t(b) * 12 + 6 + 2 * c) * N) : nullptr;
-    }
+    // split pairs of time buffer b: the stores back to back
+    d.sp = s->split_geo;
+    for (int bb = 0; bb < 2; ++bb)
+      d.sp.base[bb] = s->splits.n ? reinterpret_cast<float2*>(s->splits.p) + size_t(bb) * s->split_buf_pairs : nullptr;
   }
   d.mat = s->mat.p;
   d.rows = s->rows.p;
@@ -1632,7 +1682,7 @@ int fdtd_run_checkpointed(fdtd_sim* s, int nt, int every) {
                          s->ckpt_every != every || s->ckpt_nt != nt;
     prepare(s, nt);
     const size_t N = s->cells_padded;
-    const size_t stride = 6 * N + (s->splits.n ? 12 * N : 0);
+    const size_t stride = 6 * N + (s->splits.n ? 2 * s->split_buf_pairs : 0);
     const size_t nseg = size_t((nt + every - 1) / every);
     if (rebuild) {
       leave_adjoint_mode(s);
@@ -1740,6 +1790,12 @@ int fdtd_get_stats(const fdtd_sim* s, fdtd_stats* out) {
   *out = s->stats;
   out->h2d_bytes = s->h2d_bytes;
   out->d2h_bytes = s->d2h_bytes;
+  if (s->compiled) {
+    for (int k = 0; k < 6; ++k) out->split_slab[k] = s->split_plan.t[k];
+    out->slab_cells = s->split_plan.slab_cells;
+    out->sparse_split_cells = s->split_plan.sparse_cells;
+    out->split_bytes = int64_t(s->splits.n * sizeof(float));
+  }
   return FDTD_OK;
 }
 
@@ -2108,11 +2164,14 @@ extern "C" int fdtd_step_noalloc(const fdtd_device_grid* g, int n0, int n_steps,
         d.E[b][c] = g->fields + (size_t(b) * 6 + c) * N;
         d.H[b][c] = g->fields + (size_t(b) * 6 + 3 + c) * N;
       }
-      for (int c = 0; c < 3; ++c) {
-        d.Es[b][c] = reinterpret_cast<float2*>(g->splits + (size_t(b) * 12 + 2 * c) * N);
-        d.Hs[b][c] = reinterpret_cast<float2*>(g->splits + (size_t(b) * 12 + 6 + 2 * c) * N);
-      }
     }
+    // the caller's splits cover the whole grid: one z-face store holding every
+    // cell, component m of time buffer b at pairs (6 b + m) N
+    d.sp.t[4] = nz;
+    d.sp.w[kStZlo] = pitch;
+    d.sp.h[kStZlo] = ny;
+    d.sp.comp[kStZlo] = int64_t(N);
+    for (int b = 0; b < 2; ++b) d.sp.base[b] = reinterpret_cast<float2*>(g->splits) + size_t(b) * 6 * N;
     d.mat = g->mat;
     d.rows = reinterpret_cast<const float4*>(g->rows);
     d.cell_probes = reinterpret_cast<const int2*>(g->cell_probes);

@@ -44,6 +44,49 @@ constexpr uint32_t kESplit = 1u, kHSplit = 2u;
 constexpr uint32_t kCompSplit0 = 1u << 8;
 
 
+// Split-pair storage of one simulation. The cells of the PML slabs keep their
+// six split pairs ((ex_y ex_z) (ey_z ey_x) (ez_x ez_y) (hx_y hx_z) (hy_z hy_x)
+// (hz_x hz_y)) in six slab stores, one per face, each a box [6][depth][h][w]
+// of pairs at origin (ox, oy, oz); a cell belongs to the first of the z
+// faces, the y faces, the x faces whose slab (thickness t) holds it. A split
+// cell in no slab (a soft-source cell) is "sparse": its six pairs sit at the
+// slot named by its table row's word 31 in the sparse store [slot][6]. Per
+// time buffer the stores lie back to back from base[b].
+constexpr int kStXlo = 0, kStXhi = 1, kStYlo = 2, kStYhi = 3, kStZlo = 4, kStZhi = 5, kStSparse = 6;
+
+struct SplitDev {
+  float2* base[2];
+  int t[6];                            // slab thickness: x-lo, x-hi, y-lo, y-hi, z-lo, z-hi
+  int ox[6], oy[6], oz[6], w[6], h[6];  // slab stores: origin, row pitch (pairs), rows per plane
+  int64_t off[7];                      // pair offset of each store inside a time buffer
+  int64_t comp[6];                     // pairs per component of each slab store
+};
+
+// Store holding the split pairs of cell (x, y, z).
+__host__ __device__ __forceinline__ int split_store(const SplitDev& S, int nx, int ny, int nz, int x, int y,
+                                                    int z) {
+  if (z < S.t[4]) return kStZlo;
+  if (z >= nz - S.t[5]) return kStZhi;
+  if (y < S.t[2]) return kStYlo;
+  if (y >= ny - S.t[3]) return kStYhi;
+  if (x < S.t[0]) return kStXlo;
+  if (x >= nx - S.t[1]) return kStXhi;
+  return kStSparse;
+}
+
+// Pair of component 0 of cell (x, y, z) in store st of time buffer b (slot:
+// the cell's row word 31, used by the sparse store); component m lies m *
+// stride pairs further.
+__device__ __forceinline__ float2* split_ptr(const SplitDev& S, int b, int st, int x, int y, int z, int slot,
+                                             int64_t& stride) {
+  if (st == kStSparse) {
+    stride = 1;
+    return S.base[b] + S.off[kStSparse] + int64_t(slot) * 6;
+  }
+  stride = S.comp[st];
+  return S.base[b] + S.off[st] + (int64_t(z - S.oz[st]) * S.h[st] + (y - S.oy[st])) * S.w[st] + (x - S.ox[st]);
+}
+
 struct SimDev {
   const void* maps;       // tensor maps of the streaming kernel (set per engine)
   int nx, ny, nz, pitch;  // cells; pitch = floats per x row
@@ -51,10 +94,7 @@ struct SimDev {
   int nt;
   float* E[2][3];         // [buffer][ex, ey, ez]
   float* H[2][3];         // [buffer][hx, hy, hz]
-  // split pairs; Es[b][c] + (3 + c') * cells == Hs[b][c'] and components are
-  // `cells` pairs apart (the streaming kernel indexes them from Es[b][0])
-  float2* Es[2][3];       // [buffer][(ex_y, ex_z), (ey_z, ey_x), (ez_x, ez_y)]
-  float2* Hs[2][3];       // [buffer][(hx_y, hx_z), (hy_z, hy_x), (hz_x, hz_y)]
+  SplitDev sp;            // split pairs of the split cells
   const uint16_t* mat;    // [z][y][pitch]
   const float4* rows;     // 8 float4 per row
   const int2* cell_probes;  // (probe, field) grouped per probe cell
@@ -165,24 +205,26 @@ fdtd_step_kernel(const SimDev* __restrict__ sims, const int4* __restrict__ tiles
         ez = upd_e(d.x, __ldg(Ez + idx), d.y, dhy_x, d.w, dhx_y);
       } else {
         // per component: split pair (ex_y, ex_z), ... or unsplit total
-        float2* const* Es = S.Es[cur];
+        const int st = split_store(S.sp, nx, ny, nz, c, r, z);
+        int64_t cs;
+        const float2* Es = split_ptr(S.sp, cur, st, c, r, z, __float_as_int(rw7.w), cs);
         float2 p0 = make_float2(0.f, 0.f), p1 = p0, p2 = p0;
         if (flags & (kCompSplit0 << 0)) {
-          p0 = __ldg(Es[0] + idx);
+          p0 = __ldg(Es);
           p0.x = upd_e_split(a.x, p0.x, a.y, dhz_y);  // ex_y
           p0.y = upd_e_split(a.z, p0.y, a.w, dhy_z);  // ex_z
         } else {
           ex = upd_e(a.x, __ldg(Ex + idx), a.y, dhz_y, a.w, dhy_z);
         }
         if (flags & (kCompSplit0 << 1)) {
-          p1 = __ldg(Es[1] + idx);
+          p1 = __ldg(Es + cs);
           p1.x = upd_e_split(b.x, p1.x, b.y, dhx_z);  // ey_z
           p1.y = upd_e_split(b.z, p1.y, b.w, dhz_x);  // ey_x
         } else {
           ey = upd_e(b.x, __ldg(Ey + idx), b.y, dhx_z, b.w, dhz_x);
         }
         if (flags & (kCompSplit0 << 2)) {
-          p2 = __ldg(Es[2] + idx);
+          p2 = __ldg(Es + 2 * cs);
           p2.x = upd_e_split(d.x, p2.x, d.y, dhy_x);  // ez_x
           p2.y = upd_e_split(d.z, p2.y, d.w, dhx_y);  // ez_y
         } else {
@@ -203,19 +245,19 @@ fdtd_step_kernel(const SimDev* __restrict__ sims, const int4* __restrict__ tiles
             }
           }
         }
-        const bool st = own && z >= z0;
-        float2* const* Eo = S.Es[nxt];
+        const bool stor = own && z >= z0;
+        float2* Eo = split_ptr(S.sp, nxt, st, c, r, z, __float_as_int(rw7.w), cs);
         if (flags & (kCompSplit0 << 0)) {
           ex = __fadd_rn(p0.x, p0.y);
-          if (st) Eo[0][idx] = p0;
+          if (stor) Eo[0] = p0;
         }
         if (flags & (kCompSplit0 << 1)) {
           ey = __fadd_rn(p1.x, p1.y);
-          if (st) Eo[1][idx] = p1;
+          if (stor) Eo[cs] = p1;
         }
         if (flags & (kCompSplit0 << 2)) {
           ez = __fadd_rn(p2.x, p2.y);
-          if (st) Eo[2][idx] = p2;
+          if (stor) Eo[2 * cs] = p2;
         }
       }
     }
@@ -254,24 +296,26 @@ fdtd_step_kernel(const SimDev* __restrict__ sims, const int4* __restrict__ tiles
         hy = upd_h(da_yz, hy_c, gyz, gyx);
         hz = upd_h(da_zx, hz_c, gzx, gzy);
       } else {
-        const float2* const* Hs = S.Hs[cur];
+        const int st = split_store(S.sp, nx, ny, nz, c, r, z);
+        int64_t cs;
+        const float2* Hs = split_ptr(S.sp, cur, st, c, r, z, __float_as_int(rw7.w), cs) + 3 * cs;
         float2 p0 = make_float2(0.f, 0.f), p1 = p0, p2 = p0;
         if (flags & (kCompSplit0 << 3)) {
-          p0 = __ldg(Hs[0] + idx);
+          p0 = __ldg(Hs);
           p0.x = upd_h_split(da_xy, p0.x, gxy);
           p0.y = upd_h_split(da_xz, p0.y, gxz);
         } else {
           hx = upd_h(da_xy, hx_c, gxy, gxz);
         }
         if (flags & (kCompSplit0 << 4)) {
-          p1 = __ldg(Hs[1] + idx);
+          p1 = __ldg(Hs + cs);
           p1.x = upd_h_split(da_yz, p1.x, gyz);
           p1.y = upd_h_split(da_yx, p1.y, gyx);
         } else {
           hy = upd_h(da_yz, hy_c, gyz, gyx);
         }
         if (flags & (kCompSplit0 << 5)) {
-          p2 = __ldg(Hs[2] + idx);
+          p2 = __ldg(Hs + 2 * cs);
           p2.x = upd_h_split(da_zx, p2.x, gzx);
           p2.y = upd_h_split(da_zy, p2.y, gzy);
         } else {
@@ -290,18 +334,18 @@ fdtd_step_kernel(const SimDev* __restrict__ sims, const int4* __restrict__ tiles
             }
           }
         }
-        float2* const* Ho = S.Hs[nxt];
+        float2* Ho = split_ptr(S.sp, nxt, st, c, r, z, __float_as_int(rw7.w), cs) + 3 * cs;
         if (flags & (kCompSplit0 << 3)) {
           hx = __fadd_rn(p0.x, p0.y);
-          Ho[0][idx] = p0;
+          Ho[0] = p0;
         }
         if (flags & (kCompSplit0 << 4)) {
           hy = __fadd_rn(p1.x, p1.y);
-          Ho[1][idx] = p1;
+          Ho[cs] = p1;
         }
         if (flags & (kCompSplit0 << 5)) {
           hz = __fadd_rn(p2.x, p2.y);
-          Ho[2][idx] = p2;
+          Ho[2 * cs] = p2;
         }
       }
       S.H[nxt][0][idx] = hx;
@@ -424,11 +468,14 @@ __global__ void monitor_kernel(const SimDev* __restrict__ sim, const MonDev* __r
       else { x = a; y = b; z = M.position; }
       if (x < 0 || y < 0 || z < 0 || x >= S.nx || y >= S.ny || z >= S.nz) continue;
       const int idx = z * S.plane + y * S.pitch + x;
-      const uint32_t flags = __float_as_uint(S.rows[8 * S.mat[idx] + 7].z);
+      const float4 r7 = S.rows[8 * S.mat[idx] + 7];
+      const uint32_t flags = __float_as_uint(r7.z);
       float v;
       if (M.field < 3) {
         if (flags & (kCompSplit0 << M.field)) {
-          const float2 p = S.Es[buf][M.field][idx];
+          int64_t cs;
+          const float2 p = split_ptr(S.sp, buf, split_store(S.sp, S.nx, S.ny, S.nz, x, y, z), x, y, z,
+                                     __float_as_int(r7.w), cs)[M.field * cs];
           v = p.x + p.y;
         } else {
           v = S.E[buf][M.field][idx];

@@ -17,12 +17,14 @@
 //               H^n     3 components, rows y0-1 .. y0+TY, 40 columns
 //               E^n     3 components, rows y0-1 .. y0+TY-1, 36 columns
 //               index   16-bit material rows, 40 columns
-//               splits  the 3 E and 3 H split pairs (float2 per cell), only
-//                       for planes the host flagged as holding split-field
-//                       cells (PML slabs, soft sources) -- a 64-bit mask per
-//                       tile; over 36 columns, or over the 16-column window [wx0, wx0+16)
-//                       on planes whose split cells all lie in it (the x-PML
-//                       slab crossing an ordinary tile), a second mask
+//               splits  the 3 E and 3 H split pairs (float2 per cell) over
+//                       36 columns, only for planes the host flagged as holding
+//                       split-field cells (a 64-bit mask per tile), from at
+//                       most two slab stores (SplitDev): the plane's z-face
+//                       store, or the tile's y-face store and x-face store.
+//                       Split cells of other stores (soft-source cells, the
+//                       rare corner of a small grid) are read from global
+//                       memory directly
 //             Every box starts at an x that is a multiple of 16 bytes at or
 //             below x0-1; the consumers index from that offset. Boxes reaching
 //             outside the grid fill with zeros and a zero material index
@@ -51,22 +53,21 @@ constexpr int kStreamOwnX = 31;           // owned columns per tile (lane 0 is t
 constexpr uint32_t kStreamWaitLimit = 1u << 20;  // sleeping polls (each <= 2 us) per wait
 constexpr int kStreamBar = 1;             // named barrier of the consumer warps
 
-constexpr int kStreamWin = 16;            // columns of a narrow split window
-
-// Tensor maps of one simulation for the streaming kernel (split maps over 36
-// columns and over a 16-column window).
+// Tensor maps of one simulation for the streaming kernel: the fields, the
+// material index, and the E and H split pairs of each slab store.
 struct StreamMaps {
-  CUtensorMap E, H, ids, Es, Hs, Es16, Hs16;
+  CUtensorMap E, H, ids, Es[6], Hs[6];
 };
 
 // One tile: owned [x0, x0+31) x [y0, y0+TY) x [z0, z1). Bit j of `split` is
-// set when plane z0-1+j holds split-field cells inside the tile's E region;
-// bit j of `narrow` when all of them lie in columns [wx0, wx0+16). `plain`
-// marks a tile with no split-field cells and no probe cells, which takes the
-// consumers' interior path (no per-cell flag tests).
+// set when plane z0-1+j holds split-field cells inside the tile's E region.
+// On planes outside the z slabs the tile's split pairs come from slab store
+// ys (a y face, or -1) and xs (an x face, or -1). `plain` marks a tile with no
+// split-field cells and no probe cells, which takes the consumers' interior
+// path (no per-cell flag tests).
 struct StreamTile {
-  int sim, x0, y0, z0, z1, wx0, plain, pad1;
-  uint32_t split_lo, split_hi, narrow_lo, narrow_hi;
+  int sim, x0, y0, z0, z1, ys, plain, xs;
+  uint32_t split_lo, split_hi, pad2, pad3;
 };
 
 template <int TY>
@@ -85,13 +86,11 @@ struct StreamGeom {
   static constexpr int OFF_E = A(HB);
   static constexpr int OFF_I = OFF_E + A(EB);
   static constexpr uint32_t MAIN = OFF_I + A(IB);  // plane slot: H, E, index
-  static constexpr uint32_t SPLIT_HS = A(SEB);     // H pairs inside a split slot
-  static constexpr uint32_t SPLIT = A(SEB) + A(SHB); // split slot: E pairs, then H pairs
+  static constexpr uint32_t SPLIT_HS = A(SEB);     // H pairs inside a split region
+  static constexpr uint32_t REGION = A(SEB) + A(SHB); // one store's E pairs, then H pairs
+  static constexpr uint32_t SPLIT = 2 * REGION;    // split slot: regions A and B
   static constexpr uint32_t MAIN_BYTES = HB + EB + IB;
   static constexpr uint32_t SPLIT_BYTES = SEB + SHB;
-  static constexpr int SECN = ER * kStreamWin;     // float2 pairs per E split pair, narrow window
-  static constexpr int SHCN = TY * kStreamWin;     // float2 pairs per H split pair, narrow window
-  static constexpr uint32_t SPLIT_BYTES_N = 6 * (SECN + SHCN) * 4;
   static constexpr int NCW = TY + 1;               // consumer warps
   static constexpr int CONSUMERS = 32 * NCW;
   static constexpr int THREADS = CONSUMERS + 32;   // + the producer warp
@@ -201,22 +200,25 @@ fdtd_step_stream_kernel(const SimDev* __restrict__ sims, const StreamTile* __res
       const int t = v < unsigned(n_tiles) ? int(v) : -1;
       StreamTile td{};
       int nload = 1;
-      uint64_t mask = 0, narrow = 0;
+      uint64_t mask = 0;
       const StreamMaps* maps = nullptr;
+      const SplitDev* sp = nullptr;
+      int snz = 0;
       if (t >= 0) {
         td = load_stream_tile(tiles, t);
         nload = td.z1 - td.z0 + 2;  // planes z0-1 .. z1
         mask = uint64_t(td.split_lo) | (uint64_t(td.split_hi) << 32);
-        narrow = uint64_t(td.narrow_lo) | (uint64_t(td.narrow_hi) << 32);
         maps = reinterpret_cast<const StreamMaps*>(sims[td.sim].maps);
+        sp = &sims[td.sim].sp;
+        snz = sims[td.sim].nz;
         if (maps != cur_maps) {
           tensormap_acquire(&maps->E);
           tensormap_acquire(&maps->H);
           tensormap_acquire(&maps->ids);
-          tensormap_acquire(&maps->Es);
-          tensormap_acquire(&maps->Hs);
-          tensormap_acquire(&maps->Es16);
-          tensormap_acquire(&maps->Hs16);
+          for (int st = 0; st < 6; ++st) {
+            tensormap_acquire(&maps->Es[st]);
+            tensormap_acquire(&maps->Hs[st]);
+          }
           cur_maps = maps;
         }
       }
@@ -224,7 +226,17 @@ fdtd_step_stream_kernel(const SimDev* __restrict__ sims, const StreamTile* __res
       for (int j = 0; j < nload; ++j) {
         const bool last = t >= 0 && j == nload - 1;
         const bool split = t >= 0 && !last && ((mask >> j) & 1u);
-        const bool win = (narrow >> j) & 1u;
+        // slab stores staged for this plane: regions A and B of its split slot
+        int sa = -1, sbs = -1;
+        const int zp = td.z0 - 1 + j;
+        if (split) {
+          if (zp < sp->t[4]) sa = kStZlo;
+          else if (zp >= snz - sp->t[5]) sa = kStZhi;
+          else {
+            sa = td.ys;
+            sbs = td.xs;
+          }
+        }
         // the plane slot's previous plane, and the split slot's last user, must be released
         if (q >= uint32_t(P) && !release_upto(q - P)) {
           failed = true;
@@ -258,22 +270,23 @@ fdtd_step_stream_kernel(const SimDev* __restrict__ sims, const StreamTile* __res
         unsigned char* b = ring + uint32_t(slot) * G::MAIN;
         unsigned char* sb = ring + soff;
         uint64_t* fb = &full[slot];
-        const int zp = td.z0 - 1 + j;
         fence_proxy_async();
-        mbar_arrive_expect_tx(fb, last    ? uint32_t(G::HB)
-                                  : !split ? G::MAIN_BYTES
-                                           : G::MAIN_BYTES + (win ? G::SPLIT_BYTES_N : G::SPLIT_BYTES));
+        mbar_arrive_expect_tx(fb, last ? uint32_t(G::HB)
+                                       : G::MAIN_BYTES + (sa >= 0 ? G::SPLIT_BYTES : 0u) +
+                                             (sbs >= 0 ? G::SPLIT_BYTES : 0u));
         tma_load_5d(b, &maps->H, xs, td.y0 - 1, zp, 0, cur, fb);
         if (!last) {
           tma_load_5d(b + G::OFF_E, &maps->E, xs, td.y0 - 1, zp, 0, cur, fb);
           tma_load_3d(b + G::OFF_I, &maps->ids, xi, td.y0 - 1, zp, fb);
-          // split pairs are interleaved along x: float column 2x holds cell x
-          if (split && win) {
-            tma_load_5d(sb, &maps->Es16, 2 * td.wx0, td.y0 - 1, zp, 0, cur, fb);
-            tma_load_5d(sb + G::SPLIT_HS, &maps->Hs16, 2 * td.wx0, td.y0, zp, 0, cur, fb);
-          } else if (split) {
-            tma_load_5d(sb, &maps->Es, 2 * xs, td.y0 - 1, zp, 0, cur, fb);
-            tma_load_5d(sb + G::SPLIT_HS, &maps->Hs, 2 * xs, td.y0, zp, 0, cur, fb);
+          // split pairs are interleaved along x (float column 2x holds cell
+          // x), in each store's own coordinates (origin ox, oy, oz)
+          for (int rgn = 0; rgn < 2; ++rgn) {
+            const int st = rgn == 0 ? sa : sbs;
+            if (st < 0) continue;
+            unsigned char* d = sb + rgn * G::REGION;
+            const int sx = 2 * (xs - sp->ox[st]), sz = zp - sp->oz[st];
+            tma_load_5d(d, &maps->Es[st], sx, td.y0 - 1 - sp->oy[st], sz, 0, cur, fb);
+            tma_load_5d(d + G::SPLIT_HS, &maps->Hs[st], sx, td.y0 - sp->oy[st], sz, 0, cur, fb);
           }
         }
         ++q;
@@ -317,17 +330,12 @@ fdtd_step_stream_kernel(const SimDev* __restrict__ sims, const StreamTile* __res
     const int plane = Sd.plane;
     const int64_t N = Sd.cells;
     float* __restrict__ const fo = Sd.E[nxt][0];   // E then H components of step n+1, N apart
-    // split pairs of step n+1: E component m at m N, H component m at (3 + m) N
-    float2* __restrict__ const spo = Sd.Es[nxt][0];
     const int npl = td.z1 - z0 + 1;                // planes z0-1 .. z1-1 computed
     const int hb = w * G::HW + oh + lane;
     const int eb = w * G::EW + oh + lane;
     const int ib = w * G::IW + oi + lane;
     const int sb = (w - 1) * G::EW + oh + lane;    // H split box (owned rows)
-    // narrow window: this cell's column inside [wx0, wx0+16) when it is a split cell there
-    const int wc = c - td.wx0;
-    const int ebn = w * kStreamWin + wc, sbn = (w - 1) * kStreamWin + wc;
-    const uint64_t narrow = uint64_t(td.narrow_lo) | (uint64_t(td.narrow_hi) << 32);
+    const uint64_t smask = uint64_t(td.split_lo) | (uint64_t(td.split_hi) << 32);
     int idx = (z0 - 1) * plane + r * Sd.pitch + c; // cell offset of plane z (owned cells, z >= z0)
 
     // The plane loop, instantiated for plain tiles (FAST: every cell unsplit,
@@ -344,13 +352,30 @@ fdtd_step_stream_kernel(const SimDev* __restrict__ sims, const StreamTile* __res
         const float* sE = reinterpret_cast<const float*>(st + G::OFF_E);
         const uint16_t* sI = reinterpret_cast<const uint16_t*>(st + G::OFF_I);
         const unsigned char* ss = ring + s_soff[cp.slot];
-        const float* sEs = reinterpret_cast<const float*>(ss);
-        const float* sHs = reinterpret_cast<const float*>(ss + G::SPLIT_HS);
         const float* nH = reinterpret_cast<const float*>(ring + np.slot * G::MAIN);
         float* xb = xch + (i & 1) * (G::XCH / 4);
         constexpr int HC = G::HC, EC = G::EC;
         const bool store = own_xy && i > 0;
-        const bool win = (narrow >> i) & 1u;
+        const int z = z0 - 1 + i;
+        // split pairs of this plane: the slab stores staged in regions A and B
+        // of its split slot (as the producer chose them), other stores and
+        // sparse cells from global memory
+        int sa = -1, sbs = -1;
+        if (!FAST && ((smask >> i) & 1u)) {
+          if (z < Sd.sp.t[4]) sa = kStZlo;
+          else if (z >= Sd.nz - Sd.sp.t[5]) sa = kStZhi;
+          else {
+            sa = td.ys;
+            sbs = td.xs;
+          }
+        }
+        // the E (h = 0) or H (h = 3) pair of component m of this cell, from
+        // the staged region or the store; `cst` is the cell's store
+        auto pair_in = [&](int cst, int rgn, int m, const float2* gp, int64_t cs) -> float2 {
+          if (rgn < 0) return __ldg(gp + m * cs);
+          const float2* r2 = reinterpret_cast<const float2*>(ss + rgn * G::REGION);
+          return m < 3 ? r2[m * EC + eb] : reinterpret_cast<const float2*>(ss + rgn * G::REGION + G::SPLIT_HS)[(m - 3) * G::SHC + sb];
+        };
 
         // ------------------------------------------------------------ E phase
         // (after an expired wait the values are stale but in bounds; the vote
@@ -379,28 +404,30 @@ fdtd_step_stream_kernel(const SimDev* __restrict__ sims, const StreamTile* __res
           ey = upd_e(rb.x, sE[EC + eb], rb.y, dhx_z, rb.w, dhz_x);
           ez = upd_e(rd.x, sE[2 * EC + eb], rd.y, dhy_x, rd.w, dhx_y);
         } else {
-          // per component: the split pair (one 8-byte load at the selected
-          // offset) or the unsplit total
+          // per component: the split pair (one 8-byte load) or the unsplit total
           float2 sp[3];
-          const float2* sP = reinterpret_cast<const float2*>(sEs);
+          const int cst = split_store(Sd.sp, Sd.nx, Sd.ny, Sd.nz, c, r, z);
+          const int rgn = cst == sa ? 0 : cst == sbs ? 1 : -1;
+          int64_t cs = 0;
+          const float2* gp = rgn < 0 ? split_ptr(Sd.sp, cur, cst, c, r, z, __float_as_int(r7.w), cs) : nullptr;
   #pragma unroll
           for (int m = 0; m < 3; ++m) sp[m] = make_float2(0.f, 0.f);
           if (flags & (kCompSplit0 << 0)) {
-            sp[0] = sP[win ? ebn : eb];
+            sp[0] = pair_in(cst, rgn, 0, gp, cs);
             sp[0].x = upd_e_split(ra.x, sp[0].x, ra.y, dhz_y);  // ex_y
             sp[0].y = upd_e_split(ra.z, sp[0].y, ra.w, dhy_z);  // ex_z
           } else {
             ex = upd_e(ra.x, sE[eb], ra.y, dhz_y, ra.w, dhy_z);
           }
           if (flags & (kCompSplit0 << 1)) {
-            sp[1] = sP[win ? G::SECN + ebn : EC + eb];
+            sp[1] = pair_in(cst, rgn, 1, gp, cs);
             sp[1].x = upd_e_split(rb.x, sp[1].x, rb.y, dhx_z);  // ey_z
             sp[1].y = upd_e_split(rb.z, sp[1].y, rb.w, dhz_x);  // ey_x
           } else {
             ey = upd_e(rb.x, sE[EC + eb], rb.y, dhx_z, rb.w, dhz_x);
           }
           if (flags & (kCompSplit0 << 2)) {
-            sp[2] = sP[win ? 2 * G::SECN + ebn : 2 * EC + eb];
+            sp[2] = pair_in(cst, rgn, 2, gp, cs);
             sp[2].x = upd_e_split(rd.x, sp[2].x, rd.y, dhy_x);  // ez_x
             sp[2].y = upd_e_split(rd.z, sp[2].y, rd.w, dhx_y);  // ez_y
           } else {
@@ -411,9 +438,10 @@ fdtd_step_stream_kernel(const SimDev* __restrict__ sims, const StreamTile* __res
           if (flags & (kCompSplit0 << 1)) ey = __fadd_rn(sp[1].x, sp[1].y);
           if (flags & (kCompSplit0 << 2)) ez = __fadd_rn(sp[2].x, sp[2].y);
           if (store) {
+            float2* po = split_ptr(Sd.sp, nxt, cst, c, r, z, __float_as_int(r7.w), cs);
   #pragma unroll
             for (int m = 0; m < 3; ++m)
-              if (flags & (kCompSplit0 << m)) spo[m * N + idx] = sp[m];
+              if (flags & (kCompSplit0 << m)) po[m * cs] = sp[m];
           }
         }
         xb[w * 32 + lane] = ex;
@@ -448,25 +476,28 @@ fdtd_step_stream_kernel(const SimDev* __restrict__ sims, const StreamTile* __res
             hz = upd_h(rv.x, hz_c, gzx, gzy);
           } else {
             float2 sp[3];
-            const float2* sP = reinterpret_cast<const float2*>(sHs);
+            const int cst = split_store(Sd.sp, Sd.nx, Sd.ny, Sd.nz, c, r, z);
+            const int rgn = cst == sa ? 0 : cst == sbs ? 1 : -1;
+            int64_t cs = 0;
+            const float2* gp = rgn < 0 ? split_ptr(Sd.sp, cur, cst, c, r, z, __float_as_int(r7.w), cs) : nullptr;
   #pragma unroll
             for (int m = 0; m < 3; ++m) sp[m] = make_float2(0.f, 0.f);
             if (flags & (kCompSplit0 << 3)) {
-              sp[0] = sP[win ? sbn : sb];
+              sp[0] = pair_in(cst, rgn, 3, gp, cs);
               sp[0].x = upd_h_split(rp.x, sp[0].x, gxy);
               sp[0].y = upd_h_split(rp.w, sp[0].y, gxz);
             } else {
               hx = upd_h(rp.x, hx_c, gxy, gxz);
             }
             if (flags & (kCompSplit0 << 4)) {
-              sp[1] = sP[win ? G::SHCN + sbn : G::SHC + sb];
+              sp[1] = pair_in(cst, rgn, 4, gp, cs);
               sp[1].x = upd_h_split(rq.z, sp[1].x, gyz);
               sp[1].y = upd_h_split(ru.y, sp[1].y, gyx);
             } else {
               hy = upd_h(rq.z, hy_c, gyz, gyx);
             }
             if (flags & (kCompSplit0 << 5)) {
-              sp[2] = sP[win ? 2 * G::SHCN + sbn : 2 * G::SHC + sb];
+              sp[2] = pair_in(cst, rgn, 5, gp, cs);
               sp[2].x = upd_h_split(rv.x, sp[2].x, gzx);
               sp[2].y = upd_h_split(rv.w, sp[2].y, gzy);
             } else {
@@ -476,9 +507,10 @@ fdtd_step_stream_kernel(const SimDev* __restrict__ sims, const StreamTile* __res
             if (flags & (kCompSplit0 << 3)) hx = __fadd_rn(sp[0].x, sp[0].y);
             if (flags & (kCompSplit0 << 4)) hy = __fadd_rn(sp[1].x, sp[1].y);
             if (flags & (kCompSplit0 << 5)) hz = __fadd_rn(sp[2].x, sp[2].y);
+            float2* po = split_ptr(Sd.sp, nxt, cst, c, r, z, __float_as_int(r7.w), cs);
   #pragma unroll
             for (int m = 0; m < 3; ++m)
-              if (flags & (kCompSplit0 << (3 + m))) spo[(3 + m) * N + idx] = sp[m];
+              if (flags & (kCompSplit0 << (3 + m))) po[(3 + m) * cs] = sp[m];
           }
           fo[3 * N + idx] = hx;
           fo[4 * N + idx] = hy;

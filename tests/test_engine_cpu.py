@@ -176,3 +176,29 @@ def test_table_limit_is_reported(engine_lib):
     with pytest.raises(_lib.FdtdError, match="at most 65536"):
         sim.compile()
     sim.close()
+
+
+def test_split_storage_plan_confines_pml_pairs_to_the_slabs(engine_lib):
+    """The split pairs of the PML live in slab stores of the PML's thickness
+    (8 cells on every face here), and the only split cells outside them are
+    the ports' soft-source cells, each on a table row of its own."""
+    s = configs.boxes(n=(64, 56, 40), n_pml=8, n_boxes=6, nt=20, n_ports=2, n_probes=3)
+    co, pr, mo, mem, Nx, Ny, Nz, Nt = s.pack_inputs(gpu=True)
+    sim = _lib.Simulation(Nx, Ny, Nz)
+    sim.set_coefficients(co)
+    for p in pr:
+        sim.add_probe(p["field"], p["idx"], p["is_source"], p["values"][:Nt] if p["is_source"] else None)
+    sim.compile()
+    st = sim.stats()
+    ids, rows = sim.material_table()
+    sim.close()
+    assert st["split_slab"] == [8] * 6
+    n = Nx * Ny * Nz
+    assert st["slab_cells"] == n - (Nx - 16) * (Ny - 16) * (Nz - 16)
+    split = ((rows[:, 30] & 3) != 0)[ids]
+    inner = split[8:-8, 8:-8, 8:-8]
+    assert st["sparse_split_cells"] == int(inner.sum()) > 0
+    # the sparse cells are source cells; each has its own row
+    inner_ids = ids[8:-8, 8:-8, 8:-8][inner]
+    assert len(np.unique(inner_ids)) == len(inner_ids)
+    assert ((rows[inner_ids, 30] >> 16) > 0).all()   # they carry probe entries (the port sources)
