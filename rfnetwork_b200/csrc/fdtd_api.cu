@@ -300,15 +300,17 @@ const StreamVariant* find_stream_variant(int ty, int stages) {
 }
 
 // Dynamic shared bytes of a streaming block with (at most) `want` plane
-// slots and two or three split slots, sized for the kernel's resident blocks
-// per SM; the slot counts it fits go to n_main / n_split.
-uint32_t stream_slots(const StreamVariant& v, int want, int* n_main, int* n_split) {
+// slots and, when a simulation has split cells, two or three split slots,
+// sized for the kernel's resident blocks per SM; the slot counts it fits go to
+// n_main / n_split.
+uint32_t stream_slots(const StreamVariant& v, int want, bool splits, int* n_main, int* n_split) {
   constexpr uint32_t kSmemPerSm = 233472, kPerBlockReserve = 1024 + 512, kMaxPerBlock = 232448 - 512;
   const uint32_t budget = std::min(kSmemPerSm / v.min_blocks - kPerBlockReserve, kMaxPerBlock) - v.xch_bytes;
-  if (budget < 3 * v.main_bytes + 2 * v.split_bytes)
+  const uint32_t split_min = splits ? 2 * v.split_bytes : 0;
+  if (budget < 3 * v.main_bytes + split_min)
     throw ArgError{FDTD_ERR_LIMIT, "Streaming kernel's plane slots do not fit in shared memory."};
-  const uint32_t m = std::min<uint32_t>(uint32_t(std::min(want, kSlotsMax)), (budget - 2 * v.split_bytes) / v.main_bytes);
-  const uint32_t sp = std::min<uint32_t>(3, (budget - m * v.main_bytes) / v.split_bytes);
+  const uint32_t m = std::min<uint32_t>(uint32_t(std::min(want, kSlotsMax)), (budget - split_min) / v.main_bytes);
+  const uint32_t sp = splits ? std::min<uint32_t>(3, (budget - m * v.main_bytes) / v.split_bytes) : 0;
   *n_main = int(std::max<uint32_t>(m, 3));
   *n_split = int(sp);
   return v.xch_bytes + uint32_t(*n_main) * v.main_bytes + sp * v.split_bytes;
@@ -548,7 +550,12 @@ struct Engine {
       float best_ms = 1e30f;
       for (const auto& cand : kTuneCandidates) {
         apply({cand[0], cand[1], cand[2], cand[3]});
-        build_stream_tiles(n_sm);
+        try {
+          build_stream_tiles(n_sm);
+        } catch (const ArgError& e) {
+          if (e.code != FDTD_ERR_LIMIT) throw;
+          continue;  // this shape's slots do not fit next to these grids' split slots
+        }
         CK(cudaMemsetAsync(scls.d_counter.p, 0, sizeof(unsigned), st));
         for (int n = 0; n < warm; ++n) launch_step(st, n);
         CK(cudaEventRecord(ev0, st));
@@ -584,7 +591,9 @@ struct Engine {
       if (!c.v) throw ArgError{FDTD_ERR_ARG, "No streaming kernel instantiated for this tile height / stage count."};
       fn = reinterpret_cast<const void*>(c.v->fn);
       threads = c.v->threads;
-      c.ring = stream_slots(*c.v, cfg.stages, &c.n_main, &c.n_split);
+      bool splits = false;
+      for (auto* s : sims) splits = splits || s->splits.n > 0;
+      c.ring = stream_slots(*c.v, cfg.stages, splits, &c.n_main, &c.n_split);
       smem = int(c.ring);
       ty = c.v->ty;
     }

@@ -225,7 +225,7 @@ fdtd_step_stream_kernel(const SimDev* __restrict__ sims, const StreamTile* __res
       const int xs = (td.x0 - 1) & ~3, xi = (td.x0 - 1) & ~7;
       for (int j = 0; j < nload; ++j) {
         const bool last = t >= 0 && j == nload - 1;
-        const bool split = t >= 0 && !last && ((mask >> j) & 1u);
+        const bool split = t >= 0 && !last && n_split > 0 && ((mask >> j) & 1u);
         // slab stores staged for this plane: regions A and B of its split slot
         int sa = -1, sbs = -1;
         const int zp = td.z0 - 1 + j;
@@ -286,7 +286,8 @@ fdtd_step_stream_kernel(const SimDev* __restrict__ sims, const StreamTile* __res
             unsigned char* d = sb + rgn * G::REGION;
             const int sx = 2 * (xs - sp->ox[st]), sz = zp - sp->oz[st];
             tma_load_5d(d, &maps->Es[st], sx, td.y0 - 1 - sp->oy[st], sz, 0, cur, fb);
-            tma_load_5d(d + G::SPLIT_HS, &maps->Hs[st], sx, td.y0 - sp->oy[st], sz, 0, cur, fb);
+            // H pairs: components 3..5 of the store
+            tma_load_5d(d + G::SPLIT_HS, &maps->Hs[st], sx, td.y0 - sp->oy[st], sz, 3, cur, fb);
           }
         }
         ++q;
@@ -361,7 +362,7 @@ fdtd_step_stream_kernel(const SimDev* __restrict__ sims, const StreamTile* __res
         // of its split slot (as the producer chose them), other stores and
         // sparse cells from global memory
         int sa = -1, sbs = -1;
-        if (!FAST && ((smask >> i) & 1u)) {
+        if (!FAST && n_split > 0 && ((smask >> i) & 1u)) {
           if (z < Sd.sp.t[4]) sa = kStZlo;
           else if (z >= Sd.nz - Sd.sp.t[5]) sa = kStZhi;
           else {
