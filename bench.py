@@ -452,6 +452,42 @@ def reference_cuda_entry(ctx):
         return {"unavailable": f"{type(e).__name__}: {e}"}
 
 
+def reference_cuda_sequential(packed, nt, recs, cells_total):
+    """The batch's first members run one after another through the reference's own CUDA
+    engine (rfnetwork/core/src/solver.cu solver_run_cu, built unmodified into oracle/_ref:
+    allocation, copies, four kernel launches per step, read-back), as a user of the
+    reference runs them; wall time per member, scaled to the whole batch by the members'
+    cell-steps. Outside every timed region; a baseline, not the measurement."""
+    try:
+        from oracle import ref_cuda
+        if not ref_cuda.available():
+            return {"unavailable": "oracle/_ref/libref_cuda.so not built (needs the reference checkout at build time)"}
+        import torch
+        mem = np.zeros(0, np.float32)
+        co, pr, (Nx, Ny, Nz) = packed[0]
+        ref_cuda.solver_run_cu(co, copy.deepcopy(pr), [], mem, Nx, Ny, Nz, nt, 0, 0)  # warm-up
+        wall, cells, worst = 0.0, 0, 0.0
+        for (co, pr, (Nx, Ny, Nz)), ours in zip(packed, recs):
+            pr_ref = copy.deepcopy(pr)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            ref_cuda.solver_run_cu(co, pr_ref, [], mem, Nx, Ny, Nz, nt, 0, 0)
+            torch.cuda.synchronize()
+            wall += time.perf_counter() - t0
+            cells += Nx * Ny * Nz
+            ref_rec = np.stack([p["values"][:nt] for p in pr_ref])
+            worst = max(worst, float(np.linalg.norm(ours[:, :nt] - ref_rec) / np.linalg.norm(ref_rec)))
+        return {"members": len(packed), "time_steps": nt, "wall_s": round(wall, 3),
+                "sims_per_s": round(len(packed) / wall, 3),
+                "ms_per_batch": round(wall * 1e3 * cells_total / cells, 2),
+                "mcell_updates_per_s": round(cells * nt / wall / 1e6, 1),
+                "probe_rel_l2_vs_ours_max": worst,
+                "how": "wall time of solver_run_cu per member (allocation, copies, four launches per step, "
+                       "read-back); ms_per_batch scales the sample to all members by their cells"}
+    except Exception as e:  # a baseline, not the measurement: report why it is missing
+        return {"unavailable": f"{type(e).__name__}: {e}"}
+
+
 def workloads_entry(args, local_rank):
     """One timed run of each other workload (N = 1), summarised."""
     import argparse as _ap
@@ -584,6 +620,7 @@ def run_microstrip(args, rank, world, local_rank):
 BATCH_SIMS = 64
 BATCH_NT = 3000
 BATCH_FREQ = 21
+BATCH_REF_SAMPLE = 8   # members the reference CUDA engine runs one after another
 
 
 def run_batch(args, rank, world, local_rank):
@@ -598,10 +635,12 @@ def run_batch(args, rank, world, local_rank):
     torch.cuda.set_device(local_rank)
     ranks = RankSync(world, local_rank)
     nt = args.nt if args.nt != NT else BATCH_NT
-    sims, cells = [], 0
+    sims, cells, packed = [], 0, []
     for i in range(BATCH_SIMS):
         m = configs.batch_member(3, i, nt=nt)
         co, pr, mo, mem, Nx, Ny, Nz, Nt = m.pack_inputs(gpu=True)
+        if i < BATCH_REF_SAMPLE:
+            packed.append((co, copy.deepcopy(pr), (Nx, Ny, Nz)))
         sim = _lib.Simulation(Nx, Ny, Nz)
         sim.set_coefficients(co)
         for p in pr:
@@ -644,6 +683,7 @@ def run_batch(args, rank, world, local_rank):
             tot += s.stats()["last_run_ms"]
         t_plain.append(tot)
     same = same and all(np.array_equal(s.probe_values(), r) for s, r in zip(sims, recs))
+    ref_seq = reference_cuda_sequential(packed, nt, recs[:len(packed)], cells) if rank == 0 else None
     st = batch.stats()
     batch.close()
     for s in sims:
@@ -670,6 +710,9 @@ def run_batch(args, rank, world, local_rank):
                                       "how": "fdtd_run per simulation, plain kernel, every step launched "
                                              "from the host (no CUDA graph); device time incl. launch gaps"},
         "batched_over_sequential_plain_launches": round(ms_p / ms_b, 3),
+        "sequential_reference_cuda": ref_seq,
+        "batched_over_sequential_reference_cuda": (round(ref_seq["ms_per_batch"] / ms_b, 3)
+                                                   if ref_seq and "ms_per_batch" in ref_seq else None),
         "mcell_updates_per_s": round(world * cells * nt / (ms_b * 1e-3) / 1e6, 1),
         "bit_identical_to_sequential": same,
         "gpu_launches": int(st["step_launches"] + st["dft_launches"]) * args.steps,

@@ -281,7 +281,7 @@ struct StreamVariant {
 template <int TY>
 StreamVariant stream_variant() {
   using G = StreamGeom<TY>;
-  return StreamVariant{TY, G::THREADS, G::MIN_BLOCKS, uint32_t(2 * G::XCH), G::MAIN, G::SPLIT,
+  return StreamVariant{TY, G::THREADS, G::MIN_BLOCKS, uint32_t(2 * G::XCH), G::MAIN, G::REGION,
                        &fdtd_step_stream_kernel<TY>};
 }
 
@@ -300,20 +300,25 @@ const StreamVariant* find_stream_variant(int ty, int stages) {
 }
 
 // Dynamic shared bytes of a streaming block with (at most) `want` plane
-// slots and, when a simulation has split cells, two or three split slots,
-// sized for the kernel's resident blocks per SM; the slot counts it fits go to
-// n_main / n_split.
-uint32_t stream_slots(const StreamVariant& v, int want, bool splits, int* n_main, int* n_split) {
+// slots and, when a simulation has split cells, four to six split regions,
+// sized for the kernel's resident blocks per SM (or fewer blocks, when three
+// plane slots and four regions do not fit beside that many); the slot and
+// region counts it fits go to n_main / n_reg.
+uint32_t stream_slots(const StreamVariant& v, int want, bool splits, int* n_main, int* n_reg) {
   constexpr uint32_t kSmemPerSm = 233472, kPerBlockReserve = 1024 + 512, kMaxPerBlock = 232448 - 512;
-  const uint32_t budget = std::min(kSmemPerSm / v.min_blocks - kPerBlockReserve, kMaxPerBlock) - v.xch_bytes;
-  const uint32_t split_min = splits ? 2 * v.split_bytes : 0;
+  const uint32_t split_min = splits ? kRegionsMin * v.split_bytes : 0;
+  uint32_t budget = 0;
+  for (int blocks = v.min_blocks; blocks >= 1; --blocks) {
+    budget = std::min(kSmemPerSm / blocks - kPerBlockReserve, kMaxPerBlock) - v.xch_bytes;
+    if (budget >= 3 * v.main_bytes + split_min) break;
+  }
   if (budget < 3 * v.main_bytes + split_min)
     throw ArgError{FDTD_ERR_LIMIT, "Streaming kernel's plane slots do not fit in shared memory."};
   const uint32_t m = std::min<uint32_t>(uint32_t(std::min(want, kSlotsMax)), (budget - split_min) / v.main_bytes);
-  const uint32_t sp = splits ? std::min<uint32_t>(3, (budget - m * v.main_bytes) / v.split_bytes) : 0;
+  const uint32_t rg = splits ? std::min<uint32_t>(kRegionsMax, (budget - m * v.main_bytes) / v.split_bytes) : 0;
   *n_main = int(std::max<uint32_t>(m, 3));
-  *n_split = int(sp);
-  return v.xch_bytes + uint32_t(*n_main) * v.main_bytes + sp * v.split_bytes;
+  *n_reg = int(rg);
+  return v.xch_bytes + uint32_t(*n_main) * v.main_bytes + rg * v.split_bytes;
 }
 
 // Whether a (variant, tile height, stages) triple names an instantiated kernel.
@@ -390,7 +395,7 @@ void encode_stream_maps(StreamMaps& m, const fdtd_sim* s, int ty) {
 struct StreamClass {
   const StreamVariant* v = nullptr;
   uint32_t ring = 0;                 // dynamic shared bytes: exchange buffers, plane slots, split slots
-  int n_main = 0, n_split = 0;
+  int n_main = 0, n_reg = 0;
   std::vector<StreamTile> host_tiles;
   std::vector<StreamMaps> host_maps;
   DevBuf<StreamMaps> d_maps;
@@ -593,7 +598,7 @@ struct Engine {
       threads = c.v->threads;
       bool splits = false;
       for (auto* s : sims) splits = splits || s->splits.n > 0;
-      c.ring = stream_slots(*c.v, cfg.stages, splits, &c.n_main, &c.n_split);
+      c.ring = stream_slots(*c.v, cfg.stages, splits, &c.n_main, &c.n_reg);
       smem = int(c.ring);
       ty = c.v->ty;
     }
@@ -707,7 +712,7 @@ struct Engine {
       StreamClass& c = scls;
       const unsigned base = unsigned(n) * unsigned(c.n_tiles + c.grid);
       c.v->fn<<<c.grid, c.v->threads, c.ring, st>>>(c.d_sims.p, c.d_tiles.p, c.n_tiles, n, c.d_counter.p, base,
-                                                       d_err.p, c.n_main, c.n_split, wait_limit, withhold);
+                                                       d_err.p, c.n_main, c.n_reg, wait_limit, withhold);
       CK(cudaGetLastError());
     } else {
       fdtd_step_kernel<kTileY><<<n_tiles, dim3(32, kBlockY), 0, st>>>(d_sims.p, d_tiles.p, n);
@@ -1125,6 +1130,9 @@ void prepare(fdtd_sim* s, int nt) {
     s->fields.alloc(12 * N);
     // split pairs only in the slab stores and the sparse store
     s->split_buf_pairs = split_layout(s->split_plan, nx, ny, nz, s->pitch, s->split_geo);
+    for (int st = 0; st < 6; ++st)  // the kernels step between a store's components with 32-bit strides
+      if (6 * s->split_geo.comp[st] >= (int64_t(1) << 31))
+        throw ArgError{FDTD_ERR_LIMIT, "PML slab too large for 32-bit split-pair offsets."};
     const bool any_split = s->grid.e_split_cells > 0 || s->grid.h_split_cells > 0;
     s->splits.alloc(any_split ? 2 * 2 * s->split_buf_pairs : 0);
     // material index: upload in reference order, transpose on the device

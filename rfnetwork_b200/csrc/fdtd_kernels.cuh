@@ -78,12 +78,12 @@ __host__ __device__ __forceinline__ int split_store(const SplitDev& S, int nx, i
 // the cell's row word 31, used by the sparse store); component m lies m *
 // stride pairs further.
 __device__ __forceinline__ float2* split_ptr(const SplitDev& S, int b, int st, int x, int y, int z, int slot,
-                                             int64_t& stride) {
+                                             int& stride) {
   if (st == kStSparse) {
     stride = 1;
     return S.base[b] + S.off[kStSparse] + int64_t(slot) * 6;
   }
-  stride = S.comp[st];
+  stride = int(S.comp[st]);
   return S.base[b] + S.off[st] + (int64_t(z - S.oz[st]) * S.h[st] + (y - S.oy[st])) * S.w[st] + (x - S.ox[st]);
 }
 
@@ -206,7 +206,7 @@ fdtd_step_kernel(const SimDev* __restrict__ sims, const int4* __restrict__ tiles
       } else {
         // per component: split pair (ex_y, ex_z), ... or unsplit total
         const int st = split_store(S.sp, nx, ny, nz, c, r, z);
-        int64_t cs;
+        int cs;
         const float2* Es = split_ptr(S.sp, cur, st, c, r, z, __float_as_int(rw7.w), cs);
         float2 p0 = make_float2(0.f, 0.f), p1 = p0, p2 = p0;
         if (flags & (kCompSplit0 << 0)) {
@@ -297,8 +297,9 @@ fdtd_step_kernel(const SimDev* __restrict__ sims, const int4* __restrict__ tiles
         hz = upd_h(da_zx, hz_c, gzx, gzy);
       } else {
         const int st = split_store(S.sp, nx, ny, nz, c, r, z);
-        int64_t cs;
-        const float2* Hs = split_ptr(S.sp, cur, st, c, r, z, __float_as_int(rw7.w), cs) + 3 * cs;
+        int cs;
+        const float2* Hs = split_ptr(S.sp, cur, st, c, r, z, __float_as_int(rw7.w), cs);
+        Hs += 3 * cs;
         float2 p0 = make_float2(0.f, 0.f), p1 = p0, p2 = p0;
         if (flags & (kCompSplit0 << 3)) {
           p0 = __ldg(Hs);
@@ -334,7 +335,8 @@ fdtd_step_kernel(const SimDev* __restrict__ sims, const int4* __restrict__ tiles
             }
           }
         }
-        float2* Ho = split_ptr(S.sp, nxt, st, c, r, z, __float_as_int(rw7.w), cs) + 3 * cs;
+        float2* Ho = split_ptr(S.sp, nxt, st, c, r, z, __float_as_int(rw7.w), cs);
+        Ho += 3 * cs;
         if (flags & (kCompSplit0 << 3)) {
           hx = __fadd_rn(p0.x, p0.y);
           Ho[0] = p0;
@@ -473,9 +475,10 @@ __global__ void monitor_kernel(const SimDev* __restrict__ sim, const MonDev* __r
       float v;
       if (M.field < 3) {
         if (flags & (kCompSplit0 << M.field)) {
-          int64_t cs;
-          const float2 p = split_ptr(S.sp, buf, split_store(S.sp, S.nx, S.ny, S.nz, x, y, z), x, y, z,
-                                     __float_as_int(r7.w), cs)[M.field * cs];
+          int cs;
+          const float2* pp = split_ptr(S.sp, buf, split_store(S.sp, S.nx, S.ny, S.nz, x, y, z), x, y, z,
+                                       __float_as_int(r7.w), cs);
+          const float2 p = pp[M.field * cs];
           v = p.x + p.y;
         } else {
           v = S.E[buf][M.field][idx];

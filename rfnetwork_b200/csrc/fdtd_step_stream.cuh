@@ -87,8 +87,7 @@ struct StreamGeom {
   static constexpr int OFF_I = OFF_E + A(EB);
   static constexpr uint32_t MAIN = OFF_I + A(IB);  // plane slot: H, E, index
   static constexpr uint32_t SPLIT_HS = A(SEB);     // H pairs inside a split region
-  static constexpr uint32_t REGION = A(SEB) + A(SHB); // one store's E pairs, then H pairs
-  static constexpr uint32_t SPLIT = 2 * REGION;    // split slot: regions A and B
+  static constexpr uint32_t REGION = A(SEB) + A(SHB); // split region: one store's E pairs, then H pairs
   static constexpr uint32_t MAIN_BYTES = HB + EB + IB;
   static constexpr uint32_t SPLIT_BYTES = SEB + SHB;
   static constexpr int NCW = TY + 1;               // consumer warps
@@ -99,9 +98,13 @@ struct StreamGeom {
   static constexpr int MIN_BLOCKS = TY <= 4 ? 4 : TY <= 6 ? 3 : 2;
 };
 
-// Plane slots and split slots of the streaming and marching kernels (at most).
+// Plane slots and split regions of the streaming kernel (at most). A plane
+// with split cells takes one region per slab store it stages (one or two),
+// so four regions let the plane being computed and its look-ahead hold two
+// each.
 constexpr int kSlotsMax = 8;
-constexpr int kSplitSlotsMax = 4;
+constexpr int kRegionsMax = 6;
+constexpr int kRegionsMin = 4;
 
 // A plane's place in the ring of P plane slots: slot index and the parity of
 // the slot's current use, advanced without a division.
@@ -149,18 +152,18 @@ template <int TY>
 __global__ void __launch_bounds__(StreamGeom<TY>::THREADS, StreamGeom<TY>::MIN_BLOCKS)
 fdtd_step_stream_kernel(const SimDev* __restrict__ sims, const StreamTile* __restrict__ tiles, int n_tiles, int n,
                         unsigned* __restrict__ counter, unsigned base, int* __restrict__ err, int n_main,
-                        int n_split, uint32_t wait_limit, int withhold) {
+                        int n_reg, uint32_t wait_limit, int withhold) {
   using G = StreamGeom<TY>;
   // dynamic shared memory: the E exchange buffers, n_main plane slots (H, E,
-  // index), n_split split slots (E and H pairs). A warp holds two plane slots
-  // (the plane and its look-ahead) and one split slot at a time; a plane's
-  // split slot is free again once that plane is released.
+  // index), n_reg split regions (E and H pairs of one slab store). A warp
+  // holds two plane slots (the plane and its look-ahead) and their regions at
+  // a time; a plane's regions are free again once that plane is released.
   extern __shared__ __align__(128) unsigned char smem[];
   float* xch = reinterpret_cast<float*>(smem);  // [2][ex, ez][ER][32]
   unsigned char* ring = smem + 2 * G::XCH;
   __shared__ __align__(8) uint64_t full[kSlotsMax], empty[kSlotsMax];
-  __shared__ uint32_t s_soff[kSlotsMax];       // byte offset of each plane's split slot
-  __shared__ uint32_t s_suser[kSplitSlotsMax]; // last plane that used each split slot (producer only)
+  __shared__ int4 s_soff[kSlotsMax];           // each plane's regions: byte offsets of A and B, their stores (or -1)
+  __shared__ uint32_t s_ruser[kRegionsMax];    // last plane that used each region (producer only)
   __shared__ int s_tq[4];
   const int tid = threadIdx.x;
   const int cur = n & 1, nxt = cur ^ 1;
@@ -181,7 +184,7 @@ fdtd_step_stream_kernel(const SimDev* __restrict__ sims, const StreamTile* __res
     if (tid != NC) return;
     uint32_t q = 0;    // planes issued
     uint32_t rel = 0;  // planes below rel are known to be released by every consumer warp
-    uint32_t ns = 0;   // split slots taken
+    uint32_t nr = 0;   // regions taken
     SlotPos qp{0u, 0u}, rp{0u, 0u};  // ring positions of planes q and rel
     int k = 0;
     const StreamMaps* cur_maps = nullptr;
@@ -225,7 +228,7 @@ fdtd_step_stream_kernel(const SimDev* __restrict__ sims, const StreamTile* __res
       const int xs = (td.x0 - 1) & ~3, xi = (td.x0 - 1) & ~7;
       for (int j = 0; j < nload; ++j) {
         const bool last = t >= 0 && j == nload - 1;
-        const bool split = t >= 0 && !last && n_split > 0 && ((mask >> j) & 1u);
+        const bool split = t >= 0 && !last && n_reg > 0 && ((mask >> j) & 1u);
         // slab stores staged for this plane: regions A and B of its split slot
         int sa = -1, sbs = -1;
         const int zp = td.z0 - 1 + j;
@@ -243,18 +246,21 @@ fdtd_step_stream_kernel(const SimDev* __restrict__ sims, const StreamTile* __res
           break;
         }
         const int slot = int(qp.slot);
-        uint32_t soff = 0;
-        if (split) {
-          const uint32_t ss = ns % uint32_t(n_split);
-          if (ns >= uint32_t(n_split) && !release_upto(s_suser[ss])) {
+        // a region for each staged store; a region's last plane must be released
+        uint32_t soff[2] = {0u, 0u};
+        for (int rgn = 0; rgn < 2; ++rgn) {
+          if ((rgn == 0 ? sa : sbs) < 0) continue;
+          const uint32_t rs = nr % uint32_t(n_reg);
+          if (nr >= uint32_t(n_reg) && !release_upto(s_ruser[rs])) {
             failed = true;
             break;
           }
-          s_suser[ss] = q;
-          ++ns;
-          soff = uint32_t(P) * G::MAIN + ss * G::SPLIT;
+          s_ruser[rs] = q;
+          ++nr;
+          soff[rgn] = uint32_t(P) * G::MAIN + rs * G::REGION;
         }
-        s_soff[slot] = soff;
+        if (failed) break;
+        s_soff[slot] = make_int4(int(soff[0]), int(soff[1]), sa, sbs);
         if (j == 0) s_tq[k & 3] = t;
         if (t < 0) {  // end of the stream: complete the phase without data
           mbar_arrive(&full[slot]);
@@ -268,7 +274,6 @@ fdtd_step_stream_kernel(const SimDev* __restrict__ sims, const StreamTile* __res
           continue;
         }
         unsigned char* b = ring + uint32_t(slot) * G::MAIN;
-        unsigned char* sb = ring + soff;
         uint64_t* fb = &full[slot];
         fence_proxy_async();
         mbar_arrive_expect_tx(fb, last ? uint32_t(G::HB)
@@ -283,7 +288,7 @@ fdtd_step_stream_kernel(const SimDev* __restrict__ sims, const StreamTile* __res
           for (int rgn = 0; rgn < 2; ++rgn) {
             const int st = rgn == 0 ? sa : sbs;
             if (st < 0) continue;
-            unsigned char* d = sb + rgn * G::REGION;
+            unsigned char* d = ring + soff[rgn];
             const int sx = 2 * (xs - sp->ox[st]), sz = zp - sp->oz[st];
             tma_load_5d(d, &maps->Es[st], sx, td.y0 - 1 - sp->oy[st], sz, 0, cur, fb);
             // H pairs: components 3..5 of the store
@@ -306,9 +311,6 @@ fdtd_step_stream_kernel(const SimDev* __restrict__ sims, const StreamTile* __res
 
   // ================================================================== consumers
   const int lane = tid & 31, w = tid >> 5;
-  const float4* __restrict__ rows = nullptr;
-  int row_id = -1;
-  float4 ra = {}, rb = {}, rd = {}, rp = {}, rq = {}, ru = {}, rv = {}, r7 = {};
   SlotPos cp{0u, 0u};  // ring position of the plane being computed
   for (int k = 0;; ++k) {
     bool ok = mbar_wait_bounded(&full[cp.slot], cp.par, wait_limit);
@@ -320,23 +322,17 @@ fdtd_step_stream_kernel(const SimDev* __restrict__ sims, const StreamTile* __res
     if (ti < 0) break;
     const StreamTile td = load_stream_tile(tiles, ti);
     const SimDev& Sd = sims[td.sim];
-    if (Sd.rows != rows) {
-      rows = Sd.rows;
-      row_id = -1;
-    }
     const int x0 = td.x0, y0 = td.y0, z0 = td.z0;
     const int c = x0 - 1 + lane, r = y0 - 1 + w;
     const int oh = (x0 - 1) - ((x0 - 1) & ~3), oi = (x0 - 1) - ((x0 - 1) & ~7);
     const bool own_xy = lane >= 1 && w >= 1 && c < Sd.nx && r < Sd.ny;
     const int plane = Sd.plane;
-    const int64_t N = Sd.cells;
     float* __restrict__ const fo = Sd.E[nxt][0];   // E then H components of step n+1, N apart
     const int npl = td.z1 - z0 + 1;                // planes z0-1 .. z1-1 computed
     const int hb = w * G::HW + oh + lane;
     const int eb = w * G::EW + oh + lane;
     const int ib = w * G::IW + oi + lane;
     const int sb = (w - 1) * G::EW + oh + lane;    // H split box (owned rows)
-    const uint64_t smask = uint64_t(td.split_lo) | (uint64_t(td.split_hi) << 32);
     int idx = (z0 - 1) * plane + r * Sd.pitch + c; // cell offset of plane z (owned cells, z >= z0)
 
     // The plane loop, instantiated for plain tiles (FAST: every cell unsplit,
@@ -344,6 +340,11 @@ fdtd_step_stream_kernel(const SimDev* __restrict__ sims, const StreamTile* __res
     auto planes = [&](auto fast_tag) -> bool {
       constexpr bool FAST = decltype(fast_tag)::value;
       float ex_p = 0.f, ey_p = 0.f;  // E^{n+1} of this cell one plane below
+      // this cell's table row, reloaded when its material index changes along
+      // z (declared per path: the interior path keeps only the words it reads)
+      const float4* __restrict__ const rows = Sd.rows;
+      int row_id = -1;
+      float4 ra = {}, rb = {}, rd = {}, rp = {}, rq = {}, ru = {}, rv = {}, r7 = {};
       for (int i = 0; i < npl; ++i) {
         const SlotPos np = cp.next(P);
         // plane z was waited for as the look-ahead of the previous iteration
@@ -352,30 +353,26 @@ fdtd_step_stream_kernel(const SimDev* __restrict__ sims, const StreamTile* __res
         const float* sH = reinterpret_cast<const float*>(st);
         const float* sE = reinterpret_cast<const float*>(st + G::OFF_E);
         const uint16_t* sI = reinterpret_cast<const uint16_t*>(st + G::OFF_I);
-        const unsigned char* ss = ring + s_soff[cp.slot];
         const float* nH = reinterpret_cast<const float*>(ring + np.slot * G::MAIN);
         float* xb = xch + (i & 1) * (G::XCH / 4);
         constexpr int HC = G::HC, EC = G::EC;
         const bool store = own_xy && i > 0;
         const int z = z0 - 1 + i;
-        // split pairs of this plane: the slab stores staged in regions A and B
-        // of its split slot (as the producer chose them), other stores and
-        // sparse cells from global memory
-        int sa = -1, sbs = -1;
-        if (!FAST && n_split > 0 && ((smask >> i) & 1u)) {
-          if (z < Sd.sp.t[4]) sa = kStZlo;
-          else if (z >= Sd.nz - Sd.sp.t[5]) sa = kStZhi;
-          else {
-            sa = td.ys;
-            sbs = td.xs;
-          }
-        }
-        // the E (h = 0) or H (h = 3) pair of component m of this cell, from
-        // the staged region or the store; `cst` is the cell's store
-        auto pair_in = [&](int cst, int rgn, int m, const float2* gp, int64_t cs) -> float2 {
+        // split pairs of this plane: the slab stores the producer staged in
+        // regions A and B (region 0 / 1 of a cell whose store is one of them),
+        // other stores and sparse cells from global memory (region -1)
+        auto region_of = [&](int cst) -> int {
+          const int4 si = s_soff[cp.slot];
+          return cst == si.z ? 0 : cst == si.w ? 1 : -1;
+        };
+        // the E (m < 3) or H pair of component m of this cell, from its
+        // staged region or the store
+        auto pair_in = [&](int rgn, int m, const float2* gp, int cs) -> float2 {
           if (rgn < 0) return __ldg(gp + m * cs);
-          const float2* r2 = reinterpret_cast<const float2*>(ss + rgn * G::REGION);
-          return m < 3 ? r2[m * EC + eb] : reinterpret_cast<const float2*>(ss + rgn * G::REGION + G::SPLIT_HS)[(m - 3) * G::SHC + sb];
+          const int4 si = s_soff[cp.slot];
+          const unsigned char* rg = ring + (rgn == 0 ? si.x : si.y);
+          return m < 3 ? reinterpret_cast<const float2*>(rg)[m * EC + eb]
+                       : reinterpret_cast<const float2*>(rg + G::SPLIT_HS)[(m - 3) * G::SHC + sb];
         };
 
         // ------------------------------------------------------------ E phase
@@ -408,27 +405,27 @@ fdtd_step_stream_kernel(const SimDev* __restrict__ sims, const StreamTile* __res
           // per component: the split pair (one 8-byte load) or the unsplit total
           float2 sp[3];
           const int cst = split_store(Sd.sp, Sd.nx, Sd.ny, Sd.nz, c, r, z);
-          const int rgn = cst == sa ? 0 : cst == sbs ? 1 : -1;
-          int64_t cs = 0;
+          const int rgn = region_of(cst);
+          int cs = 0;
           const float2* gp = rgn < 0 ? split_ptr(Sd.sp, cur, cst, c, r, z, __float_as_int(r7.w), cs) : nullptr;
   #pragma unroll
           for (int m = 0; m < 3; ++m) sp[m] = make_float2(0.f, 0.f);
           if (flags & (kCompSplit0 << 0)) {
-            sp[0] = pair_in(cst, rgn, 0, gp, cs);
+            sp[0] = pair_in(rgn, 0, gp, cs);
             sp[0].x = upd_e_split(ra.x, sp[0].x, ra.y, dhz_y);  // ex_y
             sp[0].y = upd_e_split(ra.z, sp[0].y, ra.w, dhy_z);  // ex_z
           } else {
             ex = upd_e(ra.x, sE[eb], ra.y, dhz_y, ra.w, dhy_z);
           }
           if (flags & (kCompSplit0 << 1)) {
-            sp[1] = pair_in(cst, rgn, 1, gp, cs);
+            sp[1] = pair_in(rgn, 1, gp, cs);
             sp[1].x = upd_e_split(rb.x, sp[1].x, rb.y, dhx_z);  // ey_z
             sp[1].y = upd_e_split(rb.z, sp[1].y, rb.w, dhz_x);  // ey_x
           } else {
             ey = upd_e(rb.x, sE[EC + eb], rb.y, dhx_z, rb.w, dhz_x);
           }
           if (flags & (kCompSplit0 << 2)) {
-            sp[2] = pair_in(cst, rgn, 2, gp, cs);
+            sp[2] = pair_in(rgn, 2, gp, cs);
             sp[2].x = upd_e_split(rd.x, sp[2].x, rd.y, dhy_x);  // ez_x
             sp[2].y = upd_e_split(rd.z, sp[2].y, rd.w, dhx_y);  // ez_y
           } else {
@@ -461,6 +458,7 @@ fdtd_step_stream_kernel(const SimDev* __restrict__ sims, const StreamTile* __res
           const float ez_ym = xb[G::ER * 32 + (w - 1) * 32 + lane];
           // totals of the components not stored split
           if (FAST || !(flags & (kCompSplit0 << 0))) fo[idx] = ex;
+          const int64_t N = Sd.cells;  // floats per component, read where used: no register across the plane loop
           if (FAST || !(flags & (kCompSplit0 << 1))) fo[N + idx] = ey;
           if (FAST || !(flags & (kCompSplit0 << 2))) fo[2 * N + idx] = ez;
           // slots 12..29: (Da, Db1, Db2) of hx_y, hx_z, hy_z, hy_x, hz_x, hz_y
@@ -478,27 +476,27 @@ fdtd_step_stream_kernel(const SimDev* __restrict__ sims, const StreamTile* __res
           } else {
             float2 sp[3];
             const int cst = split_store(Sd.sp, Sd.nx, Sd.ny, Sd.nz, c, r, z);
-            const int rgn = cst == sa ? 0 : cst == sbs ? 1 : -1;
-            int64_t cs = 0;
+            const int rgn = region_of(cst);
+            int cs = 0;
             const float2* gp = rgn < 0 ? split_ptr(Sd.sp, cur, cst, c, r, z, __float_as_int(r7.w), cs) : nullptr;
   #pragma unroll
             for (int m = 0; m < 3; ++m) sp[m] = make_float2(0.f, 0.f);
             if (flags & (kCompSplit0 << 3)) {
-              sp[0] = pair_in(cst, rgn, 3, gp, cs);
+              sp[0] = pair_in(rgn, 3, gp, cs);
               sp[0].x = upd_h_split(rp.x, sp[0].x, gxy);
               sp[0].y = upd_h_split(rp.w, sp[0].y, gxz);
             } else {
               hx = upd_h(rp.x, hx_c, gxy, gxz);
             }
             if (flags & (kCompSplit0 << 4)) {
-              sp[1] = pair_in(cst, rgn, 4, gp, cs);
+              sp[1] = pair_in(rgn, 4, gp, cs);
               sp[1].x = upd_h_split(rq.z, sp[1].x, gyz);
               sp[1].y = upd_h_split(ru.y, sp[1].y, gyx);
             } else {
               hy = upd_h(rq.z, hy_c, gyz, gyx);
             }
             if (flags & (kCompSplit0 << 5)) {
-              sp[2] = pair_in(cst, rgn, 5, gp, cs);
+              sp[2] = pair_in(rgn, 5, gp, cs);
               sp[2].x = upd_h_split(rv.x, sp[2].x, gzx);
               sp[2].y = upd_h_split(rv.w, sp[2].y, gzy);
             } else {

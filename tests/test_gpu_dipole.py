@@ -10,7 +10,13 @@ cross polarization below -40 dB, the poles below -90 dB, S11 below -10 dB and
 the input resistance within 3.5 ohm of 73 ohm. The same model here runs the
 time loop on the engine and the near-to-far-field transform on the GPU
 (fdtd_nf2ff); the mesher is replaced by explicit graded edges with the same
-feature lines and cell-size limits, built below.
+feature lines and cell-size limits, built below. Their cells grow by at most
+1.25 from one to the next, in the spirit of the reference mesher's blending,
+which spreads the change of width to keep the growth rate low (its
+utils_mesh.blend_cell_widths). With a growth of 1.5 the 20 GHz cross
+polarization of this model reaches -39.5 dB; with 1.2 its cells take 66,305
+distinct coefficient rows, more than the engine's 16-bit material index
+addresses (the engine reports that as a size-limit error).
 """
 import numpy as np
 import pytest
@@ -23,7 +29,7 @@ pytestmark = pytest.mark.gpu
 D_MIN, D_MAX = 0.01, 0.03
 
 
-def _fill(length, d_first, d_last, growth=1.5):
+def _fill(length, d_first, d_last, growth=1.25):
     """Cell widths over `length`, growing from d_first (and, if given, back to
     d_last at the far end) by `growth`, capped at D_MAX, scaled to fit."""
     def sizes(n):
