@@ -509,6 +509,7 @@ def workloads_entry(args, local_rank):
             ("microstrip_graded", run_microstrip, dict(graded=True), common),
             ("batch", run_batch, {}, ("value", "unit", "ms_per_step", "sequential", "batched_over_sequential",
                                       "sequential_plain_launches", "batched_over_sequential_plain_launches",
+                                      "sequential_reference_cuda", "batched_over_sequential_reference_cuda",
                                       "mcell_updates_per_s", "bit_identical_to_sequential", "gpu_launches")),
             ("adjoint", run_adjoint, {}, ("value", "unit", "ms_per_step", "forward_s", "gradient_over_forward",
                                           "device", "recorded_history", "gpu_launches")),

@@ -174,26 +174,30 @@ adj_step_kernel(const AdjSim* __restrict__ sims, const int4* __restrict__ tiles,
     float h_n2[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f}, e_n[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
     load_h(z + 2, fl_n2, h_n2);
     load_e(z + 1, fl_n1, e_n);
-    // ---- table rows of this plane and of the look-ahead
-    const float4* rn = rows + 8 * id_n1;
-    const float4 p_n = __ldg(rn + 3), q_n = __ldg(rn + 4), r7_n = __ldg(rn + 7);
+    // ---- table rows of this plane and of the look-ahead (the Db1 words of
+    // hx_y, hx_z, hy_z and hz_y: this plane's own where the index is the same)
     const float4* row = rows + 8 * id_c;
     const float4 ra = __ldg(row + 0), rb = __ldg(row + 1), rd = __ldg(row + 2);
     const float4 p = __ldg(row + 3), q = __ldg(row + 4), u = __ldg(row + 5), v = __ldg(row + 6), r7 = __ldg(row + 7);
+    float pn_y = p.y, qn_x = q.x, qn_w = q.w, r7n_x = r7.x;
+    if (id_n1 != id_c) {
+      const float4* rn = rows + 8 * id_n1;
+      pn_y = __ldg(&rn[3].y); qn_x = __ldg(&rn[4].x); qn_w = __ldg(&rn[4].w); r7n_x = __ldg(&rn[7].x);
+    }
     float lE[6];
 #pragma unroll
     for (int k = 0; k < 6; ++k) lE[k] = e_c[k];
 
     // ---- Db1 lamH of the +1 neighbours: z+1 from the look-ahead, x+1 from
     // the lane on the right, y+1 from the row above (written last plane)
-    const float qz_hx = q_n.x * h_n[1], qz_hy = q_n.w * h_n[2];
+    const float qz_hx = qn_x * h_n[1], qz_hy = qn_w * h_n[2];
     const float qx_hy = __shfl_down_sync(0xffffffffu, u.z * h_c[3], 1);
     const float qx_hz = __shfl_down_sync(0xffffffffu, v.y * h_c[4], 1);
     const float qy_hx = s_qhx[buf][w + (w <= TY ? 1 : 0)][lane];
     const float qy_hz = s_qhz[buf][w + (w <= TY ? 1 : 0)][lane];
     // and this column's own values at z+1 for the row below, next plane
-    s_qhx[buf ^ 1][w][lane] = p_n.y * h_n[0];
-    s_qhz[buf ^ 1][w][lane] = r7_n.x * h_n[5];
+    s_qhx[buf ^ 1][w][lane] = pn_y * h_n[0];
+    s_qhz[buf ^ 1][w][lane] = r7n_x * h_n[5];
 
     // ---- E part: mu, lamE', ad
     float mu[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f}, ad[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};

@@ -1066,9 +1066,9 @@ struct Engine {
 namespace {
 
 // Geometry of the split stores of a plan (SplitDev without base pointers);
-// returns the pairs one time buffer holds. Slab stores span whole x rows
-// (pitch) except the x faces, whose rows hold at least 16 pairs from an even
-// origin so their TMA boxes start on 16 bytes.
+// returns the pairs one time buffer holds. z and y stores span whole x rows
+// (pitch); x stores span the core y rows and an even number of pairs from an
+// even origin, so their rows and TMA boxes start on 16 bytes.
 size_t split_layout(const SplitPlan& plan, int nx, int ny, int nz, int pitch, SplitDev& g) {
   g = SplitDev{};
   const int* t = plan.t;
@@ -1082,11 +1082,12 @@ size_t split_layout(const SplitPlan& plan, int nx, int ny, int nz, int pitch, Sp
   set(kStZhi, 0, 0, nz - t[5], pitch, ny, t[5]);
   set(kStYlo, 0, 0, zc0, pitch, t[2], zc);
   set(kStYhi, 0, ny - t[3], zc0, pitch, t[3], zc);
-  const int wxl = t[0] ? std::max(16, (t[0] + 1) & ~1) : 0;
+  const int yc = std::max(0, ny - t[2] - t[3]);
+  const int wxl = t[0] ? (t[0] + 1) & ~1 : 0;
   const int oxh = (nx - t[1]) & ~1;
-  const int wxh = t[1] ? std::max(16, (nx - oxh + 1) & ~1) : 0;
-  set(kStXlo, 0, 0, zc0, wxl, ny, zc);
-  set(kStXhi, oxh, 0, zc0, wxh, ny, zc);
+  const int wxh = t[1] ? (nx - oxh + 1) & ~1 : 0;
+  set(kStXlo, 0, t[2], zc0, wxl, yc, zc);
+  set(kStXhi, oxh, t[2], zc0, wxh, yc, zc);
   int64_t off = 0;
   for (int st = 0; st < 6; ++st) {
     g.off[st] = off;

@@ -76,15 +76,20 @@ __host__ __device__ __forceinline__ int split_store(const SplitDev& S, int nx, i
 
 // Pair of component 0 of cell (x, y, z) in store st of time buffer b (slot:
 // the cell's row word 31, used by the sparse store); component m lies m *
-// stride pairs further.
-__device__ __forceinline__ float2* split_ptr(const SplitDev& S, int b, int st, int x, int y, int z, int slot,
+// stride pairs further. split_off is its offset from the buffer's base.
+__device__ __forceinline__ int64_t split_off(const SplitDev& S, int st, int x, int y, int z, int slot,
                                              int& stride) {
   if (st == kStSparse) {
     stride = 1;
-    return S.base[b] + S.off[kStSparse] + int64_t(slot) * 6;
+    return S.off[kStSparse] + int64_t(slot) * 6;
   }
   stride = int(S.comp[st]);
-  return S.base[b] + S.off[st] + (int64_t(z - S.oz[st]) * S.h[st] + (y - S.oy[st])) * S.w[st] + (x - S.ox[st]);
+  return S.off[st] + (int64_t(z - S.oz[st]) * S.h[st] + (y - S.oy[st])) * S.w[st] + (x - S.ox[st]);
+}
+
+__device__ __forceinline__ float2* split_ptr(const SplitDev& S, int b, int st, int x, int y, int z, int slot,
+                                             int& stride) {
+  return S.base[b] + split_off(S, st, x, y, z, slot, stride);
 }
 
 struct SimDev {

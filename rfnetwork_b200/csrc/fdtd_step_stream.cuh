@@ -395,6 +395,15 @@ fdtd_step_stream_kernel(const SimDev* __restrict__ sims, const StreamTile* __res
           row_id = id;
         }
         const uint32_t flags = __float_as_uint(r7.z);
+        // a split cell's store, staged region (-1: none) and pair offset,
+        // found once per plane for both phases
+        int cst = kStSparse, rgn = -1, cs = 0;
+        int64_t so = 0;
+        if (!FAST && (flags & (kESplit | kHSplit))) {
+          cst = split_store(Sd.sp, Sd.nx, Sd.ny, Sd.nz, c, r, z);
+          rgn = region_of(cst);
+          so = split_off(Sd.sp, cst, c, r, z, __float_as_int(r7.w), cs);
+        }
         float ex, ey, ez;
         if (FAST || !(flags & kESplit)) {
           // both splits share Ca: f' = Ca f + Cb1 d1 + Cb2 d2
@@ -404,10 +413,7 @@ fdtd_step_stream_kernel(const SimDev* __restrict__ sims, const StreamTile* __res
         } else {
           // per component: the split pair (one 8-byte load) or the unsplit total
           float2 sp[3];
-          const int cst = split_store(Sd.sp, Sd.nx, Sd.ny, Sd.nz, c, r, z);
-          const int rgn = region_of(cst);
-          int cs = 0;
-          const float2* gp = rgn < 0 ? split_ptr(Sd.sp, cur, cst, c, r, z, __float_as_int(r7.w), cs) : nullptr;
+          const float2* gp = Sd.sp.base[cur] + so;
   #pragma unroll
           for (int m = 0; m < 3; ++m) sp[m] = make_float2(0.f, 0.f);
           if (flags & (kCompSplit0 << 0)) {
@@ -436,7 +442,7 @@ fdtd_step_stream_kernel(const SimDev* __restrict__ sims, const StreamTile* __res
           if (flags & (kCompSplit0 << 1)) ey = __fadd_rn(sp[1].x, sp[1].y);
           if (flags & (kCompSplit0 << 2)) ez = __fadd_rn(sp[2].x, sp[2].y);
           if (store) {
-            float2* po = split_ptr(Sd.sp, nxt, cst, c, r, z, __float_as_int(r7.w), cs);
+            float2* po = Sd.sp.base[nxt] + so;
   #pragma unroll
             for (int m = 0; m < 3; ++m)
               if (flags & (kCompSplit0 << m)) po[m * cs] = sp[m];
@@ -475,10 +481,7 @@ fdtd_step_stream_kernel(const SimDev* __restrict__ sims, const StreamTile* __res
             hz = upd_h(rv.x, hz_c, gzx, gzy);
           } else {
             float2 sp[3];
-            const int cst = split_store(Sd.sp, Sd.nx, Sd.ny, Sd.nz, c, r, z);
-            const int rgn = region_of(cst);
-            int cs = 0;
-            const float2* gp = rgn < 0 ? split_ptr(Sd.sp, cur, cst, c, r, z, __float_as_int(r7.w), cs) : nullptr;
+            const float2* gp = Sd.sp.base[cur] + so;
   #pragma unroll
             for (int m = 0; m < 3; ++m) sp[m] = make_float2(0.f, 0.f);
             if (flags & (kCompSplit0 << 3)) {
@@ -506,7 +509,7 @@ fdtd_step_stream_kernel(const SimDev* __restrict__ sims, const StreamTile* __res
             if (flags & (kCompSplit0 << 3)) hx = __fadd_rn(sp[0].x, sp[0].y);
             if (flags & (kCompSplit0 << 4)) hy = __fadd_rn(sp[1].x, sp[1].y);
             if (flags & (kCompSplit0 << 5)) hz = __fadd_rn(sp[2].x, sp[2].y);
-            float2* po = split_ptr(Sd.sp, nxt, cst, c, r, z, __float_as_int(r7.w), cs);
+            float2* po = Sd.sp.base[nxt] + so;
   #pragma unroll
             for (int m = 0; m < 3; ++m)
               if (flags & (kCompSplit0 << (3 + m))) po[(3 + m) * cs] = sp[m];

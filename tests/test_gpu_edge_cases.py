@@ -4,13 +4,16 @@ distinct row with split components, a soft source and probes on the grid's
 first and last cells, a run without probes, and a one-step run.
 
 Random coefficients give every cell its own table row and most cells split
-E and H components, so the streaming kernel's split paths, narrow windows,
-halo recomputation and zero-filled edges are all exercised; it must give
-the plain kernel's bits exactly (the plain kernel's parity with the oracle is
-tests/test_gpu_parity.py's)."""
+E and H components, so the streaming kernel's split paths (here one slab
+store covers the grid), halo recomputation and zero-filled edges are all
+exercised; it must give the plain kernel's bits exactly (the plain kernel's
+parity with the oracle is tests/test_gpu_parity.py's). PML models with slabs
+on all six faces and ragged x rows exercise the per-face stores, the two
+staged regions of corner tiles and the sparse store of the port cells."""
 import numpy as np
 import pytest
 
+from modelgen import configs
 from rfnetwork_b200 import _lib
 from rfnetwork_b200.solver_constants import COEFF_NAMES
 
@@ -90,3 +93,47 @@ def test_batch_of_tiny_grids_equals_single_runs(engine_lib, kernel):
     batch.close()
     for sim in sims:
         sim.close()
+
+
+def _boxes_sim(shape, nt, kernel):
+    m = configs.boxes(n=shape, n_pml=8, n_boxes=6, nt=nt, n_ports=2, n_probes=4)
+    co, pr, mo, mem, Nx, Ny, Nz, Nt = m.pack_inputs(gpu=True)
+    sim = _lib.Simulation(Nx, Ny, Nz)
+    sim.set_kernel(*kernel)
+    sim.set_coefficients(co)
+    for q in pr:
+        sim.add_probe(q["field"], q["idx"], q["is_source"], q["values"][:Nt] if q["is_source"] else None)
+    return sim, len(pr)
+
+
+@pytest.mark.parametrize("shape", [(64, 56, 40), (70, 45, 37)])
+def test_slab_stores_stream_equals_plain(engine_lib, shape):
+    """8-cell PML on all faces: the split pairs live in six slab stores (and a
+    sparse store for the port cells); every streaming shape gives the plain
+    kernel's bits, and the stores hold 96 bytes per slab cell and per sparse
+    slot, nothing for the core."""
+    nt = 60
+    sim, n_probes = _boxes_sim(shape, nt, (0, 0, 4, 0))
+    sim.run(nt)
+    ref = sim.probe_values()
+    st = sim.stats()
+    sim.close()
+    assert np.isfinite(ref).all() and np.abs(ref).max() > 0
+    assert st["split_slab"] == [8] * 6
+    nx, ny, nz = shape
+    pitch = (nx + 31) // 32 * 32
+    # z and y stores span the pitch; x stores an even number of pairs from an
+    # even origin over the core rows
+    oxh = (nx - 8) // 2 * 2
+    x_width = 8 + (nx - oxh + 1) // 2 * 2
+    slab_cells = 2 * 8 * ny * pitch + 2 * 8 * (nz - 16) * pitch + x_width * (ny - 16) * (nz - 16)
+    # sparse slots: one per probe-list entry (a probe cell's slot) and per other split cell
+    slots, rest = divmod(st["split_bytes"] - 96 * slab_cells, 96)
+    assert rest == 0
+    assert st["sparse_split_cells"] <= slots <= st["sparse_split_cells"] + n_probes
+    for kernel in ((1, 8, 6, 0), (1, 8, 4, 5), (1, 4, 6, 0), (1, 6, 3, 2), (1, 12, 3, 0)):
+        sim, _ = _boxes_sim(shape, nt, kernel)
+        sim.run(nt)
+        got = sim.probe_values()
+        sim.close()
+        assert np.array_equal(got, ref), kernel
