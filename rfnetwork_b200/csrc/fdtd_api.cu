@@ -433,6 +433,9 @@ struct Engine {
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   cudaStream_t cap_stream = nullptr;                   // box-history captures beside the steps
   cudaEvent_t cap_fork = nullptr, cap_join = nullptr;
+  cudaStream_t rep_stream = nullptr;                   // checkpointed adjoint: segment replays
+  cudaEvent_t seg_done[2] = {nullptr, nullptr};        // replay of a segment into history half k & 1 done
+  cudaEvent_t seg_free[2] = {nullptr, nullptr};        // its reversal done: the half may be refilled
   int64_t step_launches = 0, dft_launches = 0, adj_launches = 0;
   double adj_ms = 0;
   uint32_t wait_limit = kStreamWaitLimit;  // polls per mbarrier wait of the streaming kernel
@@ -450,6 +453,11 @@ struct Engine {
     if (!cap_stream) CK(cudaStreamCreateWithFlags(&cap_stream, cudaStreamNonBlocking));
     if (!cap_fork) CK(cudaEventCreateWithFlags(&cap_fork, cudaEventDisableTiming));
     if (!cap_join) CK(cudaEventCreateWithFlags(&cap_join, cudaEventDisableTiming));
+    if (!rep_stream) CK(cudaStreamCreateWithFlags(&rep_stream, cudaStreamNonBlocking));
+    for (int h = 0; h < 2; ++h) {
+      if (!seg_done[h]) CK(cudaEventCreateWithFlags(&seg_done[h], cudaEventDisableTiming));
+      if (!seg_free[h]) CK(cudaEventCreateWithFlags(&seg_free[h], cudaEventDisableTiming));
+    }
   }
   ~Engine() {
     if (graph) cudaGraphExecDestroy(graph);
@@ -458,6 +466,11 @@ struct Engine {
     if (cap_fork) cudaEventDestroy(cap_fork);
     if (cap_join) cudaEventDestroy(cap_join);
     if (cap_stream) cudaStreamDestroy(cap_stream);
+    for (int h = 0; h < 2; ++h) {
+      if (seg_done[h]) cudaEventDestroy(seg_done[h]);
+      if (seg_free[h]) cudaEventDestroy(seg_free[h]);
+    }
+    if (rep_stream) cudaStreamDestroy(rep_stream);
     if (own_stream) cudaStreamDestroy(own_stream);
   }
 
@@ -585,7 +598,8 @@ struct Engine {
   }
 
   // Streaming kernel: 31 x TY column tiles cut in z chunks of at most 62
-  // planes, each with the mask of its planes that hold split-field cells.
+  // planes (cut at the z slabs' inner faces), each with the mask of its
+  // planes that hold split-field cells.
   void build_stream_tiles(int n_sm) {
     StreamClass& c = scls;
     c.reset();
@@ -623,17 +637,36 @@ struct Engine {
       c.host_maps.emplace_back();
       encode_stream_maps(c.host_maps.back(), s, ty);
       const GradedIndex split_idx(s->grid, kFlagESplit | kFlagHSplit);
-      // tiles (x / 31, y / TY, z / zchunk) that own a probe cell
+      // z chunks of at most zc planes that do not straddle a z slab's inner
+      // face: the first core chunk starts one plane past the low slab (its
+      // halo plane is then a core plane), so interior columns of core chunks
+      // are plain tiles
+      std::vector<std::pair<int, int>> zr;
+      std::vector<int> chunk_of(size_t(s->nz), 0);
+      {
+        const int* pt = s->split_plan.t;
+        const int zlo = pt[4] > 0 ? std::min(s->nz, pt[4] + 1) : 0;
+        const int zhi = pt[5] > 0 ? std::max(zlo, s->nz - pt[5]) : s->nz;
+        auto cut = [&](int a, int b) {
+          for (int z = a; z < b; z += zc) zr.push_back({z, std::min(b, z + zc)});
+        };
+        cut(0, zlo);
+        cut(zlo, zhi);
+        cut(zhi, s->nz);
+        for (size_t k = 0; k < zr.size(); ++k)
+          for (int z = zr[k].first; z < zr[k].second; ++z) chunk_of[size_t(z)] = int(k);
+      }
+      // tiles (x / 31, y / TY, z chunk) that own a probe cell
       std::unordered_set<int64_t> probe_tiles;
       const int ntx = (s->nx + kStreamOwnX - 1) / kStreamOwnX, nty = (s->ny + ty - 1) / ty;
       for (const int64_t cell : s->grid.probe_cell) {
         const int z = int(cell % s->nz), y = int((cell / s->nz) % s->ny), x = int(cell / (int64_t(s->nz) * s->ny));
-        probe_tiles.insert((int64_t(z / zc) * nty + y / ty) * ntx + x / kStreamOwnX);
+        probe_tiles.insert((int64_t(chunk_of[size_t(z)]) * nty + y / ty) * ntx + x / kStreamOwnX);
       }
-      for (int z0 = 0; z0 < s->nz; z0 += zc)
+      for (size_t zk = 0; zk < zr.size(); ++zk)
         for (int y0 = 0; y0 < s->ny; y0 += ty)
           for (int x0 = 0; x0 < s->nx; x0 += kStreamOwnX) {
-            const int z1 = std::min(s->nz, z0 + zc);
+            const int z0 = zr[zk].first, z1 = zr[zk].second;
             // planes holding split cells in the E region (columns x0-1 .. x0+30, rows y0-1 .. y0+ty-1)
             uint64_t mask = 0;
             for (int j = 0; j < z1 - z0 + 1; ++j) {
@@ -659,8 +692,7 @@ struct Engine {
             t.z1 = z1;
             t.ys = ys;
             t.xs = xs;
-            t.plain = mask == 0 &&
-                      !probe_tiles.count((int64_t(z0 / zc) * nty + y0 / ty) * ntx + x0 / kStreamOwnX);
+            t.plain = mask == 0 && !probe_tiles.count((int64_t(zk) * nty + y0 / ty) * ntx + x0 / kStreamOwnX);
             t.split_lo = uint32_t(mask);
             t.split_hi = uint32_t(mask >> 32);
             c.host_tiles.push_back(t);
@@ -720,6 +752,23 @@ struct Engine {
     }
   }
 
+  // Step n of a checkpointed adjoint's segment replay (segment from step n0),
+  // with the streaming kernel on at most `per_sm` blocks per SM, so that the
+  // reversal of the next segment, running at the same time on another
+  // stream, finds room on every SM. The tile counter was cleared before n0.
+  void launch_replay_step(cudaStream_t st, int n, int n0, int n_sm, int per_sm) {
+    if (cfg.variant == 1) {
+      StreamClass& c = scls;
+      const int grid = std::min(c.grid, n_sm * per_sm);
+      const unsigned base = unsigned(n - n0) * unsigned(c.n_tiles + grid);
+      c.v->fn<<<grid, c.v->threads, c.ring, st>>>(c.d_sims.p, c.d_tiles.p, c.n_tiles, n, c.d_counter.p, base,
+                                                     d_err.p, c.n_main, c.n_reg, wait_limit, withhold);
+      CK(cudaGetLastError());
+    } else {
+      launch_step(st, n);
+    }
+  }
+
   // Box-history capture of the simulations in recorded mode (adj_mode 2):
   // one adj_capture_kernel launch per time step, before the step, inside the
   // captured time loop.
@@ -775,9 +824,10 @@ struct Engine {
   // J with respect to (Ca, Cb1, Cb2) of each E component on each box. The
   // adjoint state runs backwards from step nt-1 with one adj_step_kernel
   // launch per step over the tiles of all simulations. In recorded mode the
-  // box history of every step is already on the device; with checkpoints the
-  // run is replayed segment by segment, last segment first, capturing the
-  // segment's box history before its steps are reversed.
+  // box history of every step is already on the device. With checkpoints the
+  // run is replayed segment by segment, last segment first, capturing each
+  // segment's box history into one half of a two-segment buffer; the replay
+  // of segment k-1 (its own stream) runs while segment k is reversed.
   void adjoint(const std::vector<AdjRequest>& req) {
     init();
     cudaStream_t st = stream();
@@ -844,7 +894,7 @@ struct Engine {
       if (mode == 2) {
         a.hist = s->hist.p;
       } else {
-        B->seg.reserve(size_t(K) * 9 * size_t(nb));
+        B->seg.reserve(2 * size_t(K) * 9 * size_t(nb));
         a.hist = B->seg.p;
         CapSim c{};
         c.s = s->dev;
@@ -886,8 +936,13 @@ struct Engine {
       for (int n = nt - 1; n >= 0; --n) reverse_step(n, 0);
     } else {
       const int nseg = (nt + K - 1) / K;
-      for (int k = nseg - 1; k >= 0; --k) {
-        const int n0 = k * K, n1 = std::min(nt, n0 + K);
+      const char* rb = std::getenv("RFN_REPLAY_BLOCKS_PER_SM");
+      const int per_sm = rb ? std::max(1, std::atoi(rb)) : 1;
+      cudaStream_t rs = rep_stream;
+      // segment k replayed on rs from its snapshot into history half k & 1,
+      // each step's box capture beside it (as in a recorded run)
+      auto replay = [&](int k) {
+        const int n0 = k * K, n1 = std::min(nt, n0 + K), h0 = n0 - (k & 1) * K;
         const size_t b = size_t(n0 & 1);
         for (const auto& r : req) {
           fdtd_sim* s = r.s;
@@ -895,26 +950,35 @@ struct Engine {
           const size_t sb = s->splits.n ? 2 * s->split_buf_pairs : 0;  // split floats per time buffer
           const size_t stride = 6 * N + sb;
           const float* src = s->ckpt.p + size_t(k) * stride;
-          CK(cudaMemcpyAsync(s->fields.p + b * 6 * N, src, 6 * N * sizeof(float), cudaMemcpyDeviceToDevice, st));
+          CK(cudaMemcpyAsync(s->fields.p + b * 6 * N, src, 6 * N * sizeof(float), cudaMemcpyDeviceToDevice, rs));
           if (sb)
-            CK(cudaMemcpyAsync(s->splits.p + b * sb, src + 6 * N, sb * sizeof(float), cudaMemcpyDeviceToDevice, st));
+            CK(cudaMemcpyAsync(s->splits.p + b * sb, src + 6 * N, sb * sizeof(float), cudaMemcpyDeviceToDevice, rs));
         }
-        if (cfg.variant == 1) {
-          // the streaming kernel's tile counter as it stood before step n0
-          const unsigned c0 = unsigned(n0) * unsigned(scls.n_tiles + scls.grid);
-          CK(cudaMemcpyAsync(scls.d_counter.p, &c0, sizeof(unsigned), cudaMemcpyHostToDevice, st));
-          CK(cudaStreamSynchronize(st));  // c0 lives on this stack frame
-        }
-        for (int n = n0; n < n1; ++n) {  // the capture beside the step, as in a recorded run
-          CK(cudaEventRecord(cap_fork, st));
+        if (cfg.variant == 1) CK(cudaMemsetAsync(scls.d_counter.p, 0, sizeof(unsigned), rs));
+        for (int n = n0; n < n1; ++n) {
+          CK(cudaEventRecord(cap_fork, rs));
           CK(cudaStreamWaitEvent(cap_stream, cap_fork, 0));
-          adj_capture_kernel<<<dim3(cap_grid, unsigned(caps.size())), 256, 0, cap_stream>>>(d_c.p, n, n0);
+          adj_capture_kernel<<<dim3(cap_grid, unsigned(caps.size())), 256, 0, cap_stream>>>(d_c.p, n, h0);
           CK(cudaGetLastError());
           CK(cudaEventRecord(cap_join, cap_stream));
-          launch_step(st, n);
-          CK(cudaStreamWaitEvent(st, cap_join, 0));
+          launch_replay_step(rs, n, n0, n_sm, per_sm);
+          CK(cudaStreamWaitEvent(rs, cap_join, 0));
         }
-        for (int n = n1 - 1; n >= n0; --n) reverse_step(n, n0);
+        CK(cudaEventRecord(seg_done[k & 1], rs));
+      };
+      CK(cudaEventRecord(cap_fork, st));  // the replays start after this sweep's set-up on st
+      CK(cudaStreamWaitEvent(rs, cap_fork, 0));
+      replay(nseg - 1);
+      for (int k = nseg - 1; k >= 0; --k) {
+        if (k >= 1) {
+          // history half (k-1) & 1 was last read by the reversal of segment k+1
+          if (k + 1 < nseg) CK(cudaStreamWaitEvent(rs, seg_free[(k + 1) & 1], 0));
+          replay(k - 1);
+        }
+        const int n0 = k * K, n1 = std::min(nt, n0 + K);
+        CK(cudaStreamWaitEvent(st, seg_done[k & 1], 0));
+        for (int n = n1 - 1; n >= n0; --n) reverse_step(n, n0 - (k & 1) * K);
+        CK(cudaEventRecord(seg_free[k & 1], st));
       }
     }
     CK(cudaEventRecord(ev1, st));

@@ -45,6 +45,7 @@
 #include "fdtd_kernels.cuh"
 #include "tma.cuh"
 
+#include <climits>
 #include <type_traits>
 
 namespace rfn {
@@ -115,6 +116,15 @@ struct SlotPos {
   }
 };
 
+// A staged split region of one plane, as the producer describes it to the
+// consumers: its shared-memory offset, the cells of the plane that its store
+// holds (rows [ylo, yhi), columns [xlo, xhi)), and where those cells' pairs
+// lie in the store: cell (x, y) at pair base + y w + x, components comp apart.
+struct RegionRec {
+  int smem, ylo, yhi, xlo, xhi, w, comp, pad;
+  long long base;
+};
+
 __device__ __forceinline__ StreamTile load_stream_tile(const StreamTile* tiles, int i) {
   const int4* p = reinterpret_cast<const int4*>(tiles + i);
   const int4 a = __ldg(p), b = __ldg(p + 1), c = __ldg(p + 2);
@@ -162,7 +172,7 @@ fdtd_step_stream_kernel(const SimDev* __restrict__ sims, const StreamTile* __res
   float* xch = reinterpret_cast<float*>(smem);  // [2][ex, ez][ER][32]
   unsigned char* ring = smem + 2 * G::XCH;
   __shared__ __align__(8) uint64_t full[kSlotsMax], empty[kSlotsMax];
-  __shared__ int4 s_soff[kSlotsMax];           // each plane's regions: byte offsets of A and B, their stores (or -1)
+  __shared__ RegionRec s_rec[kSlotsMax][2];    // each plane's regions A and B (rows empty when not staged)
   __shared__ uint32_t s_ruser[kRegionsMax];    // last plane that used each region (producer only)
   __shared__ int s_tq[4];
   const int tid = threadIdx.x;
@@ -260,7 +270,22 @@ fdtd_step_stream_kernel(const SimDev* __restrict__ sims, const StreamTile* __res
           soff[rgn] = uint32_t(P) * G::MAIN + rs * G::REGION;
         }
         if (failed) break;
-        s_soff[slot] = make_int4(int(soff[0]), int(soff[1]), sa, sbs);
+        for (int rgn = 0; rgn < 2; ++rgn) {
+          const int st = rgn == 0 ? sa : sbs;
+          RegionRec rr{int(soff[rgn]), INT_MAX, INT_MAX, INT_MIN, INT_MAX, 0, 0, 0, 0};
+          if (st >= 0) {
+            // the cells of this plane that belong to store st (split_store's order: z, y, x)
+            const int t2 = sp->t[2], y3 = sims[td.sim].ny - sp->t[3];
+            rr.ylo = st == kStYhi ? y3 : (st == kStXlo || st == kStXhi) ? t2 : INT_MIN;
+            rr.yhi = st == kStYlo ? t2 : (st == kStXlo || st == kStXhi) ? y3 : INT_MAX;
+            rr.xlo = st == kStXhi ? sims[td.sim].nx - sp->t[1] : INT_MIN;
+            rr.xhi = st == kStXlo ? sp->t[0] : INT_MAX;
+            rr.w = sp->w[st];
+            rr.comp = int(sp->comp[st]);
+            rr.base = sp->off[st] + (int64_t(zp - sp->oz[st]) * sp->h[st] - sp->oy[st]) * sp->w[st] - sp->ox[st];
+          }
+          s_rec[slot][rgn] = rr;
+        }
         if (j == 0) s_tq[k & 3] = t;
         if (t < 0) {  // end of the stream: complete the phase without data
           mbar_arrive(&full[slot]);
@@ -359,18 +384,14 @@ fdtd_step_stream_kernel(const SimDev* __restrict__ sims, const StreamTile* __res
         const bool store = own_xy && i > 0;
         const int z = z0 - 1 + i;
         // split pairs of this plane: the slab stores the producer staged in
-        // regions A and B (region 0 / 1 of a cell whose store is one of them),
+        // regions A and B (region 0 / 1 of a cell that one of them holds),
         // other stores and sparse cells from global memory (region -1)
-        auto region_of = [&](int cst) -> int {
-          const int4 si = s_soff[cp.slot];
-          return cst == si.z ? 0 : cst == si.w ? 1 : -1;
-        };
+        const RegionRec* const rr = s_rec[cp.slot];
         // the E (m < 3) or H pair of component m of this cell, from its
         // staged region or the store
         auto pair_in = [&](int rgn, int m, const float2* gp, int cs) -> float2 {
           if (rgn < 0) return __ldg(gp + m * cs);
-          const int4 si = s_soff[cp.slot];
-          const unsigned char* rg = ring + (rgn == 0 ? si.x : si.y);
+          const unsigned char* rg = ring + rr[rgn].smem;
           return m < 3 ? reinterpret_cast<const float2*>(rg)[m * EC + eb]
                        : reinterpret_cast<const float2*>(rg + G::SPLIT_HS)[(m - 3) * G::SHC + sb];
         };
@@ -397,12 +418,19 @@ fdtd_step_stream_kernel(const SimDev* __restrict__ sims, const StreamTile* __res
         const uint32_t flags = __float_as_uint(r7.z);
         // a split cell's store, staged region (-1: none) and pair offset,
         // found once per plane for both phases
-        int cst = kStSparse, rgn = -1, cs = 0;
+        int rgn = -1, cs = 0;
         int64_t so = 0;
         if (!FAST && (flags & (kESplit | kHSplit))) {
-          cst = split_store(Sd.sp, Sd.nx, Sd.ny, Sd.nz, c, r, z);
-          rgn = region_of(cst);
-          so = split_off(Sd.sp, cst, c, r, z, __float_as_int(r7.w), cs);
+          rgn = r >= rr[0].ylo && r < rr[0].yhi && c >= rr[0].xlo && c < rr[0].xhi   ? 0
+                : r >= rr[1].ylo && r < rr[1].yhi && c >= rr[1].xlo && c < rr[1].xhi ? 1
+                                                                                     : -1;
+          if (rgn >= 0) {
+            so = rr[rgn].base + int64_t(r) * rr[rgn].w + c;
+            cs = rr[rgn].comp;
+          } else {
+            so = split_off(Sd.sp, split_store(Sd.sp, Sd.nx, Sd.ny, Sd.nz, c, r, z), c, r, z,
+                           __float_as_int(r7.w), cs);
+          }
         }
         float ex, ey, ez;
         if (FAST || !(flags & kESplit)) {

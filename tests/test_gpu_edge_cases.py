@@ -106,7 +106,7 @@ def _boxes_sim(shape, nt, kernel):
     return sim, len(pr)
 
 
-@pytest.mark.parametrize("shape", [(64, 56, 40), (70, 45, 37)])
+@pytest.mark.parametrize("shape", [(64, 56, 40), (70, 60, 37)])
 def test_slab_stores_stream_equals_plain(engine_lib, shape):
     """8-cell PML on all faces: the split pairs live in six slab stores (and a
     sparse store for the port cells); every streaming shape gives the plain
