@@ -270,19 +270,20 @@ void d2h(fdtd_sim* s, void* dst, const void* src, size_t bytes) {
 using StreamKernelFn = void (*)(const SimDev*, const StreamTile*, int, int, unsigned*, unsigned, int*, int, int,
                                 uint32_t, int);
 
-// One instantiation of the streaming step kernel (tile height TY) and the
-// bytes of its exchange buffers, plane slots and split slots.
+// One tile height of the streaming step kernel: the general and the
+// plain-tile instantiation, and the bytes of its exchange buffers, plane
+// slots and split regions.
 struct StreamVariant {
   int ty, threads, min_blocks;
   uint32_t xch_bytes, main_bytes, split_bytes;
-  StreamKernelFn fn;
+  StreamKernelFn fn, fn_plain;
 };
 
 template <int TY>
 StreamVariant stream_variant() {
   using G = StreamGeom<TY>;
   return StreamVariant{TY, G::THREADS, G::MIN_BLOCKS, uint32_t(2 * G::XCH), G::MAIN, G::REGION,
-                       &fdtd_step_stream_kernel<TY>};
+                       &fdtd_step_stream_kernel<TY, false>, &fdtd_step_stream_kernel<TY, true>};
 }
 
 const std::vector<StreamVariant>& stream_variants() {
@@ -396,17 +397,23 @@ struct StreamClass {
   const StreamVariant* v = nullptr;
   uint32_t ring = 0;                 // dynamic shared bytes: exchange buffers, plane slots, split slots
   int n_main = 0, n_reg = 0;
-  std::vector<StreamTile> host_tiles;
+  std::vector<StreamTile> host_tiles;     // tiles with split-field or probe cells (general kernel)
+  std::vector<StreamTile> host_tiles_p;   // plain tiles (plain-tile kernel, beside the general one)
   std::vector<StreamMaps> host_maps;
   DevBuf<StreamMaps> d_maps;
   DevBuf<SimDev> d_sims;
-  DevBuf<StreamTile> d_tiles;
-  DevBuf<unsigned> d_counter;
+  DevBuf<StreamTile> d_tiles, d_tiles_p;
+  DevBuf<unsigned> d_counter;        // tile counters: general list, plain list
   int n_tiles = 0, grid = 0;
+  int n_tiles_p = 0, grid_p = 0, n_main_p = 0;
+  uint32_t ring_p = 0;
   void reset() {
     v = nullptr;
-    ring = 0;
+    ring = ring_p = 0;
     host_tiles.clear();
+    host_tiles_p.clear();
+    d_tiles_p.free();
+    n_tiles_p = grid_p = n_main_p = 0;
     host_maps.clear();
     d_maps.free();
     d_sims.free();
@@ -433,6 +440,8 @@ struct Engine {
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   cudaStream_t cap_stream = nullptr;                   // box-history captures beside the steps
   cudaEvent_t cap_fork = nullptr, cap_join = nullptr;
+  cudaStream_t step_side = nullptr;                    // the plain-tile kernel beside the general one
+  cudaEvent_t step_fork = nullptr, step_join = nullptr;
   cudaStream_t rep_stream = nullptr;                   // checkpointed adjoint: segment replays
   cudaEvent_t seg_done[2] = {nullptr, nullptr};        // replay of a segment into history half k & 1 done
   cudaEvent_t seg_free[2] = {nullptr, nullptr};        // its reversal done: the half may be refilled
@@ -454,6 +463,9 @@ struct Engine {
     if (!cap_fork) CK(cudaEventCreateWithFlags(&cap_fork, cudaEventDisableTiming));
     if (!cap_join) CK(cudaEventCreateWithFlags(&cap_join, cudaEventDisableTiming));
     if (!rep_stream) CK(cudaStreamCreateWithFlags(&rep_stream, cudaStreamNonBlocking));
+    if (!step_side) CK(cudaStreamCreateWithFlags(&step_side, cudaStreamNonBlocking));
+    if (!step_fork) CK(cudaEventCreateWithFlags(&step_fork, cudaEventDisableTiming));
+    if (!step_join) CK(cudaEventCreateWithFlags(&step_join, cudaEventDisableTiming));
     for (int h = 0; h < 2; ++h) {
       if (!seg_done[h]) CK(cudaEventCreateWithFlags(&seg_done[h], cudaEventDisableTiming));
       if (!seg_free[h]) CK(cudaEventCreateWithFlags(&seg_free[h], cudaEventDisableTiming));
@@ -471,6 +483,9 @@ struct Engine {
       if (seg_free[h]) cudaEventDestroy(seg_free[h]);
     }
     if (rep_stream) cudaStreamDestroy(rep_stream);
+    if (step_fork) cudaEventDestroy(step_fork);
+    if (step_join) cudaEventDestroy(step_join);
+    if (step_side) cudaStreamDestroy(step_side);
     if (own_stream) cudaStreamDestroy(own_stream);
   }
 
@@ -574,7 +589,7 @@ struct Engine {
           if (e.code != FDTD_ERR_LIMIT) throw;
           continue;  // this shape's slots do not fit next to these grids' split slots
         }
-        CK(cudaMemsetAsync(scls.d_counter.p, 0, sizeof(unsigned), st));
+        CK(cudaMemsetAsync(scls.d_counter.p, 0, scls.d_counter.n * sizeof(unsigned), st));
         for (int n = 0; n < warm; ++n) launch_step(st, n);
         CK(cudaEventRecord(ev0, st));
         for (int n = warm; n < warm + timed; ++n) launch_step(st, n);
@@ -620,6 +635,16 @@ struct Engine {
     int per_sm = 0;
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, threads, smem));
     if (per_sm < 1) throw ArgError{FDTD_ERR_LIMIT, "Step kernel does not fit on an SM."};
+    // the plain-tile instantiation: plane slots only
+    int per_sm_p = 0;
+    {
+      int no_regions = 0;
+      c.ring_p = stream_slots(*c.v, cfg.stages, false, &c.n_main_p, &no_regions);
+      const void* fp = reinterpret_cast<const void*>(c.v->fn_plain);
+      CK(cudaFuncSetAttribute(fp, cudaFuncAttributeMaxDynamicSharedMemorySize, int(c.ring_p)));
+      CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_p, fp, threads, int(c.ring_p)));
+      if (per_sm_p < 1) throw ArgError{FDTD_ERR_LIMIT, "Step kernel does not fit on an SM."};
+    }
     int64_t cols = 0;
     for (auto* s : sims) cols += int64_t((s->nx + kStreamOwnX - 1) / kStreamOwnX) * ((s->ny + ty - 1) / ty);
     const int64_t slots = int64_t(per_sm) * n_sm;
@@ -698,30 +723,24 @@ struct Engine {
             c.host_tiles.push_back(t);
           }
     }
+    // Plain tiles go to the plain-tile kernel, the others to the general one.
     // Persistent blocks take tiles in list order, so the costliest go first
     // and the last tiles taken are short ones: a plane with split-field cells
     // costs about three ordinary planes. Stable, so tiles of equal cost keep
     // their z-chunk-major order and neighbours still share halos in L2.
+    {
+      std::vector<StreamTile> all;
+      all.swap(c.host_tiles);
+      for (const auto& t : all) (t.plain ? c.host_tiles_p : c.host_tiles).push_back(t);
+    }
     auto cost = [](const StreamTile& t) {
       return (t.z1 - t.z0 + 1) + 2 * (__builtin_popcount(t.split_lo) + __builtin_popcount(t.split_hi));
     };
-    const char* ord = std::getenv("RFN_TILE_ORDER");
-    if (ord && std::string(ord) == "chunk") {
-      // whole z chunks in turn, costliest chunk first, tiles of a chunk in
-      // (y, x) order: the blocks working at the same time are x / y
-      // neighbours of one chunk, so their halo rows are read from L2
-      std::map<std::pair<int, int>, int64_t> chunk_cost;
-      for (const auto& t : c.host_tiles) chunk_cost[{t.sim, t.z0}] += cost(t);
-      std::stable_sort(c.host_tiles.begin(), c.host_tiles.end(), [&](const StreamTile& a, const StreamTile& b) {
-        const int64_t ca = chunk_cost[{a.sim, a.z0}], cb = chunk_cost[{b.sim, b.z0}];
-        if (ca != cb) return ca > cb;
-        return std::make_pair(a.sim, a.z0) < std::make_pair(b.sim, b.z0);
-      });
-    } else {
-      std::stable_sort(c.host_tiles.begin(), c.host_tiles.end(),
+    for (auto* list : {&c.host_tiles, &c.host_tiles_p})
+      std::stable_sort(list->begin(), list->end(),
                        [&](const StreamTile& a, const StreamTile& b) { return cost(a) > cost(b); });
-    }
     c.n_tiles = int(c.host_tiles.size());
+    c.n_tiles_p = int(c.host_tiles_p.size());
     c.d_maps.alloc(c.host_maps.size());
     CK(cudaMemcpy(c.d_maps.p, c.host_maps.data(), c.host_maps.size() * sizeof(StreamMaps), cudaMemcpyHostToDevice));
     std::vector<SimDev> devs;
@@ -731,39 +750,71 @@ struct Engine {
     }
     c.d_sims.alloc(devs.size());
     CK(cudaMemcpy(c.d_sims.p, devs.data(), devs.size() * sizeof(SimDev), cudaMemcpyHostToDevice));
-    c.d_tiles.alloc(c.host_tiles.size());
-    CK(cudaMemcpy(c.d_tiles.p, c.host_tiles.data(), c.host_tiles.size() * sizeof(StreamTile), cudaMemcpyHostToDevice));
-    c.d_counter.alloc(1);
+    c.d_tiles.alloc(std::max<size_t>(1, c.host_tiles.size()));
+    if (c.n_tiles)
+      CK(cudaMemcpy(c.d_tiles.p, c.host_tiles.data(), c.host_tiles.size() * sizeof(StreamTile), cudaMemcpyHostToDevice));
+    c.d_tiles_p.alloc(std::max<size_t>(1, c.host_tiles_p.size()));
+    if (c.n_tiles_p)
+      CK(cudaMemcpy(c.d_tiles_p.p, c.host_tiles_p.data(), c.host_tiles_p.size() * sizeof(StreamTile),
+                    cudaMemcpyHostToDevice));
+    c.d_counter.alloc(2);
     c.grid = int(std::min<int64_t>(c.n_tiles, slots));
-    n_tiles = c.n_tiles;
-    grid = c.grid;
+    c.grid_p = int(std::min<int64_t>(c.n_tiles_p, int64_t(per_sm_p) * n_sm));
+    n_tiles = c.n_tiles + c.n_tiles_p;
+    grid = c.grid + c.grid_p;
   }
 
-  void launch_step(cudaStream_t st, int n) {
-    if (cfg.variant == 1) {
-      StreamClass& c = scls;
-      const unsigned base = unsigned(n) * unsigned(c.n_tiles + c.grid);
-      c.v->fn<<<c.grid, c.v->threads, c.ring, st>>>(c.d_sims.p, c.d_tiles.p, c.n_tiles, n, c.d_counter.p, base,
-                                                       d_err.p, c.n_main, c.n_reg, wait_limit, withhold);
+  // The streaming kernels of step n (counters counted from step n0, with at
+  // most `cap` blocks each): the general kernel on st and the plain-tile
+  // kernel beside it on a forked stream, or on st after it when `side` is
+  // false.
+  int launch_stream_step(cudaStream_t st, int n, int n0, int cap, bool side) {
+    StreamClass& c = scls;
+    const int g = std::min(c.grid, cap), gp = std::min(c.grid_p, cap);
+    const bool fork = side && c.n_tiles > 0 && c.n_tiles_p > 0;
+    if (fork) {
+      CK(cudaEventRecord(step_fork, st));
+      CK(cudaStreamWaitEvent(step_side, step_fork, 0));
+    }
+    if (c.n_tiles > 0) {
+      const unsigned base = unsigned(n - n0) * unsigned(c.n_tiles + g);
+      c.v->fn<<<g, c.v->threads, c.ring, st>>>(c.d_sims.p, c.d_tiles.p, c.n_tiles, n, c.d_counter.p, base, d_err.p,
+                                                  c.n_main, c.n_reg, wait_limit, withhold);
       CK(cudaGetLastError());
+    }
+    if (c.n_tiles_p > 0) {
+      const unsigned base = unsigned(n - n0) * unsigned(c.n_tiles_p + gp);
+      c.v->fn_plain<<<gp, c.v->threads, c.ring_p, fork ? step_side : st>>>(
+          c.d_sims.p, c.d_tiles_p.p, c.n_tiles_p, n, c.d_counter.p + 1, base, d_err.p, c.n_main_p, 0, wait_limit,
+          withhold);
+      CK(cudaGetLastError());
+    }
+    if (fork) {
+      CK(cudaEventRecord(step_join, step_side));
+      CK(cudaStreamWaitEvent(st, step_join, 0));
+    }
+    return int(c.n_tiles > 0) + int(c.n_tiles_p > 0);
+  }
+
+  // The kernels of time step n on st; returns how many were launched.
+  int launch_step(cudaStream_t st, int n) {
+    if (cfg.variant == 1) {
+      return launch_stream_step(st, n, 0, 1 << 30, true);
     } else {
       fdtd_step_kernel<kTileY><<<n_tiles, dim3(32, kBlockY), 0, st>>>(d_sims.p, d_tiles.p, n);
       CK(cudaGetLastError());
+      return 1;
     }
   }
 
   // Step n of a checkpointed adjoint's segment replay (segment from step n0),
-  // with the streaming kernel on at most `per_sm` blocks per SM, so that the
-  // reversal of the next segment, running at the same time on another
-  // stream, finds room on every SM. The tile counter was cleared before n0.
+  // with the streaming kernels on at most `per_sm` blocks per SM each, one
+  // after the other, so that the reversal of the next segment, running at the
+  // same time on another stream, finds room on every SM. The tile counters
+  // were cleared before n0.
   void launch_replay_step(cudaStream_t st, int n, int n0, int n_sm, int per_sm) {
     if (cfg.variant == 1) {
-      StreamClass& c = scls;
-      const int grid = std::min(c.grid, n_sm * per_sm);
-      const unsigned base = unsigned(n - n0) * unsigned(c.n_tiles + grid);
-      c.v->fn<<<grid, c.v->threads, c.ring, st>>>(c.d_sims.p, c.d_tiles.p, c.n_tiles, n, c.d_counter.p, base,
-                                                     d_err.p, c.n_main, c.n_reg, wait_limit, withhold);
-      CK(cudaGetLastError());
+      launch_stream_step(st, n, n0, n_sm * per_sm, false);
     } else {
       launch_step(st, n);
     }
@@ -954,7 +1005,7 @@ struct Engine {
           if (sb)
             CK(cudaMemcpyAsync(s->splits.p + b * sb, src + 6 * N, sb * sizeof(float), cudaMemcpyDeviceToDevice, rs));
         }
-        if (cfg.variant == 1) CK(cudaMemsetAsync(scls.d_counter.p, 0, sizeof(unsigned), rs));
+        if (cfg.variant == 1) CK(cudaMemsetAsync(scls.d_counter.p, 0, scls.d_counter.n * sizeof(unsigned), rs));
         for (int n = n0; n < n1; ++n) {
           CK(cudaEventRecord(cap_fork, rs));
           CK(cudaStreamWaitEvent(cap_stream, cap_fork, 0));
@@ -1003,7 +1054,7 @@ struct Engine {
       for (size_t m = 0; m < s->monitors.size(); ++m)
         CK(cudaMemsetAsync(s->mon_out[m]->p, 0, s->mon_out[m]->n, st));
     }
-    if (scls.d_counter.n) CK(cudaMemsetAsync(scls.d_counter.p, 0, sizeof(unsigned), st));
+    if (scls.d_counter.n) CK(cudaMemsetAsync(scls.d_counter.p, 0, scls.d_counter.n * sizeof(unsigned), st));
     int dft_from = 0;
     for (int n = 0; n < nt; ++n) {
       for (auto* s : sims)
@@ -1025,8 +1076,7 @@ struct Engine {
         CK(cudaGetLastError());
         CK(cudaEventRecord(cap_join, cap_stream));
       }
-      launch_step(st, n);
-      ++step_launches;
+      step_launches += launch_step(st, n);
       if (n_caps) CK(cudaStreamWaitEvent(st, cap_join, 0));
       for (auto* s : sims)
         if (!s->monitors.empty()) {

@@ -158,7 +158,11 @@ __device__ __forceinline__ void stream_inject(const SimDev& Sd, const float4& r7
   }
 }
 
-template <int TY>
+// PLAIN_ONLY: an instantiation for lists of plain tiles only, compiled
+// with the interior plane loop alone (fewer live registers, no split
+// regions); it runs beside the general instantiation, which takes the tiles
+// with split-field or probe cells.
+template <int TY, bool PLAIN_ONLY>
 __global__ void __launch_bounds__(StreamGeom<TY>::THREADS, StreamGeom<TY>::MIN_BLOCKS)
 fdtd_step_stream_kernel(const SimDev* __restrict__ sims, const StreamTile* __restrict__ tiles, int n_tiles, int n,
                         unsigned* __restrict__ counter, unsigned base, int* __restrict__ err, int n_main,
@@ -565,7 +569,11 @@ fdtd_step_stream_kernel(const SimDev* __restrict__ sims, const StreamTile* __res
       }
       return true;
     };
-    if (!(td.plain ? planes(std::true_type{}) : planes(std::false_type{}))) return;
+    if constexpr (PLAIN_ONLY) {
+      if (!planes(std::true_type{})) return;
+    } else {
+      if (!(td.plain ? planes(std::true_type{}) : planes(std::false_type{}))) return;
+    }
     // the look-ahead plane z1 was read only by the last iteration
     __syncwarp();
     if (lane == 0) mbar_arrive(&empty[cp.slot]);
