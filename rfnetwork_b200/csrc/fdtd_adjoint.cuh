@@ -171,6 +171,8 @@ adj_step_kernel(const AdjSim* __restrict__ sims, const int4* __restrict__ tiles,
     // ---- loads for the planes ahead (addresses from registers only)
     const int id_n4 = mat_at(z + 4);
     const uint32_t fl_n3 = flags_of(id_n3);
+    // the table row two planes ahead into L1 where the index changes (z-graded PML rows)
+    if (id_n2 != id_n1) prefetch_l1(rows + 8 * id_n2);
     float h_n2[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f}, e_n[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
     load_h(z + 2, fl_n2, h_n2);
     load_e(z + 1, fl_n1, e_n);

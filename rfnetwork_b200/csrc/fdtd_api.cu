@@ -462,7 +462,12 @@ struct Engine {
     if (!cap_stream) CK(cudaStreamCreateWithFlags(&cap_stream, cudaStreamNonBlocking));
     if (!cap_fork) CK(cudaEventCreateWithFlags(&cap_fork, cudaEventDisableTiming));
     if (!cap_join) CK(cudaEventCreateWithFlags(&cap_join, cudaEventDisableTiming));
-    if (!rep_stream) CK(cudaStreamCreateWithFlags(&rep_stream, cudaStreamNonBlocking));
+    if (!rep_stream) {
+      // the replays take SMs first as blocks retire; the reversal fills the rest
+      int lo = 0, hi = 0;
+      CK(cudaDeviceGetStreamPriorityRange(&lo, &hi));
+      CK(cudaStreamCreateWithPriority(&rep_stream, cudaStreamNonBlocking, hi));
+    }
     if (!step_side) CK(cudaStreamCreateWithFlags(&step_side, cudaStreamNonBlocking));
     if (!step_fork) CK(cudaEventCreateWithFlags(&step_fork, cudaEventDisableTiming));
     if (!step_join) CK(cudaEventCreateWithFlags(&step_join, cudaEventDisableTiming));

@@ -375,6 +375,11 @@ fdtd_step_kernel(const SimDev* __restrict__ sims, const int4* __restrict__ tiles
   }
 }
 
+// Brings the cache line holding p into L1 ahead of its use.
+__device__ __forceinline__ void prefetch_l1(const void* p) {
+  asm volatile("prefetch.global.L1 [%0];" ::"l"(p));
+}
+
 // Error codes the kernels record in the engine's error word.
 constexpr int kErrWaitExpired = 1;  // a bounded pipeline wait gave up
 constexpr int kErrNonFinite = 2;    // a probe record or a final field value is NaN or infinite

@@ -131,10 +131,6 @@ __device__ __forceinline__ StreamTile load_stream_tile(const StreamTile* tiles, 
   return StreamTile{a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w, uint32_t(c.x), uint32_t(c.y), uint32_t(c.z), uint32_t(c.w)};
 }
 
-__device__ __forceinline__ void prefetch_l1(const void* p) {
-  asm volatile("prefetch.global.L1 [%0];" ::"l"(p));
-}
-
 // Soft sources of one field group of a cell (solver.cu:459-488, 515-541):
 // s1 += v; s2 += v for every source probe on a component of that group (a
 // sourced component is always stored as its split pair).
