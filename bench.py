@@ -489,7 +489,8 @@ def reference_cuda_sequential(packed, nt, recs, cells_total):
 
 
 def workloads_entry(args, local_rank):
-    """One timed run of each other workload (N = 1), summarised."""
+    """One timed run of each other workload (N = 1; three gradient evaluations for the
+    adjoint, whose single wall-time samples vary most), summarised."""
     import argparse as _ap
     out = {}
     base = dict(vars(args))
@@ -511,7 +512,7 @@ def workloads_entry(args, local_rank):
                                       "sequential_plain_launches", "batched_over_sequential_plain_launches",
                                       "sequential_reference_cuda", "batched_over_sequential_reference_cuda",
                                       "mcell_updates_per_s", "bit_identical_to_sequential", "gpu_launches")),
-            ("adjoint", run_adjoint, {}, ("value", "unit", "ms_per_step", "forward_s", "gradient_over_forward",
+            ("adjoint", run_adjoint, dict(steps=3), ("value", "unit", "ms_per_step", "forward_s", "gradient_over_forward",
                                           "device", "recorded_history", "gpu_launches")),
             ("design", run_design, {}, ("value", "unit", "ms_per_step", "device", "sequential",
                                         "batched_over_sequential", "gpu_launches"))):
