@@ -15,7 +15,7 @@ def test_peak_fallback_and_measured(tmp_path, monkeypatch):
 
 
 def test_profiled_traffic_of_the_committed_summary(tmp_path):
-    assert bench.profiled_traffic(1) == 692300000          # profiles/fdtd_step_stream_boxes256.md
+    assert bench.profiled_traffic(1) == 636571136          # profiles/fdtd_step_stream_boxes256.md
     assert bench.profiled_traffic(0) is None               # the plain kernel's is not recorded there
     assert bench.profiled_traffic(1, tmp_path / "missing.md") is None
 
