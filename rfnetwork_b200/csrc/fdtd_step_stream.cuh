@@ -117,12 +117,15 @@ struct SlotPos {
 };
 
 // A staged split region of one plane, as the producer describes it to the
-// consumers: its shared-memory offset, the cells of the plane that its store
-// holds (rows [ylo, yhi), columns [xlo, xhi)), and where those cells' pairs
-// lie in the store: cell (x, y) at pair base + y w + x, components comp apart.
+// consumers: its shared-memory offset, and where the step writes the pairs of
+// its store's cells: cell (x, y) at pn + y w + x, components comp pairs apart.
+// `kind` (of region A) says which cells the staged stores hold: 0 every cell
+// of the plane (its z store), 1 the cells of the tile's y-face store (A) and
+// x-face store (B), -1 none (nothing staged).
 struct RegionRec {
-  int smem, ylo, yhi, xlo, xhi, w, comp, pad;
-  long long base;
+  int smem, w, comp, kind;
+  float2* pn;
+  long long pad;
 };
 
 __device__ __forceinline__ StreamTile load_stream_tile(const StreamTile* tiles, int i) {
@@ -172,7 +175,8 @@ fdtd_step_stream_kernel(const SimDev* __restrict__ sims, const StreamTile* __res
   float* xch = reinterpret_cast<float*>(smem);  // [2][ex, ez][ER][32]
   unsigned char* ring = smem + 2 * G::XCH;
   __shared__ __align__(8) uint64_t full[kSlotsMax], empty[kSlotsMax];
-  __shared__ RegionRec s_rec[kSlotsMax][2];    // each plane's regions A and B (rows empty when not staged)
+  __shared__ RegionRec s_rec[kSlotsMax][2];    // each plane's regions A and B
+  __shared__ signed char s_memb[G::CONSUMERS];  // each consumer cell's region on core planes (own thread only)
   __shared__ uint32_t s_ruser[kRegionsMax];    // last plane that used each region (producer only)
   __shared__ int s_tq[4];
   const int tid = threadIdx.x;
@@ -272,17 +276,13 @@ fdtd_step_stream_kernel(const SimDev* __restrict__ sims, const StreamTile* __res
         if (failed) break;
         for (int rgn = 0; rgn < 2; ++rgn) {
           const int st = rgn == 0 ? sa : sbs;
-          RegionRec rr{int(soff[rgn]), INT_MAX, INT_MAX, INT_MIN, INT_MAX, 0, 0, 0, 0};
+          RegionRec rr{int(soff[rgn]), 0, 0, -1, nullptr, 0};
+          if (rgn == 0) rr.kind = sa == kStZlo || sa == kStZhi ? 0 : (sa >= 0 || sbs >= 0) ? 1 : -1;
           if (st >= 0) {
-            // the cells of this plane that belong to store st (split_store's order: z, y, x)
-            const int t2 = sp->t[2], y3 = sims[td.sim].ny - sp->t[3];
-            rr.ylo = st == kStYhi ? y3 : (st == kStXlo || st == kStXhi) ? t2 : INT_MIN;
-            rr.yhi = st == kStYlo ? t2 : (st == kStXlo || st == kStXhi) ? y3 : INT_MAX;
-            rr.xlo = st == kStXhi ? sims[td.sim].nx - sp->t[1] : INT_MIN;
-            rr.xhi = st == kStXlo ? sp->t[0] : INT_MAX;
+            const int64_t o = sp->off[st] + (int64_t(zp - sp->oz[st]) * sp->h[st] - sp->oy[st]) * sp->w[st] - sp->ox[st];
             rr.w = sp->w[st];
             rr.comp = int(sp->comp[st]);
-            rr.base = sp->off[st] + (int64_t(zp - sp->oz[st]) * sp->h[st] - sp->oy[st]) * sp->w[st] - sp->ox[st];
+            rr.pn = sp->base[cur ^ 1] + o;
           }
           s_rec[slot][rgn] = rr;
         }
@@ -359,6 +359,16 @@ fdtd_step_stream_kernel(const SimDev* __restrict__ sims, const StreamTile* __res
     const int ib = w * G::IW + oi + lane;
     const int sb = (w - 1) * G::EW + oh + lane;    // H split box (owned rows)
     int idx = (z0 - 1) * plane + r * Sd.pitch + c; // cell offset of plane z (owned cells, z >= z0)
+    // this thread's cell on the tile's core planes: held by the tile's y-face
+    // store (staged as region A: 0), its x-face store (region B: 1) or neither
+    // (kept in shared memory: no register across the plane loop)
+    if (!PLAIN_ONLY && !td.plain) {
+      const int t0 = Sd.sp.t[0], t1 = Sd.sp.t[1], t2 = Sd.sp.t[2], y3 = Sd.ny - Sd.sp.t[3];
+      int memb = -1;
+      if ((td.ys == kStYlo && r < t2) || (td.ys == kStYhi && r >= y3)) memb = 0;
+      else if (r >= t2 && r < y3 && ((td.xs == kStXlo && c < t0) || (td.xs == kStXhi && c >= Sd.nx - t1))) memb = 1;
+      s_memb[tid] = (signed char)memb;
+    }
 
     // The plane loop, instantiated for plain tiles (FAST: every cell unsplit,
     // no probes, so no per-cell flag tests) and for the general case.
@@ -418,14 +428,14 @@ fdtd_step_stream_kernel(const SimDev* __restrict__ sims, const StreamTile* __res
         const uint32_t flags = __float_as_uint(r7.z);
         // a split cell's store, staged region (-1: none) and pair offset,
         // found once per plane for both phases
+        // (so: from the staged region's pointers, or from the store base for region -1)
         int rgn = -1, cs = 0;
         int64_t so = 0;
         if (!FAST && (flags & (kESplit | kHSplit))) {
-          rgn = r >= rr[0].ylo && r < rr[0].yhi && c >= rr[0].xlo && c < rr[0].xhi   ? 0
-                : r >= rr[1].ylo && r < rr[1].yhi && c >= rr[1].xlo && c < rr[1].xhi ? 1
-                                                                                     : -1;
+          const int kind = rr[0].kind;
+          rgn = kind == 0 ? 0 : kind == 1 ? int(s_memb[tid]) : -1;
           if (rgn >= 0) {
-            so = rr[rgn].base + int64_t(r) * rr[rgn].w + c;
+            so = int64_t(r) * rr[rgn].w + c;
             cs = rr[rgn].comp;
           } else {
             so = split_off(Sd.sp, split_store(Sd.sp, Sd.nx, Sd.ny, Sd.nz, c, r, z), c, r, z,
@@ -441,7 +451,7 @@ fdtd_step_stream_kernel(const SimDev* __restrict__ sims, const StreamTile* __res
         } else {
           // per component: the split pair (one 8-byte load) or the unsplit total
           float2 sp[3];
-          const float2* gp = Sd.sp.base[cur] + so;
+          const float2* gp = rgn >= 0 ? nullptr : Sd.sp.base[cur] + so;  // read only for region -1
   #pragma unroll
           for (int m = 0; m < 3; ++m) sp[m] = make_float2(0.f, 0.f);
           if (flags & (kCompSplit0 << 0)) {
@@ -470,7 +480,7 @@ fdtd_step_stream_kernel(const SimDev* __restrict__ sims, const StreamTile* __res
           if (flags & (kCompSplit0 << 1)) ey = __fadd_rn(sp[1].x, sp[1].y);
           if (flags & (kCompSplit0 << 2)) ez = __fadd_rn(sp[2].x, sp[2].y);
           if (store) {
-            float2* po = Sd.sp.base[nxt] + so;
+            float2* po = rgn >= 0 ? rr[rgn].pn + so : Sd.sp.base[nxt] + so;
   #pragma unroll
             for (int m = 0; m < 3; ++m)
               if (flags & (kCompSplit0 << m)) po[m * cs] = sp[m];
@@ -509,7 +519,7 @@ fdtd_step_stream_kernel(const SimDev* __restrict__ sims, const StreamTile* __res
             hz = upd_h(rv.x, hz_c, gzx, gzy);
           } else {
             float2 sp[3];
-            const float2* gp = Sd.sp.base[cur] + so;
+            const float2* gp = rgn >= 0 ? nullptr : Sd.sp.base[cur] + so;  // read only for region -1
   #pragma unroll
             for (int m = 0; m < 3; ++m) sp[m] = make_float2(0.f, 0.f);
             if (flags & (kCompSplit0 << 3)) {
@@ -537,7 +547,7 @@ fdtd_step_stream_kernel(const SimDev* __restrict__ sims, const StreamTile* __res
             if (flags & (kCompSplit0 << 3)) hx = __fadd_rn(sp[0].x, sp[0].y);
             if (flags & (kCompSplit0 << 4)) hy = __fadd_rn(sp[1].x, sp[1].y);
             if (flags & (kCompSplit0 << 5)) hz = __fadd_rn(sp[2].x, sp[2].y);
-            float2* po = Sd.sp.base[nxt] + so;
+            float2* po = rgn >= 0 ? rr[rgn].pn + so : Sd.sp.base[nxt] + so;
   #pragma unroll
             for (int m = 0; m < 3; ++m)
               if (flags & (kCompSplit0 << (3 + m))) po[(3 + m) * cs] = sp[m];
