@@ -514,8 +514,8 @@ def workloads_entry(args, local_rank):
                                       "mcell_updates_per_s", "bit_identical_to_sequential", "gpu_launches")),
             ("adjoint", run_adjoint, dict(steps=3), ("value", "unit", "ms_per_step", "forward_s", "gradient_over_forward",
                                           "device", "recorded_history", "gpu_launches")),
-            ("design", run_design, {}, ("value", "unit", "ms_per_step", "device", "sequential",
-                                        "batched_over_sequential", "gpu_launches"))):
+            ("design", run_design, {}, ("value", "unit", "ms_per_step", "device", "recorded_history",
+                                        "sequential", "batched_over_sequential", "gpu_launches"))):
         t0 = time.perf_counter()
         try:
             line = fn(ns(**kw), 0, 1, local_rank)
@@ -812,58 +812,70 @@ def run_design(args, rank, world, local_rank):
     """32 variants of a 96x96x64 microstrip (10-cell PML, 3000 steps), each with its own
     32x32x4-cell design block above the strip, eps_r = 1 + 9 sigmoid(theta), theta ~ N(0, 1)
     (seed 5); J_i = sum over 5 frequencies (8-12 GHz) of |DFT of the output Ez probe|^2.
-    One step = one Adam step (lr 0.05) on all 32 designs: a batched forward solve with the
-    box histories recorded, a batched adjoint sweep, the optimizer update."""
+    One step = one Adam step (lr 0.05) on all 32 designs: a batched forward solve with state
+    snapshots every ~sqrt(nt) steps, a batched adjoint sweep that replays the segments of all
+    variants together, the optimizer update. Beside it: the same Adam step with the box
+    histories recorded instead (no replay), and the 32 gradients one after another through
+    FDTDDesign with the same checkpoints."""
+    import math
     import torch
     from modelgen import configs
-    from rfnetwork_b200.adjoint import FDTDDesignBatch
+    from rfnetwork_b200.adjoint import FDTDDesign, FDTDDesignBatch
 
     torch.cuda.set_device(local_rank)
     ranks = RankSync(world, local_rank)
     nt = args.nt if args.nt != NT else 3000
     n_var = 32
+    every = max(1, round(math.sqrt(nt)))
     s = configs.microstrip(n=(96, 96, 64), n_pml=10, nt=nt)
     co, pr, *_ = s.pack_inputs(gpu=True)
     omega = 2 * np.pi * np.linspace(8e9, 12e9, 5) * float(s.dt)
     box = (32, 64, 32, 64, 22, 26)
-    designs = FDTDDesignBatch([s] * n_var, box, [(0, len(pr) - 1, 1.0)], omega)
+    terms = [(0, len(pr) - 1, 1.0)]
     gen = torch.Generator().manual_seed(5)
-    theta = torch.randn(n_var, 32, 32, 4, dtype=torch.float64, generator=gen).requires_grad_(True)
-    opt = torch.optim.Adam([theta], lr=0.05)
-    scale = None
-    J_hist = []
+    theta0 = torch.randn(n_var, 32, 32, 4, dtype=torch.float64, generator=gen)
 
-    def adam_step():
-        nonlocal scale
-        opt.zero_grad()
-        X = designs(list(1 + 9 * torch.sigmoid(theta)))
-        J = (X.abs() ** 2).sum(dim=(1, 2))          # per variant
-        if scale is None:
-            scale = float(J.detach().mean())
-        (-(J / scale).sum()).backward()               # maximise the output power of every variant
-        opt.step()
-        J_hist.append(J.detach().numpy() / scale)
+    def adam_loop(designs):
+        """Warm-up and timed Adam steps from theta0; wall times, device times, objectives."""
+        theta = theta0.clone().requires_grad_(True)
+        opt = torch.optim.Adam([theta], lr=0.05)
+        scale = None
+        J_hist = []
 
-    for _ in range(max(args.warmup, 1)):
-        adam_step()
-    t = []
-    fwd_ms, adj_ms = [], []
-    for _ in range(args.steps):
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        adam_step()
-        torch.cuda.synchronize()
-        t.append(time.perf_counter() - t0)
+        def adam_step():
+            nonlocal scale
+            opt.zero_grad()
+            X = designs(list(1 + 9 * torch.sigmoid(theta)))
+            J = (X.abs() ** 2).sum(dim=(1, 2))          # per variant
+            if scale is None:
+                scale = float(J.detach().mean())
+            (-(J / scale).sum()).backward()               # maximise the output power of every variant
+            opt.step()
+            J_hist.append(J.detach().numpy() / scale)
+
+        for _ in range(max(args.warmup, 1)):
+            adam_step()
+        t, fwd_ms, adj_ms = [], [], []
+        for _ in range(args.steps):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            adam_step()
+            torch.cuda.synchronize()
+            t.append(time.perf_counter() - t0)
+            st = designs.batch.stats()
+            fwd_ms.append(st["last_run_ms"])
+            adj_ms.append(st["adjoint_ms"])
         st = designs.batch.stats()
-        fwd_ms.append(st["last_run_ms"])
-        adj_ms.append(st["adjoint_ms"])
-    st = designs.batch.stats()
-    designs.close()
+        designs.close()
+        return theta.detach(), t, fwd_ms, adj_ms, st, J_hist
+
+    th, t, fwd_ms, adj_ms, st, J_hist = adam_loop(FDTDDesignBatch([s] * n_var, box, terms, omega,
+                                                                  checkpoint_every=every))
+    _, t_rec, fwd_rec, adj_rec, _, _ = adam_loop(FDTDDesignBatch([s] * n_var, box, terms, omega,
+                                                                 history_budget=float("inf")))
     # the same gradients one variant after another: one model, one forward
-    # (recorded box history) and one adjoint per variant
-    from rfnetwork_b200.adjoint import FDTDDesign
-    single = FDTDDesign(s, box, [(0, len(pr) - 1, 1.0)], omega)
-    th = theta.detach()
+    # (same checkpoints) and one adjoint per variant
+    single = FDTDDesign(s, box, terms, omega, checkpoint_every=every)
 
     def sequential_pass():
         for v in range(n_var):
@@ -880,26 +892,37 @@ def run_design(args, rank, world, local_rank):
         t_seq.append(time.perf_counter() - t0)
     single.close()
     ts = ranks.max(statistics.fmean(t))   # wall time of the slowest rank
+    ts_rec = ranks.max(statistics.fmean(t_rec))
     ts_seq = ranks.max(statistics.fmean(t_seq))
     ranks.close()
     if rank != 0:
         return None
     cells = 96 * 96 * 64
+
+    def device(fw, ad):
+        return {"forward_ms": round(statistics.fmean(fw), 1), "adjoint_ms": round(statistics.fmean(ad), 1),
+                "forward_mcell_updates_per_s": round(n_var * cells * nt / statistics.fmean(fw) / 1e3, 1),
+                "adjoint_mcell_updates_per_s": round(n_var * cells * nt / statistics.fmean(ad) / 1e3, 1)}
+
     return {
         "metric": "grad evals/s", "value": round(world * n_var / ts, 3), "unit": "gradient evaluations/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ts * 1e3, 1),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32 fields, f64 accumulators",
         "data": "synthetic: microstrip background, seeded theta per variant",
         "config": {"workload": f"design: {n_var} variants of 96x96x64, 10-cell PML, {nt} steps, 32x32x4 design "
-                               "each, 5 freqs, Adam lr 0.05", "time_steps": nt, "variants": n_var,
-                   "step": "one Adam step of all variants (batched forward + batched adjoint), wall time"},
-        "device": {"forward_ms": round(statistics.fmean(fwd_ms), 1), "adjoint_ms": round(statistics.fmean(adj_ms), 1),
-                   "forward_mcell_updates_per_s": round(n_var * cells * nt / statistics.fmean(fwd_ms) / 1e3, 1),
-                   "adjoint_mcell_updates_per_s": round(n_var * cells * nt / statistics.fmean(adj_ms) / 1e3, 1)},
+                               f"each, 5 freqs, Adam lr 0.05, checkpoints every {every}", "time_steps": nt,
+                   "variants": n_var, "checkpoint_every": every,
+                   "step": "one Adam step of all variants (batched forward with checkpoints + batched adjoint "
+                           "with segment replays), wall time"},
+        "device": device(fwd_ms, adj_ms),
         "objective_mean": [round(float(np.mean(j)), 4) for j in J_hist],
+        "recorded_history": {"value": round(world * n_var / ts_rec, 3), "ms_per_step": round(ts_rec * 1e3, 1),
+                             "device": device(fwd_rec, adj_rec),
+                             "how": "the same Adam steps with every variant's box history recorded by the "
+                                    "batched forward (no replay in the adjoint)"},
         "sequential": {"value": round(world * n_var / ts_seq, 3), "unit": "gradient evaluations/s",
-                       "how": f"the {n_var} gradients one after another through FDTDDesign (forward with the "
-                              "recorded box history, then the adjoint), wall time, no optimizer step"},
+                       "how": f"the {n_var} gradients one after another through FDTDDesign (forward with "
+                              f"checkpoints every {every}, then the adjoint), wall time, no optimizer step"},
         "batched_over_sequential": round(ts_seq / ts, 3),
         "gpu_launches": int(st["step_launches"] + st["adjoint_launches"]),
     }

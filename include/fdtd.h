@@ -232,11 +232,16 @@ int fdtd_batch_set_stream(fdtd_batch* b, void* stream);
 int fdtd_batch_get_stats(const fdtd_batch* b, fdtd_stats* out);
 
 /* Gradients of a batch (no reference counterpart): fdtd_batch_run_recorded is
- * fdtd_run_recorded for every member, boxes = n_sims x 6 ints; then
+ * fdtd_run_recorded for every member, boxes = n_sims x 6 ints;
+ * fdtd_batch_run_checkpointed is fdtd_run_checkpointed for every member (state
+ * snapshots every `every` steps), with the boxes fixed at the run. Then
  * fdtd_batch_adjoint runs the adjoints of all members together, one launch per
- * reverse step over all their tiles. dJ_dX[i] and grad[i] are member i's
- * arrays, sized as for fdtd_adjoint by its own DFT and box. */
+ * reverse step over all their tiles; after a checkpointed run it replays each
+ * segment of all members with one step launch per time step. dJ_dX[i] and
+ * grad[i] are member i's arrays, sized as for fdtd_adjoint by its own DFT and
+ * box. */
 int fdtd_batch_run_recorded(fdtd_batch* b, int nt, const int* boxes);
+int fdtd_batch_run_checkpointed(fdtd_batch* b, int nt, int every, const int* boxes);
 int fdtd_batch_adjoint(fdtd_batch* b, const double* const* dJ_dX, double* const* grad);
 const char* fdtd_batch_last_error(const fdtd_batch* b);
 void fdtd_batch_destroy(fdtd_batch* b);

@@ -24,7 +24,7 @@ EXPORTED = (
     "fdtd_batch_create", "fdtd_batch_run", "fdtd_batch_set_stream", "fdtd_batch_get_stats",
     "fdtd_batch_last_error", "fdtd_batch_destroy", "fdtd_global_error", "fdtd_step_noalloc",
     "fdtd_run_checkpointed", "fdtd_run_recorded", "fdtd_adjoint", "fdtd_batch_run_recorded",
-    "fdtd_batch_adjoint", "fdtd_set_graph", "fdtd_set_box_coefficients", "fdtd_nf2ff", "fdtd_set_debug",
+    "fdtd_batch_run_checkpointed", "fdtd_batch_adjoint", "fdtd_set_graph", "fdtd_set_box_coefficients", "fdtd_nf2ff", "fdtd_set_debug",
 )
 
 
@@ -103,6 +103,7 @@ def load():
         "fdtd_run_recorded": ([vp, ip, vp], ip),
         "fdtd_adjoint": ([vp, vp, ip, ip, vp, vp], ip),
         "fdtd_batch_run_recorded": ([vp, ip, vp], ip),
+        "fdtd_batch_run_checkpointed": ([vp, ip, ip, vp], ip),
         "fdtd_batch_adjoint": ([vp, pp, pp], ip),
     }
     for name, (args, res) in sig.items():
@@ -367,8 +368,18 @@ class Batch:
         for s in self.sims:
             s.nt = int(nt)
 
+    def run_checkpointed(self, nt: int, every: int, boxes):
+        """Batched ``Simulation.run_checkpointed`` (state snapshots every ``every``
+        steps); boxes[i] is member i's gradient box, fixed at the run."""
+        b = np.ascontiguousarray(boxes, dtype=np.int32).reshape(len(self.sims), 6)
+        self._check(self.lib.fdtd_batch_run_checkpointed(self.h, int(nt), int(every), _ptr(b)))
+        self.boxes = b.copy()
+        for s in self.sims:
+            s.nt = int(nt)
+
     def adjoint(self, dJ_dX) -> list:
-        """Gradients of all members after ``run_recorded``: dJ_dX[i] complex [series, freq] of member i."""
+        """Gradients of all members after ``run_recorded`` or ``run_checkpointed``:
+        dJ_dX[i] complex [series, freq] of member i."""
         gs = [_dj_pairs(d) for d in dJ_dX]
         outs = [np.empty(_grad_shape(b), dtype=np.float64) for b in self.boxes]
         n = len(self.sims)

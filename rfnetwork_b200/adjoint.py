@@ -230,22 +230,36 @@ class FDTDDesignBatch:
         designs = FDTDDesignBatch([model] * 32, box, terms, omega)
         X = designs([1 + 9 * torch.sigmoid(t) for t in thetas])   # complex [member, series, freq]
 
-    Every member keeps the box history of its forward run (fdtd_batch_run_recorded);
-    the gradient boxes must have one shape so the coefficients stack."""
+    As for one design, the members keep the box history of their forward run
+    (fdtd_batch_run_recorded) while all histories together fit
+    ``history_budget`` bytes and ``checkpoint_every`` is not given; otherwise
+    each member's state is snapshot every ``checkpoint_every`` (default
+    ~sqrt(nt)) steps (fdtd_batch_run_checkpointed) and the batched adjoint
+    replays the segments of all members together. The gradient boxes must have
+    one shape so the coefficients stack."""
 
-    def __init__(self, models, design_box, terms, omega):
+    def __init__(self, models, design_box, terms, omega, checkpoint_every: int | None = None,
+                 history_budget: float = 8 * 2**30):
         self.members = [FDTDDesign(m, design_box, terms, omega, checkpoint_every=None, history_budget=float("inf"))
                         for m in models]
         shapes = {tuple(b - a for a, b in zip(m.box[0::2], m.box[1::2])) for m in self.members}
         if len(shapes) != 1 or len({m.nt for m in self.members}) != 1:
             raise ValueError("batch members need one gradient-box shape and one number of time steps")
         self.nt = self.members[0].nt
+        bx0, bx1, by0, by1, bz0, bz1 = self.members[0].box
+        history_bytes = 36 * (bx1 - bx0) * (by1 - by0) * (bz1 - bz0) * self.nt * len(self.members)
+        self.recorded = checkpoint_every is None and history_bytes <= history_budget
+        self.checkpoint_every = None if self.recorded else int(checkpoint_every or max(1, round(math.sqrt(self.nt))))
         self.batch = Batch([m.sim for m in self.members])
 
     def _run(self, coefs: np.ndarray) -> np.ndarray:
         for m, c in zip(self.members, coefs):
             m._set(c)
-        self.batch.run_recorded(self.nt, [m.box for m in self.members])
+        boxes = [m.box for m in self.members]
+        if self.recorded:
+            self.batch.run_recorded(self.nt, boxes)
+        else:
+            self.batch.run_checkpointed(self.nt, self.checkpoint_every, boxes)
         return np.stack([m.sim.dft() for m in self.members])
 
     def __call__(self, eps_r, sigma=None):

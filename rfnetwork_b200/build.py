@@ -21,7 +21,7 @@ LIB = PKG / "librfn_fdtd.so"
 NVCC = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 SOURCES = ["fdtd_api.cu", "fdtd_compile.cpp"]
-HEADERS = ["fdtd_kernels.cuh", "fdtd_step_stream.cuh", "fdtd_adjoint.cuh", "fdtd_nf2ff.cuh", "tma.cuh", "fdtd_compile.h"]
+HEADERS = ["fdtd_kernels.cuh", "fdtd_step_stream.cuh", "fdtd_adjoint.cuh", "fdtd_adjoint_stream.cuh", "fdtd_nf2ff.cuh", "tma.cuh", "fdtd_compile.h"]
 
 
 def _stale() -> bool:

@@ -84,6 +84,73 @@ __device__ __forceinline__ void adj_load_h(const float* tot, const float* half, 
 
 __device__ __forceinline__ uint32_t adj_flags(const float4* row) { return __float_as_uint(__ldg(row + 7).z); }
 
+// Per-cell arithmetic of one reverse step, with the rounding fixed by
+// intrinsics so that every kernel that uses it gives the same bits.
+//
+// E part: from the cell's E adjoint lE (totals in 0..2, or six halves), its
+// own H adjoint h (six halves; an unsplit cell's halves repeat its totals),
+// the Db1-weighted H adjoints of its +1 neighbours (z: qz_hx, qz_hy; x:
+// qx_hy, qx_hz; y: qy_hx, qy_hz) and its table row: mu, lamE' (into lE) and
+// the adjoints ad of the six H differences.
+__device__ __forceinline__ void adj_e_part(const float4& ra, const float4& rb, const float4& rd, const float4& p,
+                                           const float4& q, const float4& u, const float4& v, const float4& r7,
+                                           uint32_t fl, const float (&h)[6], float qz_hx, float qz_hy, float qx_hy,
+                                           float qx_hz, float qy_hx, float qy_hz, float (&lE)[6], float (&mu)[6],
+                                           float (&ad)[6]) {
+  // Db2 slots: hx_y p.z, hx_z q.y, hy_z u.x, hy_x u.w, hz_x v.z, hz_y r7.y
+  const float aEx = __fadd_rn(__fmaf_rn(u.x, h[2], -qz_hy), __fmaf_rn(r7.y, h[5], -qy_hz));
+  const float aEy = __fadd_rn(__fmaf_rn(q.y, h[1], -qz_hx), __fmaf_rn(v.z, h[4], -qx_hz));
+  const float aEz = __fadd_rn(__fmaf_rn(p.z, h[0], -qy_hx), __fmaf_rn(u.w, h[3], -qx_hy));
+  if (!(fl & kESplit)) {
+    const float mx = __fadd_rn(lE[0], aEx), my = __fadd_rn(lE[1], aEy), mz = __fadd_rn(lE[2], aEz);
+    mu[0] = mx; mu[1] = mx; mu[2] = my; mu[3] = my; mu[4] = mz; mu[5] = mz;
+    lE[0] = __fmul_rn(ra.x, mx); lE[1] = __fmul_rn(rb.x, my); lE[2] = __fmul_rn(rd.x, mz);
+  } else {
+    const float aE[3] = {aEx, aEy, aEz};
+    const float ca[6] = {ra.x, ra.z, rb.x, rb.z, rd.x, rd.z};
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+      mu[k] = __fadd_rn(lE[k], aE[k / 2]);
+      lE[k] = __fmul_rn(ca[k], mu[k]);
+    }
+  }
+  const float cb[6] = {ra.y, ra.w, rb.y, rb.w, rd.y, rd.w};
+#pragma unroll
+  for (int k = 0; k < 6; ++k) ad[k] = __fmul_rn(cb[k], mu[k]);
+}
+
+// H part: lamH' of a cell from its H adjoint h, its ad and the ad of its -1
+// neighbours (y: a0_m, a5_m; x: a3_m, a4_m; z: a1_p, a2_p).
+__device__ __forceinline__ void adj_h_part(const float4& p, const float4& q, const float4& u, const float4& v,
+                                           uint32_t fl, const float (&h)[6], const float (&ad)[6], float a0_m,
+                                           float a5_m, float a3_m, float a4_m, float a1_p, float a2_p,
+                                           float (&lh)[6]) {
+  const float aH[3] = {__fadd_rn(__fsub_rn(a2_p, ad[2]), __fsub_rn(a5_m, ad[5])),
+                       __fadd_rn(__fsub_rn(a1_p, ad[1]), __fsub_rn(a4_m, ad[4])),
+                       __fadd_rn(__fsub_rn(a0_m, ad[0]), __fsub_rn(a3_m, ad[3]))};
+  if (!(fl & kHSplit)) {
+    lh[0] = __fmaf_rn(p.x, h[0], aH[0]);
+    lh[1] = __fmaf_rn(q.z, h[2], aH[1]);
+    lh[2] = __fmaf_rn(v.x, h[4], aH[2]);
+  } else {
+    const float da[6] = {p.x, p.w, q.z, u.y, v.x, v.w};
+#pragma unroll
+    for (int k = 0; k < 6; ++k) lh[k] = __fmaf_rn(da[k], h[k], aH[k / 2]);
+  }
+}
+
+// dJ/d(Ca, Cb1, Cb2) of one box cell accumulated for one step (FP64).
+__device__ __forceinline__ void adj_grad_cell(double* grad, int64_t nb, int64_t bi, const float* hs,
+                                              const float (&mu)[6]) {
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    double* g = grad + 3 * k * nb + bi;
+    g[0] = __fma_rn(double(mu[2 * k]), double(__ldg(hs + k * nb + bi)), g[0]);
+    g[nb] = __fma_rn(double(mu[2 * k]), double(__ldg(hs + (3 + 2 * k) * nb + bi)), g[nb]);
+    g[2 * nb] = __fma_rn(double(mu[2 * k + 1]), double(__ldg(hs + (4 + 2 * k) * nb + bi)), g[2 * nb]);
+  }
+}
+
 // Tile of the adjoint step kernel: lane 0 is the -1 halo column, lanes 1..30
 // the owned columns and lane 31 only provides Db1 lamH of the column above
 // the tile (x0 + 30) to lane 30; warp 0 is the -1 halo row, warps 1..TY the
@@ -156,8 +223,8 @@ adj_step_kernel(const AdjSim* __restrict__ sims, const int4* __restrict__ tiles,
   load_e(z0 - 1, fl_c, e_c);
   {
     const float4* rc = rows + 8 * id_c;
-    s_qhx[(z0 - 1) & 1][w][lane] = __ldg(rc + 3).y * h_c[0];
-    s_qhz[(z0 - 1) & 1][w][lane] = __ldg(rc + 7).x * h_c[5];
+    s_qhx[(z0 - 1) & 1][w][lane] = __fmul_rn(__ldg(rc + 3).y, h_c[0]);
+    s_qhz[(z0 - 1) & 1][w][lane] = __fmul_rn(__ldg(rc + 7).x, h_c[5]);
   }
   float a1_p = 0.f, a2_p = 0.f;
   __syncthreads();
@@ -192,39 +259,19 @@ adj_step_kernel(const AdjSim* __restrict__ sims, const int4* __restrict__ tiles,
 
     // ---- Db1 lamH of the +1 neighbours: z+1 from the look-ahead, x+1 from
     // the lane on the right, y+1 from the row above (written last plane)
-    const float qz_hx = qn_x * h_n[1], qz_hy = qn_w * h_n[2];
-    const float qx_hy = __shfl_down_sync(0xffffffffu, u.z * h_c[3], 1);
-    const float qx_hz = __shfl_down_sync(0xffffffffu, v.y * h_c[4], 1);
+    const float qz_hx = __fmul_rn(qn_x, h_n[1]), qz_hy = __fmul_rn(qn_w, h_n[2]);
+    const float qx_hy = __shfl_down_sync(0xffffffffu, __fmul_rn(u.z, h_c[3]), 1);
+    const float qx_hz = __shfl_down_sync(0xffffffffu, __fmul_rn(v.y, h_c[4]), 1);
     const float qy_hx = s_qhx[buf][w + (w <= TY ? 1 : 0)][lane];
     const float qy_hz = s_qhz[buf][w + (w <= TY ? 1 : 0)][lane];
     // and this column's own values at z+1 for the row below, next plane
-    s_qhx[buf ^ 1][w][lane] = pn_y * h_n[0];
-    s_qhz[buf ^ 1][w][lane] = r7n_x * h_n[5];
+    s_qhx[buf ^ 1][w][lane] = __fmul_rn(pn_y, h_n[0]);
+    s_qhz[buf ^ 1][w][lane] = __fmul_rn(r7n_x, h_n[5]);
 
     // ---- E part: mu, lamE', ad
     float mu[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f}, ad[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-    if (live && worker) {
-      // Db2 slots: hx_y p.z, hx_z q.y, hy_z u.x, hy_x u.w, hz_x v.z, hz_y r7.y
-      const float aEx = (u.x * h_c[2] - qz_hy) + (r7.y * h_c[5] - qy_hz);
-      const float aEy = (q.y * h_c[1] - qz_hx) + (v.z * h_c[4] - qx_hz);
-      const float aEz = (p.z * h_c[0] - qy_hx) + (u.w * h_c[3] - qx_hy);
-      if (!(fl_c & kESplit)) {
-        const float mx = lE[0] + aEx, my = lE[1] + aEy, mz = lE[2] + aEz;
-        mu[0] = mx; mu[1] = mx; mu[2] = my; mu[3] = my; mu[4] = mz; mu[5] = mz;
-        lE[0] = ra.x * mx; lE[1] = rb.x * my; lE[2] = rd.x * mz;
-      } else {
-        const float aE[3] = {aEx, aEy, aEz};
-        const float ca[6] = {ra.x, ra.z, rb.x, rb.z, rd.x, rd.z};
-#pragma unroll
-        for (int k = 0; k < 6; ++k) {
-          mu[k] = lE[k] + aE[k / 2];
-          lE[k] = ca[k] * mu[k];
-        }
-      }
-      const float cb[6] = {ra.y, ra.w, rb.y, rb.w, rd.y, rd.w};
-#pragma unroll
-      for (int k = 0; k < 6; ++k) ad[k] = cb[k] * mu[k];
-    }
+    if (live && worker)
+      adj_e_part(ra, rb, rd, p, q, u, v, r7, fl_c, h_c, qz_hx, qz_hy, qx_hy, qx_hz, qy_hx, qy_hz, lE, mu, ad);
 
     // ---- -1 neighbours' ad
     s_a0[buf][w][lane] = ad[0];
@@ -236,18 +283,8 @@ adj_step_kernel(const AdjSim* __restrict__ sims, const int4* __restrict__ tiles,
     if (own && z >= z0 && zin) {
       const float a0_m = s_a0[buf][w - 1][lane];
       const float a5_m = s_a5[buf][w - 1][lane];
-      const float aH[3] = {(a2_p - ad[2]) + (a5_m - ad[5]), (a1_p - ad[1]) + (a4_m - ad[4]),
-                           (a0_m - ad[0]) + (a3_m - ad[3])};
       float lh[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-      if (!(fl_c & kHSplit)) {
-        lh[0] = p.x * h_c[0] + aH[0];
-        lh[1] = q.z * h_c[2] + aH[1];
-        lh[2] = v.x * h_c[4] + aH[2];
-      } else {
-        const float da[6] = {p.x, p.w, q.z, u.y, v.x, v.w};
-#pragma unroll
-        for (int k = 0; k < 6; ++k) lh[k] = da[k] * h_c[k] + aH[k / 2];
-      }
+      adj_h_part(p, q, u, v, fl_c, h_c, ad, a0_m, a5_m, a3_m, a4_m, a1_p, a2_p, lh);
       // adjoints of this cell's records of step n-1 (E^n, H^n)
       const int np = int(fl_c >> 16);
       if (np && n >= 1) {
@@ -262,8 +299,8 @@ adj_step_kernel(const AdjSim* __restrict__ sims, const int4* __restrict__ tiles,
 #pragma unroll
           for (int k = 0; k < 6; ++k)
             if (sp ? (k / 2 == cc) : (k == cc)) {
-              if (is_e) lE[k] += rv;
-              else lh[k] += rv;
+              if (is_e) lE[k] = __fadd_rn(lE[k], rv);
+              else lh[k] = __fadd_rn(lh[k], rv);
             }
         }
       }
@@ -284,12 +321,7 @@ adj_step_kernel(const AdjSim* __restrict__ sims, const int4* __restrict__ tiles,
         const int64_t nb = A.nb;
         const int64_t bi = (int64_t(c - A.bx0) * bny + (r - A.by0)) * bnz + (z - A.bz0);
         const float* hs = A.hist + int64_t(n - hist_n0) * 9 * nb;
-#pragma unroll
-        for (int k = 0; k < 3; ++k) {
-          A.grad[(3 * k + 0) * nb + bi] += double(mu[2 * k]) * double(__ldg(hs + k * nb + bi));
-          A.grad[(3 * k + 1) * nb + bi] += double(mu[2 * k]) * double(__ldg(hs + (3 + 2 * k) * nb + bi));
-          A.grad[(3 * k + 2) * nb + bi] += double(mu[2 * k + 1]) * double(__ldg(hs + (4 + 2 * k) * nb + bi));
-        }
+        adj_grad_cell(A.grad, nb, bi, hs, mu);
       }
     }
     a1_p = ad[1];

@@ -28,6 +28,7 @@
 #include "fdtd_adjoint.cuh"
 #include "fdtd_nf2ff.cuh"
 #include "fdtd_step_stream.cuh"
+#include "fdtd_adjoint_stream.cuh"
 #include <cudaTypedefs.h>
 
 using namespace rfn;
@@ -861,9 +862,59 @@ struct Engine {
   DevBuf<AdjSim> adj_d_as;
   DevBuf<int4> adj_d_t;
   DevBuf<CapSim> adj_d_c;
+  DevBuf<AdjMaps> adj_d_maps;     // streaming reverse step: tensor maps of each simulation's adjoint state
+  DevBuf<int4> adj_d_ts;          // its tiles (w: the tile's boxes hold split cells)
+  DevBuf<unsigned> adj_counter;   // its tile counter
   static int adj_tiles_per_sm() {
     const char* v = std::getenv("RFN_ADJ_TILES_PER_SM");
     return v ? std::max(1, std::atoi(v)) : 4;
+  }
+  // planes per tile along z (0: picked by adj_pick_zchunk)
+  static int adj_zchunk() {
+    const char* v = std::getenv("RFN_ADJ_ZCHUNK");
+    return v ? std::max(0, std::atoi(v)) : 0;
+  }
+  // Planes per reverse-step tile along z when `slots` blocks of tx x ty tiles
+  // are resident at once: the tiles should fill whole waves of blocks (a short
+  // last wave leaves SMs idle) and load few halo planes (two per tile). Picks
+  // the largest (tiles / (waves * slots)) * (owned planes / loaded planes)
+  // over chunks of 4 planes or more that give at least two waves; 4 planes
+  // when even those give fewer.
+  // Planes per tile for the persistent reverse step on `slots` blocks: the
+  // longest even chunks (nz_max / c planes, c = 1, 2, ...) that still give
+  // at least 15/16 of the blocks a tile; 4 planes when none do.
+  int adj_pick_zchunk_persistent(int64_t slots, int tx, int ty) const {
+    int nz_max = 0;
+    for (auto* s : sims) nz_max = std::max(nz_max, s->nz);
+    for (int c = 1; c <= nz_max / 4; ++c) {
+      const int zl = (nz_max + c - 1) / c;
+      int64_t tiles = 0;
+      for (auto* s : sims) tiles += int64_t((s->nx + tx - 1) / tx) * ((s->ny + ty - 1) / ty) * ((s->nz + zl - 1) / zl);
+      if (16 * tiles >= 15 * slots) return zl;
+    }
+    return 4;
+  }
+  int adj_pick_zchunk(int64_t slots, int tx, int ty) const {
+    int nz_max = 0;
+    int64_t owned = 0;  // tile columns x planes
+    for (auto* s : sims) {
+      nz_max = std::max(nz_max, s->nz);
+      owned += int64_t((s->nx + tx - 1) / tx) * ((s->ny + ty - 1) / ty) * s->nz;
+    }
+    double best = -1.0;
+    int pick = 4;
+    for (int zl = 4; zl <= nz_max; ++zl) {
+      int64_t tiles = 0;
+      for (auto* s : sims) tiles += int64_t((s->nx + tx - 1) / tx) * ((s->ny + ty - 1) / ty) * ((s->nz + zl - 1) / zl);
+      const int64_t waves = (tiles + slots - 1) / slots;
+      if (waves < 2) break;  // the tile count only falls as the chunks grow
+      const double score = double(tiles) / double(waves * slots) * double(owned) / double(owned + 2 * tiles);
+      if (score > best + 1e-12) {
+        best = score;
+        pick = zl;
+      }
+    }
+    return pick;
   }
 
   // One simulation's part of an adjoint sweep: dJ/dX of its device DFT, the
@@ -960,12 +1011,80 @@ struct Engine {
         caps.push_back(c);
       }
     }
-    const std::vector<int4> tiles = plain_tiles(n_sm, 0, nullptr, kAdjTileX, kAdjTileY, adj_tiles_per_sm());
+    int plain_per_sm = 2;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&plain_per_sm, &adj_step_kernel<kAdjTileY, 2>,
+                                                     32 * (kAdjTileY + 2), 0));
+    const int zc = adj_zchunk() ? adj_zchunk()
+                   : std::getenv("RFN_ADJ_TILES_PER_SM")
+                       ? 0
+                       : adj_pick_zchunk(int64_t(std::max(plain_per_sm, 1)) * n_sm, kAdjTileX, kAdjTileY);
+    const std::vector<int4> tiles = plain_tiles(n_sm, zc, nullptr, kAdjTileX, kAdjTileY, adj_tiles_per_sm());
+    // The streaming reverse step, on request (RFN_ADJ_STREAM=1; the plain one
+    // is the default): tiles (split tiles first), tensor maps of each
+    // simulation's adjoint state and material index, plane slots sized for
+    // two blocks per SM.
+    using AG = AdjGeom<kAdjStreamTileY>;
+    const char* sv = std::getenv("RFN_ADJ_STREAM");
+    const bool stream_adj = sv && std::atoi(sv) != 0;
+    int n_ts = 0, adj_grid = 0, adj_slots = 0;
+    uint32_t adj_smem = 0;
+    unsigned adj_base = 0;
+    if (stream_adj) {
+      constexpr uint32_t kBudget = 233472 / 2 - 1024 - 512 - 9600;  // two blocks per SM, beside the static arrays
+      adj_slots = int(std::min<uint32_t>(kAdjStreamSlotsMax, kBudget / AG::SLOT));
+      if (adj_slots < 3) throw ArgError{FDTD_ERR_LIMIT, "Streaming reverse step's plane slots do not fit."};
+      adj_smem = uint32_t(adj_slots) * AG::SLOT;
+      const void* fn = reinterpret_cast<const void*>(&adj_stream_kernel<kAdjStreamTileY>);
+      CK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(adj_smem)));
+      int per_sm = 0;
+      CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, AG::THREADS, int(adj_smem)));
+      if (per_sm < 1) throw ArgError{FDTD_ERR_LIMIT, "Streaming reverse step does not fit on an SM."};
+      const int zcs = adj_zchunk() ? adj_zchunk()
+                      : std::getenv("RFN_ADJ_TILES_PER_SM")
+                          ? 0
+                          : adj_pick_zchunk_persistent(int64_t(per_sm) * n_sm, kAdjTileX, kAdjStreamTileY);
+      std::vector<int4> ts = plain_tiles(n_sm, zcs, nullptr, kAdjTileX, kAdjStreamTileY, adj_tiles_per_sm());
+      std::vector<GradedIndex> gis;
+      for (const auto& rq : req) gis.emplace_back(rq.s->grid, kFlagESplit | kFlagHSplit);
+      for (auto& t : ts) {
+        // the boxes of every plane of the tile: columns x0-1 .. x0+30, rows y0-1 .. y0+TY, planes z0-1 .. z1
+        const int x0 = t.y & 0xffff, y0 = int(unsigned(t.y) >> 16), z0 = t.z & 0xffff, z1 = int(unsigned(t.z) >> 16);
+        t.w = gis[size_t(t.x)].count(x0 - 1, x0 + kAdjTileX + 1, y0 - 1, y0 + kAdjStreamTileY + 1, z0 - 1, z1 + 1) > 0;
+      }
+      std::stable_sort(ts.begin(), ts.end(), [](const int4& a, const int4& b) { return a.w > b.w; });
+      n_ts = int(ts.size());
+      std::vector<AdjMaps> hm(req.size());
+      for (size_t i = 0; i < req.size(); ++i) {
+        fdtd_sim* s = req[i].s;
+        const size_t N = s->cells_padded;
+        std::memset(&hm[i], 0, sizeof(AdjMaps));
+        const auto F = CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
+        float* lam = adj_bufs[i]->lam.p;
+        encode_map(&hm[i].lam_e, lam, F, 4, s, 5, AG::EW, AG::ER, 3, N, 6 * N);
+        encode_map(&hm[i].lam_h, lam + 3 * N, F, 4, s, 5, AG::HW, AG::HR, 3, N, 6 * N);
+        if (s->splits.n) encode_map(&hm[i].halves, adj_bufs[i]->lams.p, F, 4, s, 5, AG::SW, AG::HR, 12, N, 12 * N);
+        encode_map(&hm[i].ids, s->mat.p, CU_TENSOR_MAP_DATA_TYPE_UINT16, 2, s, 3, AG::IW, AG::HR, 1, 0, 0);
+      }
+      adj_d_maps.reserve(hm.size());
+      CK(cudaMemcpy(adj_d_maps.p, hm.data(), hm.size() * sizeof(AdjMaps), cudaMemcpyHostToDevice));
+      adj_d_ts.reserve(ts.size());
+      CK(cudaMemcpy(adj_d_ts.p, ts.data(), ts.size() * sizeof(int4), cudaMemcpyHostToDevice));
+      adj_grid = int(std::min<int64_t>(n_ts, int64_t(per_sm) * n_sm));
+      adj_counter.reserve(1);
+      CK(cudaMemsetAsync(adj_counter.p, 0, sizeof(unsigned), st));
+    }
     auto reverse_step = [&](int n, int hist_n0) {
-      // register cap: two resident blocks per SM (default) or three
-      const char* mb = std::getenv("RFN_ADJ_MINB");
-      auto adj_fn = (mb && std::atoi(mb) == 3) ? &adj_step_kernel<kAdjTileY, 3> : &adj_step_kernel<kAdjTileY, 2>;
-      adj_fn<<<int(tiles.size()), dim3(32, kAdjTileY + 2), 0, st>>>(adj_d_as.p, adj_d_t.p, n, hist_n0);
+      if (stream_adj) {
+        adj_stream_kernel<kAdjStreamTileY><<<adj_grid, AG::THREADS, adj_smem, st>>>(
+            adj_d_as.p, adj_d_maps.p, adj_d_ts.p, n_ts, n, hist_n0, adj_counter.p, adj_base, d_err.p, adj_slots,
+            wait_limit);
+        adj_base += unsigned(n_ts + adj_grid);
+      } else {
+        // register cap: two resident blocks per SM (default) or three
+        const char* mb = std::getenv("RFN_ADJ_MINB");
+        auto adj_fn = (mb && std::atoi(mb) == 3) ? &adj_step_kernel<kAdjTileY, 3> : &adj_step_kernel<kAdjTileY, 2>;
+        adj_fn<<<int(tiles.size()), dim3(32, kAdjTileY + 2), 0, st>>>(adj_d_as.p, adj_d_t.p, n, hist_n0);
+      }
       CK(cudaGetLastError());
       ++adj_launches;
     };
@@ -2085,15 +2204,64 @@ int fdtd_batch_run_recorded(fdtd_batch* b, int nt, const int* boxes) {
   });
 }
 
+int fdtd_batch_run_checkpointed(fdtd_batch* b, int nt, int every, const int* boxes) {
+  if (!b) return FDTD_ERR_ARG;
+  return guarded(&b->err, [&] {
+    if (nt < 1 || every < 1 || !boxes)
+      throw ArgError{FDTD_ERR_ARG, "nt and the checkpoint interval must be positive and the boxes given."};
+    bool rebuild = b->engine.graph_nt != nt || b->engine.n_tiles == 0 || b->dirty;
+    b->dirty = false;
+    const size_t nseg = size_t((nt + every - 1) / every);
+    for (size_t i = 0; i < b->sims.size(); ++i) {
+      fdtd_sim* s = b->sims[i];
+      const int* box = boxes + 6 * i;
+      if (!s->prepared || s->prepared_nt != nt) rebuild = true;
+      try {
+        prepare(s, nt);
+        check_gradient_box(s, box);
+      } catch (ArgError& a) {
+        a.msg = "batch member " + std::to_string(i) + ": " + a.msg;
+        throw;
+      }
+      if (s->adj_mode != 1 || !s->adj_in_batch || s->ckpt_nt != nt || s->ckpt_every != every ||
+          !std::equal(box, box + 6, s->adj_box)) {
+        leave_adjoint_mode(s);
+        const size_t stride = 6 * s->cells_padded + (s->splits.n ? 2 * s->split_buf_pairs : 0);
+        s->ckpt.alloc(nseg * stride);
+        s->adj_mode = 1;
+        s->adj_in_batch = true;
+        s->ckpt_every = every;
+        s->ckpt_nt = nt;
+        std::copy(box, box + 6, s->adj_box);
+        rebuild = true;
+      }
+    }
+    if (batch_moved(b)) rebuild = true;
+    if (rebuild) {
+      b->engine.graph_nt = -1;
+      b->engine.build_tiles();
+      note_generations(b);
+    }
+    b->engine.run_async(nt);
+    b->engine.sync();
+    for (auto* s : b->sims) fill_stats(s, &b->engine);
+    b->stats.nt = nt;
+    b->stats.last_run_ms = b->engine.last_ms;
+    b->stats.step_launches = b->engine.step_launches;
+  });
+}
+
 int fdtd_batch_adjoint(fdtd_batch* b, const double* const* dJ_dX, double* const* grad) {
   if (!b) return FDTD_ERR_ARG;
   return guarded(&b->err, [&] {
     if (!dJ_dX || !grad) throw ArgError{FDTD_ERR_ARG, "null argument"};
     std::vector<Engine::AdjRequest> req;
+    const int mode = b->sims.empty() ? 0 : b->sims[0]->adj_mode;
     for (size_t i = 0; i < b->sims.size(); ++i) {
       fdtd_sim* s = b->sims[i];
-      if (s->adj_mode != 2 || !s->adj_in_batch || b->engine.graph_nt != s->ckpt_nt)
-        throw ArgError{FDTD_ERR_STATE, "fdtd_batch_adjoint needs a preceding fdtd_batch_run_recorded."};
+      if (s->adj_mode == 0 || s->adj_mode != mode || !s->adj_in_batch || b->engine.graph_nt != s->ckpt_nt)
+        throw ArgError{FDTD_ERR_STATE,
+                       "fdtd_batch_adjoint needs a preceding fdtd_batch_run_recorded or fdtd_batch_run_checkpointed."};
       if (s->n_series < 1 || s->n_freq < 1) throw ArgError{FDTD_ERR_STATE, "batch member without a DFT."};
       if (!dJ_dX[i] || !grad[i]) throw ArgError{FDTD_ERR_ARG, "null member array"};
       req.push_back(Engine::AdjRequest{s, dJ_dX[i], s->adj_box, grad[i]});

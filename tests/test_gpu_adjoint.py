@@ -156,3 +156,63 @@ def test_gpu_box_patch_runs_equal_full_arrays(engine_lib):
         ref.close()
     sim.close()
 
+
+
+@pytest.mark.parametrize("every,graded", [(0, False), (40, False), (0, True)])
+def test_gpu_stream_adjoint_equals_plain_adjoint(engine_lib, every, graded, monkeypatch):
+    """The streaming reverse step (RFN_ADJ_STREAM=1, after streaming forward
+    runs) gives the plain reverse step's gradient (after plain forward runs)
+    bit for bit: same per-cell arithmetic with fixed rounding, on a model of
+    several tiles along x, y and z with split tiles, plain tiles and records
+    at split cells."""
+    s = configs.microstrip(n=(70, 44, 37), n_pml=5, nt=160, graded=graded)
+    box = (30, 42, 18, 26, 5, 9)
+    # output E probes, H probes around the strip, source (split E) cells
+    terms = ([(0, p, 1.0) for p in (20, 21, 22, 23)] + [(1, p, (-1.0) ** p) for p in range(40, 48)]
+             + [(2, p, -1.0) for p in (0, 1, 2, 3)])
+    out = {}
+    for variant in (0, 1):
+        monkeypatch.setenv("RFN_ADJ_STREAM", str(variant))
+        sim, _, nt, _ = _sim(s, variant, every, terms, box)
+        X = sim.dft()
+        g = sim.adjoint(2 * X, box)
+        assert sim.stats()["adjoint_launches"] == nt
+        sim.close()
+        out[variant] = (X, g)
+    assert np.array_equal(out[0][0], out[1][0])
+    assert np.abs(out[0][1]).max() > 0
+    assert np.array_equal(out[0][1], out[1][1])
+
+
+def test_gpu_batch_checkpointed_adjoint_equals_recorded(engine_lib):
+    """fdtd_batch_run_checkpointed + fdtd_batch_adjoint (the segments of all
+    members replayed together) give the gradients of the recorded batch and
+    of single checkpointed runs bit for bit: the replay repeats the forward
+    arithmetic exactly."""
+    models = [configs.microstrip(n=(18, 16, 14), n_pml=3, nt=400),
+              configs.microstrip(n=(23, 19, 15), n_pml=3, nt=400)]
+    boxes = [BOX, (9, 13, 7, 10, 4, 6)]
+    single = []
+    for s, box in zip(models, boxes):
+        sim, _, _, _ = _sim(s, 1, 50, TERMS, box)
+        X = sim.dft()
+        single.append((X, sim.adjoint(2 * X, box)))
+        sim.close()
+    sims = [_make(s, 1, TERMS)[0] for s in models]
+    b = _lib.Batch(sims)
+    out = {}
+    for mode in ("checkpointed", "recorded"):
+        if mode == "checkpointed":
+            b.run_checkpointed(400, 50, boxes)
+        else:
+            b.run_recorded(400, boxes)
+        Xs = [sim.dft() for sim in sims]
+        out[mode] = (Xs, b.adjoint([2 * X for X in Xs]))
+        assert b.stats()["adjoint_launches"] == 400
+    b.close()
+    for sim in sims:
+        sim.close()
+    for i, (X1, g1) in enumerate(single):
+        for mode in ("checkpointed", "recorded"):
+            assert np.array_equal(out[mode][0][i], X1)
+            assert np.array_equal(out[mode][1][i], g1)
