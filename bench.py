@@ -318,6 +318,9 @@ def run_ours(args, rank, world, local_rank):
             "config": bench_config(Nt, world, len(names), len(pr)),
             "step": f"one full simulation ({Nt} Yee time steps)",
             "kernel": {k: st[k] for k in ("variant", "tile_y", "stages", "zchunk", "grid", "n_tiles")},
+            "autotune": {"ms": round(st["tune_ms"], 1), "trials": st["tune_trials"],
+                         "when": "once per set of grid sizes per process, inside its first run (a warm-up run "
+                                 "here); later runs take the cached shape"},
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s",
                          "frac": round(achieved / hbm, 4), "traffic": traffic,
                          "peak_source": peak_kind,
@@ -513,7 +516,8 @@ def workloads_entry(args, local_rank):
                                       "sequential_reference_cuda", "batched_over_sequential_reference_cuda",
                                       "mcell_updates_per_s", "bit_identical_to_sequential", "gpu_launches")),
             ("adjoint", run_adjoint, dict(steps=3), ("value", "unit", "ms_per_step", "forward_s", "gradient_over_forward",
-                                          "device", "recorded_history", "gpu_launches")),
+                                          "device", "recorded_history", "checkpoints_every_32",
+                                          "gradients_bit_identical_across_modes", "gpu_launches")),
             ("design", run_design, {}, ("value", "unit", "ms_per_step", "device", "recorded_history",
                                         "sequential", "batched_over_sequential", "gpu_launches"))):
         t0 = time.perf_counter()
@@ -784,10 +788,13 @@ def run_adjoint(args, rank, world, local_rank):
                        "gradient_over_forward": round(dev_grad / dev_plain, 3),
                        "adjoint_launches": st["adjoint_launches"]},
             "gpu_launches": int(st["step_launches"] + st["adjoint_launches"]),
+            "grad": g.detach().clone(),
         }
 
     ck = measure(FDTDDesign(s, box, [(0, len(pr) - 1, 1.0)], omega, checkpoint_every=64))
+    ck32 = measure(FDTDDesign(s, box, [(0, len(pr) - 1, 1.0)], omega, checkpoint_every=32))
     rec = measure(FDTDDesign(s, box, [(0, len(pr) - 1, 1.0)], omega))
+    same = bool(torch.equal(ck.pop("grad"), rec["grad"]) and torch.equal(ck32.pop("grad"), rec.pop("grad")))
     ranks.close()
     if rank != 0:
         return None
@@ -803,6 +810,10 @@ def run_adjoint(args, rank, world, local_rank):
         "J": ck["J"], "gpu_launches": ck["gpu_launches"],
         "recorded_history": {k: rec[k] for k in ("value", "ms_per_step", "forward_s", "gradient_over_forward",
                                                    "device", "J")},
+        "checkpoints_every_32": {k: ck32[k] for k in ("value", "ms_per_step", "gradient_over_forward", "device")},
+        "replay": "each replayed step runs the tiles within reach of the design box (the steps left in its "
+                  "segment, in cells)",
+        "gradients_bit_identical_across_modes": same,
     }
 
 

@@ -69,6 +69,9 @@ typedef struct fdtd_stats {
   int64_t slab_cells;    /* cells inside those slabs */
   int64_t sparse_split_cells; /* split cells outside them (soft-source cells) */
   int64_t split_bytes;   /* device bytes of the split-pair storage (both time buffers) */
+  double tune_ms;        /* host time the step-kernel autotuner spent timing candidate shapes when this
+                          * engine was last tiled (0 when the choice came from its process-wide cache) */
+  int tune_trials;       /* candidate shapes it timed */
 } fdtd_stats;
 
 /* --------------------------------------------------------------- one grid */
@@ -274,8 +277,17 @@ typedef struct fdtd_nf2ff_face {
 int fdtd_nf2ff(const fdtd_nf2ff_face* faces, int n_faces, int n_freq, const float* beta, int n_theta,
                const float* theta, int n_phi, const float* phi, float* out);
 
+/* The engine keeps the device memory of destroyed simulations in a pool of
+ * its own per device, so the next solve of a similar size maps nothing new.
+ * This returns the pool's unused memory on the current device to the driver,
+ * down to keep_bytes of unused reserve, and reports the pool's reserved and
+ * in-use bytes afterwards (either pointer may be null). Synchronises the
+ * device first. No reference counterpart: the reference allocates and frees
+ * per solve (rfnetwork/core/src/solver.cu:560-760, 1100-1140). */
+int fdtd_trim_memory(int64_t keep_bytes, int64_t* reserved, int64_t* used);
+
 /* Last error of calls that have no handle (fdtd_create, fdtd_batch_create,
- * fdtd_step_noalloc, fdtd_nf2ff), kept per calling thread. */
+ * fdtd_step_noalloc, fdtd_nf2ff, fdtd_trim_memory), kept per calling thread. */
 const char* fdtd_global_error(void);
 
 /* ------------------------------------------------ caller-owned buffers */

@@ -25,6 +25,7 @@ EXPORTED = (
     "fdtd_batch_last_error", "fdtd_batch_destroy", "fdtd_global_error", "fdtd_step_noalloc",
     "fdtd_run_checkpointed", "fdtd_run_recorded", "fdtd_adjoint", "fdtd_batch_run_recorded",
     "fdtd_batch_run_checkpointed", "fdtd_batch_adjoint", "fdtd_set_graph", "fdtd_set_box_coefficients", "fdtd_nf2ff", "fdtd_set_debug",
+    "fdtd_trim_memory",
 )
 
 
@@ -45,7 +46,7 @@ class FdtdStats(ctypes.Structure):
         ("grid", ctypes.c_int), ("h2d_bytes", ctypes.c_int64), ("d2h_bytes", ctypes.c_int64),
         ("adjoint_launches", ctypes.c_int64), ("adjoint_ms", ctypes.c_double),
         ("split_slab", ctypes.c_int * 6), ("slab_cells", ctypes.c_int64), ("sparse_split_cells", ctypes.c_int64),
-        ("split_bytes", ctypes.c_int64),
+        ("split_bytes", ctypes.c_int64), ("tune_ms", ctypes.c_double), ("tune_trials", ctypes.c_int),
     ]
 
     def as_dict(self):
@@ -99,6 +100,7 @@ def load():
         "fdtd_batch_last_error": ([vp], ctypes.c_char_p),
         "fdtd_batch_destroy": ([vp], None),
         "fdtd_global_error": ([], ctypes.c_char_p),
+        "fdtd_trim_memory": ([i64, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64)], ip),
         "fdtd_run_checkpointed": ([vp, ip, ip], ip),
         "fdtd_run_recorded": ([vp, ip, vp], ip),
         "fdtd_adjoint": ([vp, vp, ip, ip, vp, vp], ip),
@@ -449,3 +451,15 @@ def nf2ff(J_xyz, M_xyz, r_grid, ds_grid, surf_pos, ff_data) -> int:
     if rc:
         raise FdtdError(f"{FDTD_ERRORS.get(rc, rc)}: {lib.fdtd_global_error().decode()}")
     return 0
+
+
+def trim_memory(keep_bytes: int = 0) -> dict:
+    """Return the engine's unused pooled device memory (current device) to the
+    driver, keeping at most ``keep_bytes`` of unused reserve; returns the pool's
+    reserved and in-use bytes afterwards."""
+    lib = load()
+    reserved, used = ctypes.c_int64(0), ctypes.c_int64(0)
+    rc = lib.fdtd_trim_memory(int(keep_bytes), ctypes.byref(reserved), ctypes.byref(used))
+    if rc:
+        raise FdtdError(f"{FDTD_ERRORS.get(rc, rc)}: {lib.fdtd_global_error().decode()}")
+    return {"reserved": reserved.value, "used": used.value}

@@ -10,6 +10,7 @@
 
 #include <algorithm>
 #include <array>
+#include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -452,6 +453,8 @@ struct Engine {
   int withhold = -1;                       // test hook: plane the TMA kernels' producers never issue
   bool use_graph = true;  // replay the time loop as a captured CUDA graph
   double last_ms = 0;
+  double tune_ms = 0;      // host time of the autotuner's trial runs in the last tiling (0: cached choice)
+  int tune_trials = 0;     // candidate shapes it timed
   bool timing_pending = false;
 
   cudaStream_t stream() const { return ext_stream ? ext_stream : own_stream; }
@@ -559,6 +562,8 @@ struct Engine {
   // themselves (their fields are cleared again by the next run), the fastest
   // is kept and remembered for the same grid sizes.
   void autotune(int n_sm) {
+    tune_ms = 0;
+    tune_trials = 0;
     std::vector<int> key;
     int nt_min = 1 << 30;
     for (auto* s : sims) {
@@ -584,6 +589,7 @@ struct Engine {
     std::array<int, 4> best = {kTuneCandidates[0][0], kTuneCandidates[0][1], kTuneCandidates[0][2],
                                kTuneCandidates[0][3]};
     if (timed >= 2) {
+      const auto t0 = std::chrono::steady_clock::now();
       init();
       cudaStream_t st = stream();
       float best_ms = 1e30f;
@@ -603,12 +609,14 @@ struct Engine {
         CK(cudaStreamSynchronize(st));
         float ms = 0;
         CK(cudaEventElapsedTime(&ms, ev0, ev1));
+        ++tune_trials;
         if (ms < best_ms) {
           best_ms = ms;
           best = {cand[0], cand[1], cand[2], cand[3]};
         }
       }
       check_error();
+      tune_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
     }
     {
       std::lock_guard<std::mutex> lock(g_tune_mutex);
@@ -826,6 +834,61 @@ struct Engine {
     }
   }
 
+  // Orders the streaming kernels' tile lists for segment replays by the
+  // Chebyshev distance (cells) of each tile's owned cells from the gradient
+  // box of its simulation (boxes[i] for sims[i]; null: never needed).
+  void build_replay_tiles(const std::vector<const int*>& boxes) {
+    StreamClass& c = scls;
+    auto order = [&](const std::vector<StreamTile>& src, DevBuf<StreamTile>& dst, std::vector<int>& dist) {
+      std::vector<std::pair<int, StreamTile>> v;
+      v.reserve(src.size());
+      for (const auto& t : src) {
+        const fdtd_sim* s = sims[size_t(t.sim)];
+        const int* b = boxes[size_t(t.sim)];
+        if (!b) continue;
+        auto gap = [](int a0, int a1, int b0, int b1) { return std::max(0, std::max(a0 - (b1 - 1), b0 - (a1 - 1))); };
+        const int x1 = std::min(s->nx, t.x0 + kStreamOwnX), y1 = std::min(s->ny, t.y0 + c.v->ty);
+        const int d = std::max(gap(t.x0, x1, b[0], b[1]), std::max(gap(t.y0, y1, b[2], b[3]), gap(t.z0, t.z1, b[4], b[5])));
+        v.emplace_back(d, t);
+      }
+      std::stable_sort(v.begin(), v.end(), [](const auto& a, const auto& b) { return a.first < b.first; });
+      dist.resize(v.size());
+      std::vector<StreamTile> h(v.size());
+      for (size_t i = 0; i < v.size(); ++i) {
+        dist[i] = v[i].first;
+        h[i] = v[i].second;
+      }
+      dst.reserve(std::max<size_t>(1, h.size()));
+      if (!h.empty()) CK(cudaMemcpy(dst.p, h.data(), h.size() * sizeof(StreamTile), cudaMemcpyHostToDevice));
+    };
+    order(c.host_tiles, rep_tiles, rep_dist);
+    order(c.host_tiles_p, rep_tiles_p, rep_dist_p);
+  }
+
+  // Step n of a segment replay restricted to the tiles within `reach` cells of
+  // the gradient boxes (lists from build_replay_tiles), the general kernel
+  // then the plain-tile kernel on st, at most `cap` blocks each; base_g /
+  // base_p carry the tile counters' bases from step to step of the segment.
+  void launch_replay_subset(cudaStream_t st, int n, int reach, int cap, unsigned& base_g, unsigned& base_p) {
+    StreamClass& c = scls;
+    const int ng = int(std::upper_bound(rep_dist.begin(), rep_dist.end(), reach) - rep_dist.begin());
+    const int np = int(std::upper_bound(rep_dist_p.begin(), rep_dist_p.end(), reach) - rep_dist_p.begin());
+    if (ng > 0) {
+      const int g = std::min(std::min(c.grid, cap), ng);
+      c.v->fn<<<g, c.v->threads, c.ring, st>>>(c.d_sims.p, rep_tiles.p, ng, n, c.d_counter.p, base_g, d_err.p,
+                                                  c.n_main, c.n_reg, wait_limit, withhold);
+      CK(cudaGetLastError());
+      base_g += unsigned(ng + g);
+    }
+    if (np > 0) {
+      const int g = std::min(std::min(c.grid_p, cap), np);
+      c.v->fn_plain<<<g, c.v->threads, c.ring_p, st>>>(c.d_sims.p, rep_tiles_p.p, np, n, c.d_counter.p + 1, base_p,
+                                                        d_err.p, c.n_main_p, 0, wait_limit, withhold);
+      CK(cudaGetLastError());
+      base_p += unsigned(np + g);
+    }
+  }
+
   // Box-history capture of the simulations in recorded mode (adj_mode 2):
   // one adj_capture_kernel launch per time step, before the step, inside the
   // captured time loop.
@@ -855,9 +918,15 @@ struct Engine {
   // Adjoint work buffers of each request slot, kept between sweeps.
   struct AdjBufs {
     DevBuf<float> lam, lams, radj, seg;
+    DevBuf<float> rec_save;  // the forward's probe records, kept while segment replays rewrite them
     DevBuf<int> pidx, pfld;
     DevBuf<double> grad;
   };
+  // Segment replays of a checkpointed adjoint (streaming kernels): the general
+  // and plain tile lists ordered by each tile's distance from its simulation's
+  // gradient box, nearest first, with those distances (cells).
+  DevBuf<StreamTile> rep_tiles, rep_tiles_p;
+  std::vector<int> rep_dist, rep_dist_p;
   std::vector<std::unique_ptr<AdjBufs>> adj_bufs;
   DevBuf<AdjSim> adj_d_as;
   DevBuf<int4> adj_d_t;
@@ -1114,6 +1183,29 @@ struct Engine {
       const char* rb = std::getenv("RFN_REPLAY_BLOCKS_PER_SM");
       const int per_sm = rb ? std::max(1, std::atoi(rb)) : 1;
       cudaStream_t rs = rep_stream;
+      // The history of step n is the state before step n, so a segment
+      // [n0, n1) replays steps n0 .. n1-2 only. The history reads the box and
+      // the H values one cell beyond it (the +1 neighbours of the E update's
+      // differences), and a step moves information by at most one cell along
+      // each axis, so step n needs to be right only within n1-1-n cells of the
+      // box: with the streaming kernels each replay step runs the tiles within
+      // that reach (nearest first). Tiles outside it keep stale values, which
+      // never reach what the history reads before the segment ends.
+      const bool cone = cfg.variant == 1 && !std::getenv("RFN_REPLAY_FULL");
+      if (cone) {
+        std::vector<const int*> boxes(sims.size(), nullptr);
+        for (const auto& r : req)
+          for (size_t i = 0; i < sims.size(); ++i)
+            if (sims[i] == r.s) boxes[i] = r.box;
+        build_replay_tiles(boxes);
+      }
+      // the replays rewrite probe records (outside the reach, with stale
+      // values): the forward's records are kept aside and put back at the end
+      for (size_t i = 0; i < req.size(); ++i) {
+        fdtd_sim* s = req[i].s;
+        adj_bufs[i]->rec_save.reserve(s->rec.n);
+        CK(cudaMemcpyAsync(adj_bufs[i]->rec_save.p, s->rec.p, s->rec.n * sizeof(float), cudaMemcpyDeviceToDevice, st));
+      }
       // segment k replayed on rs from its snapshot into history half k & 1,
       // each step's box capture beside it (as in a recorded run)
       auto replay = [&](int k) {
@@ -1130,13 +1222,19 @@ struct Engine {
             CK(cudaMemcpyAsync(s->splits.p + b * sb, src + 6 * N, sb * sizeof(float), cudaMemcpyDeviceToDevice, rs));
         }
         if (cfg.variant == 1) CK(cudaMemsetAsync(scls.d_counter.p, 0, scls.d_counter.n * sizeof(unsigned), rs));
+        unsigned base_g = 0, base_p = 0;
         for (int n = n0; n < n1; ++n) {
           CK(cudaEventRecord(cap_fork, rs));
           CK(cudaStreamWaitEvent(cap_stream, cap_fork, 0));
           adj_capture_kernel<<<dim3(cap_grid, unsigned(caps.size())), 256, 0, cap_stream>>>(d_c.p, n, h0);
           CK(cudaGetLastError());
           CK(cudaEventRecord(cap_join, cap_stream));
-          launch_replay_step(rs, n, n0, n_sm, per_sm);
+          if (n + 1 < n1) {
+            if (cone)
+              launch_replay_subset(rs, n, n1 - 1 - n, n_sm * per_sm, base_g, base_p);
+            else
+              launch_replay_step(rs, n, n0, n_sm, per_sm);
+          }
           CK(cudaStreamWaitEvent(rs, cap_join, 0));
         }
         CK(cudaEventRecord(seg_done[k & 1], rs));
@@ -1154,6 +1252,10 @@ struct Engine {
         CK(cudaStreamWaitEvent(st, seg_done[k & 1], 0));
         for (int n = n1 - 1; n >= n0; --n) reverse_step(n, n0 - (k & 1) * K);
         CK(cudaEventRecord(seg_free[k & 1], st));
+      }
+      for (size_t i = 0; i < req.size(); ++i) {
+        fdtd_sim* s = req[i].s;
+        CK(cudaMemcpyAsync(s->rec.p, adj_bufs[i]->rec_save.p, s->rec.n * sizeof(float), cudaMemcpyDeviceToDevice, st));
       }
     }
     CK(cudaEventRecord(ev1, st));
@@ -1487,6 +1589,8 @@ void fill_stats(fdtd_sim* s, const Engine* e) {
     st.step_launches = e->step_launches;
     st.dft_launches = e->dft_launches;
     st.last_run_ms = e->last_ms;
+    st.tune_ms = e->tune_ms;
+    st.tune_trials = e->tune_trials;
   }
 }
 
@@ -2152,6 +2256,8 @@ int fdtd_batch_run(fdtd_batch* b, int nt) {
     st.step_launches = b->engine.step_launches;
     st.dft_launches = b->engine.dft_launches;
     st.last_run_ms = b->engine.last_ms;
+    st.tune_ms = b->engine.tune_ms;
+    st.tune_trials = b->engine.tune_trials;
     for (auto* s : b->sims) {
       st.e_split_cells += s->grid.e_split_cells;
       st.h_split_cells += s->grid.h_split_cells;
@@ -2201,6 +2307,8 @@ int fdtd_batch_run_recorded(fdtd_batch* b, int nt, const int* boxes) {
     b->stats.nt = nt;
     b->stats.last_run_ms = b->engine.last_ms;
     b->stats.step_launches = b->engine.step_launches;
+    b->stats.tune_ms = b->engine.tune_ms;
+    b->stats.tune_trials = b->engine.tune_trials;
   });
 }
 
@@ -2248,6 +2356,8 @@ int fdtd_batch_run_checkpointed(fdtd_batch* b, int nt, int every, const int* box
     b->stats.nt = nt;
     b->stats.last_run_ms = b->engine.last_ms;
     b->stats.step_launches = b->engine.step_launches;
+    b->stats.tune_ms = b->engine.tune_ms;
+    b->stats.tune_trials = b->engine.tune_trials;
   });
 }
 
@@ -2287,6 +2397,21 @@ void fdtd_batch_destroy(fdtd_batch* b) {
 }
 
 const char* fdtd_global_error(void) { return g_error.c_str(); }
+
+int fdtd_trim_memory(int64_t keep_bytes, int64_t* reserved, int64_t* used) {
+  return guarded(&g_error, [&] {
+    if (keep_bytes < 0) throw ArgError{FDTD_ERR_ARG, "fdtd_trim_memory: keep_bytes must be >= 0"};
+    cudaMemPool_t pool = engine_pool();
+    // blocks freed by destroyed simulations are returned once every stream is past their last use
+    CK(cudaDeviceSynchronize());
+    CK(cudaMemPoolTrimTo(pool, size_t(keep_bytes)));
+    uint64_t r = 0, u = 0;
+    CK(cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &r));
+    CK(cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent, &u));
+    if (reserved) *reserved = int64_t(r);
+    if (used) *used = int64_t(u);
+  });
+}
 
 int fdtd_nf2ff(const fdtd_nf2ff_face* faces, int n_faces, int n_freq, const float* beta, int n_theta,
                const float* theta, int n_phi, const float* phi, float* out) {

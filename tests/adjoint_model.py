@@ -78,49 +78,67 @@ def _gterms(C, E):
             C[29] * ex - C[28] * bwd(ex, 1)]   # hz_y
 
 
-def forward(model, probes, src, nt, box=None):
+def step(model, probes, src, n, state):
+    """One time step n of the engine's update: state = (E, H, Es, Hs) lists of
+    arrays (3, 3, 6, 6) before the step; returns the state after it."""
+    C, es, hs = model.coef, model.es, model.hs
+    E, H, Es, Hs = state
+    d = _diffs(H)
+    newE, newEs = [], []
+    for c in range(3):
+        newE.append(C[4 * c] * E[c] + C[4 * c + 1] * d[c][0] + C[4 * c + 3] * d[c][1])
+        newEs.append(C[4 * c] * Es[2 * c] + C[4 * c + 1] * d[c][0])
+        newEs.append(C[4 * c + 2] * Es[2 * c + 1] + C[4 * c + 3] * d[c][1])
+    for i, (fld, x, y, z, is_src) in enumerate(probes):
+        if is_src and fld < 3:
+            newEs[2 * fld][x, y, z] += src[i, n]
+            newEs[2 * fld + 1][x, y, z] += src[i, n]
+    E = [np.where(es, newEs[2 * c] + newEs[2 * c + 1], newE[c]) for c in range(3)]
+    Es = [np.where(es, v, 0.0) for v in newEs]
+    g = _gterms(C, E)
+    da = [C[12], C[15], C[18], C[21], C[24], C[27]]
+    newH = [da[2 * c] * H[c] + g[2 * c] + g[2 * c + 1] for c in range(3)]
+    newHs = [da[s] * Hs[s] + g[s] for s in range(6)]
+    for i, (fld, x, y, z, is_src) in enumerate(probes):
+        if is_src and fld >= 3:
+            c = fld - 3
+            newHs[2 * c][x, y, z] += src[i, n]
+            newHs[2 * c + 1][x, y, z] += src[i, n]
+    H = [np.where(hs, newHs[2 * c] + newHs[2 * c + 1], newH[c]) for c in range(3)]
+    Hs = [np.where(hs, v, 0.0) for v in newHs]
+    return E, H, Es, Hs
+
+
+def box_history(state, box):
+    """E^n and the H differences (dA, dB) on the box, from the state before step n."""
+    E, H = state[0], state[1]
+    d = _diffs(H)
+    sl = (slice(box[0], box[1]), slice(box[2], box[3]), slice(box[4], box[5]))
+    return (np.array([E[c][sl] for c in range(3)]),
+            np.array([[d[c][0][sl], d[c][1][sl]] for c in range(3)]))
+
+
+def zero_state(shape):
+    return ([np.zeros(shape) for _ in range(3)], [np.zeros(shape) for _ in range(3)],
+            [np.zeros(shape) for _ in range(6)], [np.zeros(shape) for _ in range(6)])
+
+
+def forward(model, probes, src, nt, box=None, states=None):
     """probes: (field, x, y, z, is_source) after the Yee shift; src: [P, nt].
 
     Returns rec [P, nt] and, with box = (x0, x1, y0, y1, z0, z1), the history
-    of E^n and of the H differences (dA, dB) on the box for every step."""
-    C, es, hs = model.coef, model.es, model.hs
-    shp = model.shape
-    E = [np.zeros(shp) for _ in range(3)]
-    H = [np.zeros(shp) for _ in range(3)]
-    Es = [np.zeros(shp) for _ in range(6)]
-    Hs = [np.zeros(shp) for _ in range(6)]
+    of E^n and of the H differences (dA, dB) on the box for every step. With
+    a dict `states`, the state before each step n in it is stored there."""
+    state = zero_state(model.shape)
     rec = np.zeros((len(probes), nt))
     hist = [] if box is not None else None
     for n in range(nt):
-        d = _diffs(H)
+        if states is not None and n in states:
+            states[n] = state
         if hist is not None:
-            sl = (slice(box[0], box[1]), slice(box[2], box[3]), slice(box[4], box[5]))
-            hist.append((np.array([E[c][sl] for c in range(3)]),
-                         np.array([[d[c][0][sl], d[c][1][sl]] for c in range(3)])))
-        newE, newEs = [], []
-        for c in range(3):
-            newE.append(C[4 * c] * E[c] + C[4 * c + 1] * d[c][0] + C[4 * c + 3] * d[c][1])
-            newEs.append(C[4 * c] * Es[2 * c] + C[4 * c + 1] * d[c][0])
-            newEs.append(C[4 * c + 2] * Es[2 * c + 1] + C[4 * c + 3] * d[c][1])
-        for i, (fld, x, y, z, is_src) in enumerate(probes):
-            if is_src and fld < 3:
-                newEs[2 * fld][x, y, z] += src[i, n]
-                newEs[2 * fld + 1][x, y, z] += src[i, n]
-        for c in range(3):
-            E[c] = np.where(es, newEs[2 * c] + newEs[2 * c + 1], newE[c])
-        Es = [np.where(es, v, 0.0) for v in newEs]
-        g = _gterms(C, E)
-        da = [C[12], C[15], C[18], C[21], C[24], C[27]]
-        newH = [da[2 * c] * H[c] + g[2 * c] + g[2 * c + 1] for c in range(3)]
-        newHs = [da[s] * Hs[s] + g[s] for s in range(6)]
-        for i, (fld, x, y, z, is_src) in enumerate(probes):
-            if is_src and fld >= 3:
-                c = fld - 3
-                newHs[2 * c][x, y, z] += src[i, n]
-                newHs[2 * c + 1][x, y, z] += src[i, n]
-        for c in range(3):
-            H[c] = np.where(hs, newHs[2 * c] + newHs[2 * c + 1], newH[c])
-        Hs = [np.where(hs, v, 0.0) for v in newHs]
+            hist.append(box_history(state, box))
+        state = step(model, probes, src, n, state)
+        E, H = state[0], state[1]
         for i, (fld, x, y, z, _) in enumerate(probes):
             rec[i, n] = (E + H)[fld][x, y, z]
     return rec, hist

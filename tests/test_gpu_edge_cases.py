@@ -137,3 +137,43 @@ def test_slab_stores_stream_equals_plain(engine_lib, shape):
         got = sim.probe_values()
         sim.close()
         assert np.array_equal(got, ref), kernel
+
+
+def test_autotuner_cost_in_stats(engine_lib):
+    # a grid size no other test uses, so the first engine tunes and the second
+    # takes the cached shape
+    shape = (45, 23, 19)
+    first = _random_sim(shape, 5, 12, 1, tile_y=0)
+    first.run(12)
+    st = first.stats()
+    ref = first.probe_values()
+    first.close()
+    assert st["tune_trials"] >= 2 and st["tune_ms"] > 0.0
+    second = _random_sim(shape, 5, 12, 1, tile_y=0)
+    second.run(12)
+    st2 = second.stats()
+    got = second.probe_values()
+    second.close()
+    assert st2["tune_trials"] == 0 and st2["tune_ms"] == 0.0
+    assert (st2["tile_y"], st2["stages"], st2["zchunk"]) == (st["tile_y"], st["stages"], st["zchunk"])
+    # the trial steps leave no trace in the results
+    assert np.array_equal(got, ref)
+
+
+def test_trim_memory_returns_pooled_memory(engine_lib):
+    shape = (64, 64, 64)
+    sim = _random_sim(shape, 3, 8, 1, tile_y=8, stages=4)
+    sim.run(8)
+    sim.close()
+    before = _lib.trim_memory(1 << 60)  # keeps every unused byte: only reads the pool
+    after = _lib.trim_memory(0)
+    fields = 12 * 64 * 64 * 64 * 4
+    assert before["reserved"] - after["reserved"] >= fields // 2
+    assert after["used"] == before["used"] and after["reserved"] >= after["used"]
+    # the engine allocates again from the trimmed pool
+    again = _random_sim(shape, 3, 8, 1, tile_y=8, stages=4)
+    again.run(8)
+    assert np.isfinite(again.probe_values()).all()
+    again.close()
+    with pytest.raises(_lib.FdtdError):
+        _lib.trim_memory(-1)
