@@ -230,6 +230,7 @@ def test_gpu_light_cone_replay_equals_recorded(engine_lib, monkeypatch):
         if mode == "full":
             monkeypatch.setenv("RFN_REPLAY_FULL", "1")
         sim, pr, nt, _ = _make(s, 1, TERMS)
+        sim.set_kernel(1, tile_y=8, stages=6)  # the streaming kernels, whose tile lists the replays cut
         if mode == "recorded":
             sim.run_recorded(nt, box)
         else:
