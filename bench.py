@@ -89,9 +89,12 @@ def parse_args():
 def bench_config(nt: int, world: int, n_series: int, n_probes: int) -> dict:
     """The workload's `config`, the same for both arms."""
     cells = GRID[0] * GRID[1] * GRID[2]
+    interior = (GRID[0] - 2 * N_PML) * (GRID[1] - 2 * N_PML) * (GRID[2] - 2 * N_PML)
+    # both time buffers of the 6 fields, the 16-bit index, 12 split halves per PML slab cell
+    state = cells * (48 + 2) + (cells - interior) * 96
     return {"workload": WORKLOAD, "grid": list(GRID), "n_pml": N_PML, "time_steps": nt,
             "dft_frequencies": N_FREQ, "dft_series": n_series, "probes": n_probes,
-            "l2": "inputs larger than L2 (fields+splits+index %.2f GB per replica)" % ((cells * (48 + 96) + cells * 2) / 1e9),
+            "l2": "inputs larger than L2 (fields, split-pair slab stores and index %.2f GB per replica)" % (state / 1e9),
             "parallelism": f"replicas{world}" if world > 1 else "single"}
 
 

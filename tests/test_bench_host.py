@@ -32,3 +32,27 @@ def test_clock_summary(tmp_path):
     out = c.summary()
     assert out["sm_mhz"] == 1935.0 and out["sm_max_mhz"] == 1965.0
     assert out["reasons"] == ["sw_power_cap"] and out["samples"] == 3
+
+
+def test_reference_arm_line_matches_our_contract(monkeypatch):
+    """`bench.py --impl reference` (the CPU restatement of the reference
+    engine, on a bounded sample) prints the metric, unit, direction and config
+    of this engine's line, with zero host-device bytes."""
+    import argparse
+
+    from oracle import cpu_engine
+    monkeypatch.setattr(bench, "sample_steps", lambda n_threads, seconds=10.0: 2)
+    monkeypatch.setattr(cpu_engine, "default_threads", lambda: 2)
+    args = argparse.Namespace(steps=1, warmup=0, nt=bench.NT)
+    line = bench.run_reference(args, 0, 1)
+    assert bench.run_reference(args, 1, 2) is None          # other ranks print nothing
+    assert line["impl"] == "reference"
+    assert (line["metric"], line["unit"], line["higher_is_better"]) == (bench.METRIC, bench.UNIT, True)
+    s = bench.build_model(2)
+    co, pr, *_ = s.pack_inputs(gpu=True)
+    names, _, _ = bench.dft_spec(s, pr)
+    assert line["config"] == bench.bench_config(bench.NT, 1, len(names), len(pr))
+    assert line["e2e"]["h2d_bytes_per_step"] == 0 and line["e2e"]["d2h_bytes_per_step"] == 0
+    assert line["e2e"]["value"] == line["value"] > 0
+    assert line["cpu_baseline"]["kind"] == "port" and line["cpu_baseline"]["cores"] == 2
+    json.dumps(line)
