@@ -138,11 +138,13 @@ int fdtd_synchronize(fdtd_sim* s);
  * tiles), 1 = TMA streaming, one thread per cell (31 x tile_y tiles, tile_y in
  * {4, 6, 8, 12}; stages = shared-memory plane slots, 3..8). zchunk = z planes
  * per tile (0: derived from the grid). tile_y = 0 with variant 1 autotunes:
- * the first run times a few candidate (tile_y, stages, zchunk) shapes on the
- * simulation itself for a few steps and keeps the fastest, remembered per set
- * of grid sizes for the life of the process. The default comes from
- * RFN_FDTD_KERNEL (plain / stream) / RFN_FDTD_TY / RFN_FDTD_STAGES /
- * RFN_FDTD_ZCHUNK or is (1, 0, 6, 0): autotuned streaming.
+ * the first run times a few candidate (tile_y, stages, zchunk, one or two
+ * tile lists) shapes on the simulation itself for a few steps and keeps the
+ * fastest, remembered per set of grid sizes for the life of the process. The
+ * default comes from RFN_FDTD_KERNEL (plain / stream) / RFN_FDTD_TY /
+ * RFN_FDTD_STAGES / RFN_FDTD_ZCHUNK or is (1, 0, 6, 0): autotuned streaming.
+ * RFN_FDTD_ONE_LIST=1 sends the plain tiles of an explicit streaming shape
+ * through the general kernel (one launch per step instead of two).
  * All variants give bit-identical results. The reference has one fixed 8x8x8
  * launch shape (solver.cu:549-557). */
 int fdtd_set_kernel(fdtd_sim* s, int variant, int tile_y, int stages, int zchunk);

@@ -140,15 +140,28 @@ struct KernelConfig {
   int ty = 0;       // tile height; 0 (with variant 1): autotuned (ty, stages, zchunk)
   int stages = 6;   // streaming: shared-memory plane slots
   int zchunk = 0;   // 0: pick from the grid size
+  int one_list = 0; // streaming: every tile through the general instantiation (no plain-tile kernel beside it)
 };
 
-// Step-kernel shapes the autotuner times, (variant, tile height, stages or
-// rows per warp, z chunk), and its choices per set of grid sizes (process-wide).
-constexpr int kTuneCandidates[][4] = {{1, 8, 6, 0},  {1, 8, 8, 0}, {1, 8, 4, 0},  {1, 8, 6, 32}, {1, 12, 4, 0},
-                                      {1, 6, 6, 0},  {1, 4, 6, 0}, {1, 4, 6, 16}, {1, 8, 6, 4},  {1, 4, 6, 4},
-                                      };
+// Step-kernel shapes the autotuner times, (variant, tile height, plane slots,
+// z chunk, one tile list), and its choices per set of grid sizes
+// (process-wide). With one list the plain tiles run in the general kernel's
+// interior path: one launch per step instead of two side by side, which can
+// pay on grids whose step time is mostly launch and pipeline latency.
+constexpr int kTuneCandidates[][5] = {{1, 8, 6, 0, 0}, {1, 8, 8, 0, 0},  {1, 8, 4, 0, 0}, {1, 8, 6, 32, 0},
+                                      {1, 12, 4, 0, 0}, {1, 6, 6, 0, 0}, {1, 4, 6, 0, 0}, {1, 4, 6, 16, 0},
+                                      {1, 8, 6, 4, 0}, {1, 4, 6, 4, 0},  {1, 8, 6, 0, 1}, {1, 8, 6, 4, 1},
+                                      {1, 4, 6, 4, 1}};
+using TuneChoice = std::array<int, 5>;
 std::mutex g_tune_mutex;
-std::map<std::vector<int>, std::array<int, 4>> g_tune_cache;
+std::map<std::vector<int>, TuneChoice> g_tune_cache;
+
+// RFN_FDTD_ONE_LIST=1: explicit streaming shapes run every tile through the
+// general kernel (the autotuner decides this by itself).
+int one_list_env() {
+  const char* v = std::getenv("RFN_FDTD_ONE_LIST");
+  return v && std::atoi(v) != 0 ? 1 : 0;
+}
 
 KernelConfig default_config() {
   KernelConfig c;
@@ -157,6 +170,7 @@ KernelConfig default_config() {
   if (const char* v = std::getenv("RFN_FDTD_TY")) c.ty = std::atoi(v);
   if (const char* v = std::getenv("RFN_FDTD_STAGES")) c.stages = std::atoi(v);
   if (const char* v = std::getenv("RFN_FDTD_ZCHUNK")) c.zchunk = std::atoi(v);
+  c.one_list = one_list_env();
   return c;
 }
 
@@ -570,11 +584,12 @@ struct Engine {
       key.insert(key.end(), {s->nx, s->ny, s->nz});
       nt_min = std::min(nt_min, s->prepared_nt);
     }
-    auto apply = [&](const std::array<int, 4>& c) {
+    auto apply = [&](const TuneChoice& c) {
       cfg.variant = c[0];
       cfg.ty = c[1];
       cfg.stages = c[2];
       cfg.zchunk = c[3];
+      cfg.one_list = c[4];
     };
     {
       std::lock_guard<std::mutex> lock(g_tune_mutex);
@@ -586,15 +601,15 @@ struct Engine {
       }
     }
     const int warm = 2, timed = std::min(8, nt_min - warm);
-    std::array<int, 4> best = {kTuneCandidates[0][0], kTuneCandidates[0][1], kTuneCandidates[0][2],
-                               kTuneCandidates[0][3]};
+    TuneChoice best = {kTuneCandidates[0][0], kTuneCandidates[0][1], kTuneCandidates[0][2],
+                       kTuneCandidates[0][3], kTuneCandidates[0][4]};
     if (timed >= 2) {
       const auto t0 = std::chrono::steady_clock::now();
       init();
       cudaStream_t st = stream();
       float best_ms = 1e30f;
       for (const auto& cand : kTuneCandidates) {
-        apply({cand[0], cand[1], cand[2], cand[3]});
+        apply({cand[0], cand[1], cand[2], cand[3], cand[4]});
         try {
           build_stream_tiles(n_sm);
         } catch (const ArgError& e) {
@@ -612,7 +627,7 @@ struct Engine {
         ++tune_trials;
         if (ms < best_ms) {
           best_ms = ms;
-          best = {cand[0], cand[1], cand[2], cand[3]};
+          best = {cand[0], cand[1], cand[2], cand[3], cand[4]};
         }
       }
       check_error();
@@ -745,7 +760,7 @@ struct Engine {
     {
       std::vector<StreamTile> all;
       all.swap(c.host_tiles);
-      for (const auto& t : all) (t.plain ? c.host_tiles_p : c.host_tiles).push_back(t);
+      for (const auto& t : all) (t.plain && !cfg.one_list ? c.host_tiles_p : c.host_tiles).push_back(t);
     }
     auto cost = [](const StreamTile& t) {
       return (t.z1 - t.z0 + 1) + 2 * (__builtin_popcount(t.split_lo) + __builtin_popcount(t.split_hi));
@@ -1982,6 +1997,7 @@ int fdtd_set_kernel(fdtd_sim* s, int variant, int tile_y, int stages, int zchunk
     c.ty = tile_y;
     c.stages = stages;
     c.zchunk = zchunk;
+    c.one_list = one_list_env();
     s->cfg = c;
     s->engine.reset();
   });
@@ -2206,6 +2222,7 @@ int fdtd_batch_set_kernel(fdtd_batch* b, int variant, int tile_y, int stages, in
     b->engine.cfg.ty = tile_y;
     b->engine.cfg.stages = stages;
     b->engine.cfg.zchunk = zchunk;
+    b->engine.cfg.one_list = one_list_env();
     b->dirty = true;
   });
 }

@@ -196,3 +196,16 @@ def test_host_launched_steps_equal_graph_replay(engine_lib, variant):
     b, sb = _engine_probe_matrix(s, variant, graph=False)
     assert sb["step_launches"] == 200
     assert np.abs(a).max() > 0 and np.array_equal(a, b)
+
+
+@pytest.mark.parametrize("ty,stages,zchunk", [(8, 6, 0), (4, 6, 4)])
+def test_stream_kernel_one_list_equals_plain(engine_lib, monkeypatch, ty, stages, zchunk):
+    """Every tile through the general streaming kernel (its interior path for
+    the plain tiles, one launch per step): the plain kernel's bits."""
+    monkeypatch.setenv("RFN_FDTD_ONE_LIST", "1")
+    s = configs.microstrip(n=(72, 40, 30), n_pml=5, nt=150)
+    a, sa = _engine_probe_matrix(s, 0)
+    b, sb = _engine_probe_matrix(s, 1, tile_y=ty, stages=stages, zchunk=zchunk)
+    assert sb["variant"] == 1 and sb["step_launches"] == 150
+    assert np.abs(a).max() > 0
+    assert np.array_equal(a, b)
