@@ -175,12 +175,19 @@ bool plan_split_storage(CompiledGrid& g, SplitPlan& plan, std::string& err) {
                        std::max(0, nz - t[4] - t[5]);
   plan.slab_cells = ncell - core;
   // sparse split cells: probe cells keep their (unique) probe-list offset as
-  // slot; the others get fresh slots after the probe entries, on rows of their own
+  // slot; the others get fresh slots after the probe entries, on rows of their
+  // own. They lie in the core box that no slab covers (split_store_of gives
+  // the sparse store there), visited in cell order; x planes and (x, y) rows
+  // of the core box without split cells are skipped through the summed-volume
+  // counts.
   int64_t next = int64_t(g.cell_probes.size());
-  for (int x = 0; x < nx; ++x)
-    for (int y = 0; y < ny; ++y)
-      for (int z = 0; z < nz; ++z) {
-        if (split_store_of(t, nx, ny, nz, x, y, z) != kStoreSparse) continue;
+  const int cx0 = t[0], cx1 = nx - t[1], cy0 = t[2], cy1 = ny - t[3], cz0 = t[4], cz1 = nz - t[5];
+  const bool any_sparse = cx1 > cx0 && cy1 > cy0 && cz1 > cz0 && split.count(cx0, cx1, cy0, cy1, cz0, cz1) > 0;
+  for (int x = any_sparse ? cx0 : cx1; x < cx1; ++x) {
+    if (split.count(x, x + 1, cy0, cy1, cz0, cz1) == 0) continue;
+    for (int y = cy0; y < cy1; ++y) {
+      if (split.count(x, x + 1, y, y + 1, cz0, cz1) == 0) continue;
+      for (int z = cz0; z < cz1; ++z) {
         uint16_t& id = g.ids[(size_t(x) * ny + y) * nz + z];
         const Row& r = g.rows[id];
         if (!(r.w[R_FLAGS] & (kFlagESplit | kFlagHSplit))) continue;
@@ -195,6 +202,8 @@ bool plan_split_storage(CompiledGrid& g, SplitPlan& plan, std::string& err) {
         id = uint16_t(g.rows.size());
         g.rows.push_back(u);
       }
+    }
+  }
   plan.n_sparse = next;
   return true;
 }
