@@ -48,6 +48,9 @@ def test_argument_errors(engine_lib):
     sim.add_probe(0, (0, 0, 3))           # ex at y=0 lies on the PEC edge
     with pytest.raises(_lib.FdtdError, match="Source cannot be placed on grid edge"):
         sim.compile()
+    # the pool trim checks its argument before it touches a device
+    with pytest.raises(_lib.FdtdError, match="keep_bytes must be >= 0"):
+        _lib.trim_memory(-1)
 
 
 @pytest.fixture(scope="module")
