@@ -367,13 +367,30 @@ def sample_steps(n_threads: int, seconds: float = 10.0) -> int:
     return int(min(256, max(8, seconds * v * 1e6 / cells)))
 
 
+def host_cpu() -> str:
+    """The host CPU's model name (/proc/cpuinfo), or the platform's processor string."""
+    try:
+        for line in Path("/proc/cpuinfo").read_text().splitlines():
+            if line.lower().startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    import platform
+    return platform.processor() or "unknown"
+
+
 def cpu_baseline_entry():
     from oracle import cpu_engine
     n = cpu_engine.default_threads()
     nt_sample = sample_steps(n)
     v, dt = cpu_sample(nt_sample, n)
+    # the reference solve()'s default n_threads (rfnetwork/solver.py:1410), on a short sample
+    v4, dt4 = cpu_sample(8, 4)
     return {"value": round(v, 2), "unit": UNIT, "cores": n, "kind": "port",
-            "sample": f"{nt_sample} time steps of the {GRID[0]}x{GRID[1]}x{GRID[2]} model ({dt:.1f} s)"}
+            "sample": f"{nt_sample} time steps of the {GRID[0]}x{GRID[1]}x{GRID[2]} model ({dt:.1f} s)",
+            "host": {"cpu": host_cpu(), "nproc": os.cpu_count()},
+            "at_reference_default_threads": {"value": round(v4, 2), "cores": 4,
+                                             "sample": f"8 time steps of the same model ({dt4:.1f} s)"}}
 
 
 def run_reference(args, rank, world):

@@ -56,3 +56,18 @@ def test_reference_arm_line_matches_our_contract(monkeypatch):
     assert line["e2e"]["value"] == line["value"] > 0
     assert line["cpu_baseline"]["kind"] == "port" and line["cpu_baseline"]["cores"] == 2
     json.dumps(line)
+
+
+def test_cpu_baseline_entry_reports_host_and_default_threads(monkeypatch):
+    from oracle import cpu_engine
+    monkeypatch.setattr(bench, "sample_steps", lambda n_threads, seconds=10.0: 2)
+    monkeypatch.setattr(cpu_engine, "default_threads", lambda: 2)
+    calls = []
+    real = bench.cpu_sample
+    monkeypatch.setattr(bench, "cpu_sample", lambda nt, n: calls.append((nt, n)) or real(2, n))
+    out = bench.cpu_baseline_entry()
+    assert calls == [(2, 2), (8, 4)]
+    assert out["kind"] == "port" and out["cores"] == 2 and out["value"] > 0
+    assert out["host"]["nproc"] >= 1 and isinstance(out["host"]["cpu"], str)
+    assert out["at_reference_default_threads"]["cores"] == 4 and out["at_reference_default_threads"]["value"] > 0
+    json.dumps(out)
