@@ -205,3 +205,33 @@ def test_split_storage_plan_confines_pml_pairs_to_the_slabs(engine_lib):
     inner_ids = ids[8:-8, 8:-8, 8:-8][inner]
     assert len(np.unique(inner_ids)) == len(inner_ids)
     assert ((rows[inner_ids, 30] >> 16) > 0).all()   # they carry probe entries (the port sources)
+
+
+def test_sparse_split_cells_get_slots_in_cell_order(engine_lib):
+    """Split cells inside the core box that carry no probe (here: interior
+    cells given differing split decays) get rows of their own whose word 31
+    numbers their sparse slots after the probe entries, in cell order."""
+    s = configs.boxes(n=(64, 56, 40), n_pml=8, n_boxes=6, nt=20, n_ports=2, n_probes=3)
+    co, pr, mo, mem, Nx, Ny, Nz, Nt = s.pack_inputs(gpu=True)
+    co = {k: np.array(v) for k, v in co.items()}
+    planted = [(20, 30, 15), (20, 30, 16), (20, 41, 9), (33, 12, 30), (47, 47, 31)]
+    for c in planted:
+        co["Ca_ex_z"][c] = np.float32(0.5) * co["Ca_ex_y"][c]
+    sim = _lib.Simulation(Nx, Ny, Nz)
+    sim.set_coefficients(co)
+    for p in pr:
+        sim.add_probe(p["field"], p["idx"], p["is_source"], p["values"][:Nt] if p["is_source"] else None)
+    sim.compile()
+    st = sim.stats()
+    ids, rows = sim.material_table()
+    sim.close()
+    assert st["split_slab"] == [8] * 6
+    split = ((rows[:, 30] & 3) != 0)[ids]
+    inner = np.zeros_like(split)
+    inner[8:-8, 8:-8, 8:-8] = split[8:-8, 8:-8, 8:-8]
+    assert st["sparse_split_cells"] == int(inner.sum())
+    slots = [int(rows[ids[c], 31]) for c in planted]   # planted in cell order
+    n_probe_entries = len(pr)
+    assert all(sl >= n_probe_entries for sl in slots)
+    assert slots == sorted(slots) and len(set(slots)) == len(slots)
+    assert all((rows[ids[c], 30] >> 16) == 0 for c in planted)   # no probe entries on them
