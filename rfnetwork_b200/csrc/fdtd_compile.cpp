@@ -72,11 +72,12 @@ using RowMap = std::unordered_map<Row, uint32_t, RowHash, RowEq>;
 
 GradedIndex::GradedIndex(const CompiledGrid& g, uint32_t mask) : nx(g.nx), ny(g.ny), nz(g.nz) {
   // summed-volume table of flagged cells, indexed [x][y][z] with a zero border:
-  // the 2D sums over (y, z) of every x plane (planes in parallel), then the
-  // running sum along x (plane positions in parallel)
+  // the 2D sums over (y, z) of every x plane (planes in parallel, each thread
+  // writing its planes' borders too, so the table needs no serial zero fill),
+  // then the running sum along x (plane positions in parallel)
   sy_ = nz + 1;
   sx_ = int64_t(ny + 1) * sy_;
-  sv_.assign(size_t(nx + 1) * sx_, 0);
+  sv_.reset(new int32_t[size_t(nx + 1) * size_t(sx_)]);
   const int n_threads = int(std::max(1u, std::min(std::thread::hardware_concurrency(), 32u)));
   auto parallel = [n_threads](int64_t n, auto&& body) {  // body(a, b) over [a, b) slices of [0, n)
     const int k = int(std::max<int64_t>(1, std::min<int64_t>(n_threads, n)));
@@ -84,11 +85,15 @@ GradedIndex::GradedIndex(const CompiledGrid& g, uint32_t mask) : nx(g.nx), ny(g.
     for (int t = 0; t < k; ++t) pool.emplace_back(body, n * t / k, n * (t + 1) / k);
     for (auto& th : pool) th.join();
   };
+  int32_t* const sv = sv_.get();
   parallel(nx, [&](int64_t xa, int64_t xb) {
+    if (xa == 0) std::fill(sv, sv + sx_, 0);  // the x = -1 plane
     for (int64_t x = xa; x < xb; ++x) {
-      int32_t* P = sv_.data() + (x + 1) * sx_;
+      int32_t* P = sv + (x + 1) * sx_;
+      std::fill(P, P + sy_, 0);  // the y = -1 row
       for (int y = 0; y < ny; ++y) {
         const uint16_t* id = g.ids.data() + (size_t(x) * ny + y) * nz;
+        P[(y + 1) * sy_] = 0;  // the z = -1 entry
         int32_t run = 0;
         for (int z = 0; z < nz; ++z) {
           run += (g.rows[id[z]].w[R_FLAGS] & mask) ? 1 : 0;
@@ -99,7 +104,7 @@ GradedIndex::GradedIndex(const CompiledGrid& g, uint32_t mask) : nx(g.nx), ny(g.
   });
   parallel(sx_, [&](int64_t ja, int64_t jb) {
     for (int x = 1; x <= nx; ++x) {
-      int32_t* cur = sv_.data() + x * sx_;
+      int32_t* cur = sv + x * sx_;
       const int32_t* prev = cur - sx_;
       for (int64_t j = ja; j < jb; ++j) cur[j] += prev[j];
     }
@@ -110,7 +115,7 @@ int64_t GradedIndex::count(int x0, int x1, int y0, int y1, int z0, int z1) const
   x0 = std::max(x0, 0); y0 = std::max(y0, 0); z0 = std::max(z0, 0);
   x1 = std::min(x1, nx); y1 = std::min(y1, ny); z1 = std::min(z1, nz);
   if (x1 <= x0 || y1 <= y0 || z1 <= z0) return 0;
-  auto at = [&](int x, int y, int z) { return int64_t(sv_[x * sx_ + y * sy_ + z]); };
+  auto at = [&](int x, int y, int z) { return int64_t(sv_[size_t(x * sx_ + y * sy_ + z)]); };
   return at(x1, y1, z1) - at(x0, y1, z1) - at(x1, y0, z1) - at(x1, y1, z0) + at(x0, y0, z1) + at(x0, y1, z0) +
          at(x1, y0, z0) - at(x0, y0, z0);
 }

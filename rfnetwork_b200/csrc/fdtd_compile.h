@@ -4,6 +4,7 @@
 #pragma once
 
 #include <cstdint>
+#include <memory>
 #include <string>
 #include <vector>
 
@@ -123,7 +124,7 @@ class GradedIndex {
   int nx, ny, nz;
 
  private:
-  std::vector<int32_t> sv_;
+  std::unique_ptr<int32_t[]> sv_;  // every entry written by the constructor's parallel passes
   int64_t sx_, sy_;
 };
 
