@@ -27,6 +27,7 @@
 #include <algorithm>
 #include <chrono>
 #include <cstring>
+#include <memory>
 #include <thread>
 #include <unordered_map>
 
@@ -292,7 +293,8 @@ bool compile_grid(int nx, int ny, int nz, const float* const* coef, const std::v
   n_threads = std::max(1, std::min(n_threads, nx));
   std::vector<RowMap> local_maps(n_threads);
   std::vector<std::vector<Row>> local_rows(n_threads);
-  std::vector<uint32_t> local_ids(static_cast<size_t>(ncell));
+  // every cell's entry is written by the worker of its x slab (no serial zero fill)
+  std::unique_ptr<uint32_t[]> local_ids(new uint32_t[size_t(ncell)]);
   std::vector<int64_t> e_split(n_threads, 0), h_split(n_threads, 0);
   auto work = [&](int t, int xa, int xb) {
     RowMap& map = local_maps[t];
